@@ -1,0 +1,216 @@
+"""Generate golden vectors by running the reference's own Python operators.
+
+Run in a container that has the reference source tree (read-only is fine):
+
+    python tests/golden/make_golden.py /path/to/holotomocupy/src
+
+The reference is CuPy code; ``oracle/refshim.py`` maps CuPy to NumPy and its
+raw CUDA kernels to the NumPy restatements in ``oracle/kernels_np.py``, then
+imports ``tomo.py``, ``shift.py``, ``propagation.py`` and ``rec_mpi.py``
+unchanged.  Everything runs in the reference's FP32 arithmetic.  Outputs are
+small ``.npz`` files next to this script; the GPU parity tests and the oracle
+tests compare against them.
+"""
+import os
+import sys
+import types
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+
+from oracle.refshim import load_reference  # noqa: E402
+
+
+def crand(rng, shape, scale=1.0):
+    return ((rng.standard_normal(shape) + 1j * rng.standard_normal(shape)) * scale).astype("complex64")
+
+
+def frand(rng, shape, scale=1.0):
+    return (rng.standard_normal(shape) * scale).astype("float32")
+
+
+def tomo_cases(ns):
+    out = {}
+    for (n, nz, ntheta, mask_r, tag) in [(32, 4, 24, 1, "a"), (18, 3, 10, 0, "b"), (48, 2, 40, 0.9, "c")]:
+        rng = np.random.default_rng(100 + n)
+        theta = np.linspace(0, np.pi, ntheta, endpoint=False).astype("float32")
+        t = ns.tomo.Tomo(n, nz, theta, mask_r)
+        xc = crand(rng, (nz, n, n))
+        yc = crand(rng, (ntheta, nz, n))
+        xf = frand(rng, (nz, n, n))
+        yf = frand(rng, (ntheta, nz, n))
+        out.update({
+            f"{tag}_n": n, f"{tag}_nz": nz, f"{tag}_mask_r": mask_r, f"{tag}_theta": theta,
+            f"{tag}_xc": xc, f"{tag}_yc": yc, f"{tag}_xf": xf, f"{tag}_yf": yf,
+            f"{tag}_Rxc": t.R(ns.cp.array(xc)).get(), f"{tag}_RTyc": t.RT(ns.cp.array(yc)).get(),
+            f"{tag}_Rxf": t.R(ns.cp.array(xf)).get(), f"{tag}_RTyf": t.RT(ns.cp.array(yf)).get(),
+            f"{tag}_mask": np.asarray(t.mask, dtype="float32") * np.ones((n, n), "float32"),
+            f"{tag}_m": t.pars[0], f"{tag}_phi": np.asarray(t.pars[2]),
+        })
+    np.savez_compressed(os.path.join(HERE, "tomo.npz"), **out)
+
+
+def prop_cases(ns):
+    out = {}
+    wavelength = 1.24e-9 / 17.1
+    for (n, nz, ntheta, tag) in [(32, 24, 3, "a"), (64, 64, 2, "b"), (48, 36, 2, "c")]:
+        rng = np.random.default_rng(200 + n)
+        distance = np.array([3e-3, 4.5e-3, 6e-3])
+        p = ns.propagation.Propagation(n, nz, ntheta, len(distance), wavelength, 20e-9, distance)
+        a = crand(rng, (ntheta, nz, n))
+        b = crand(rng, (ntheta, nz, n))
+        out.update({f"{tag}_n": n, f"{tag}_nz": nz, f"{tag}_a": a, f"{tag}_b": b,
+                    f"{tag}_distance": distance, f"{tag}_wavelength": wavelength,
+                    f"{tag}_voxelsize": 20e-9, f"{tag}_fker": np.asarray(p.fker)})
+        for j in range(len(distance)):
+            out[f"{tag}_D{j}"] = p.D(ns.cp.array(a), j).get()
+            out[f"{tag}_DT{j}"] = p.DT(ns.cp.array(b), j).get()
+        out[f"{tag}_D2d"] = p.D(ns.cp.array(a[0]), 1).get()
+    np.savez_compressed(os.path.join(HERE, "prop.npz"), **out)
+
+
+def shift_cases(ns):
+    out = {}
+    for dt in ("complex64", "float32"):
+        for (n, npsi, nz, nzpsi, ntheta, tag) in [(24, 32, 20, 28, 3, "a"), (32, 32, 32, 32, 2, "b")]:
+            key = f"{dt}_{tag}"
+            rng = np.random.default_rng(300 + n + len(dt))
+            s = ns.shift.Shift(n, npsi, nz, nzpsi, dt)
+            mk = (lambda sh: crand(rng, sh)) if dt == "complex64" else (lambda sh: frand(rng, sh))
+            psi = mk((ntheta, nzpsi, npsi))
+            c1 = mk((ntheta, nzpsi, npsi))
+            c2 = mk((ntheta, nzpsi, npsi))
+            g = mk((ntheta, nz, n))
+            r = (rng.uniform(-3, 3, (ntheta, 2))).astype("float32")
+            d1 = frand(rng, (ntheta, 2))
+            d2 = frand(rng, (ntheta, 2))
+            m = np.ones(ntheta, "float32")
+            if tag == "a":
+                m = np.array([1.0, 0.93, 1.07], "float32")[:ntheta]
+            C = lambda x: ns.cp.array(x)
+            c = s.coeff(C(psi))
+            o1, o2 = s.dcurlySadjc(c, C(r), C(m), C(g))
+            out.update({
+                f"{key}_dims": np.array([n, npsi, nz, nzpsi, ntheta]),
+                f"{key}_psi": psi, f"{key}_c1": c1, f"{key}_c2": c2, f"{key}_g": g,
+                f"{key}_r": r, f"{key}_d1": d1, f"{key}_d2": d2, f"{key}_m": m,
+                f"{key}_coeff": c.get(),
+                f"{key}_S": s.S(c, C(r), C(m)).get(),
+                f"{key}_Sadj": s.Sadj(C(g), C(r), C(m)).get(),
+                f"{key}_curlyS": s.curlyS(C(psi), C(r), C(m)).get(),
+                f"{key}_dS": s.dcurlySc(c, C(r), C(m), C(c1), C(d1)).get(),
+                f"{key}_d2S": s.d2curlySc(c, C(r), C(m), C(c1), C(d1), C(c2), C(d2)).get(),
+                f"{key}_dSadj1": o1.get(), f"{key}_dSadj2": o2.get(),
+            })
+    np.savez_compressed(os.path.join(HERE, "shift.npz"), **out)
+
+
+def rec_args(n, ntheta, ndist, nobj, niter=1):
+    return types.SimpleNamespace(
+        energy=17.1, detector_pixelsize=1.4760147601476e-6 * 2 * 2048 / n,
+        focustodetectordistance=1.217,
+        z1=(np.array([5.110, 5.464, 6.879, 9.817]) * 1e-3 + 3.135e-3)[:ndist],
+        theta=np.linspace(0, np.pi, ntheta, endpoint=False).astype("float32"),
+        ndist=ndist, ntheta=ntheta, nz=n, n=n, nzobj=nobj, nobj=nobj,
+        obj_dtype="complex64", mask=0.9, lam_prbfit=0.0, rho=[1, 0.05, 0.02],
+        niter=niter, nchunk=max(nobj, ntheta), vis_step=-1, err_step=-1, start_iter=0,
+        comm=sys.modules["mpi4py"].MPI.COMM_WORLD)
+
+
+def phantom(n, rng, nell=6):
+    """Small ellipsoid phantom: delta/beta inside random ellipsoids."""
+    ax = np.arange(n) - n / 2
+    z, y, x = np.meshgrid(ax, ax, ax, indexing="ij")
+    obj = np.zeros((n, n, n), "complex64")
+    for _ in range(nell):
+        c = rng.uniform(-n / 5, n / 5, 3)
+        s = rng.uniform(n / 12, n / 5, 3)
+        delta = rng.uniform(1, 3)
+        inside = ((z - c[0]) / s[0]) ** 2 + ((y - c[1]) / s[1]) ** 2 + ((x - c[2]) / s[2]) ** 2 <= 1
+        obj[inside] += (-delta + 1j * delta / 50) * 0.05
+    return obj
+
+
+def rec_cases(ns):
+    out = {}
+    # ---- cascade building blocks at one point
+    n, ntheta, ndist, nobj = 32, 6, 2, 32
+    rng = np.random.default_rng(42)
+    args = rec_args(n, ntheta, ndist, nobj)
+    rec = ns.rec_mpi.Rec(args)
+    prb = (1 + 0.2 * crand(rng, (ndist, n, n))).astype("complex64")
+    proj = crand(rng, (ntheta, nobj, nobj), 0.1)
+    pos = frand(rng, (ntheta, ndist, 2), 0.8)
+    data = (np.abs(frand(rng, (ntheta, ndist, n, n))) + 0.5).astype("float32")
+    dirs = {}
+    for name in ("g", "e"):
+        dirs[name] = {"prb": crand(rng, (ndist, n, n), 0.1), "proj": crand(rng, (ntheta, nobj, nobj), 0.05),
+                      "pos": frand(rng, (ntheta, ndist, 2), 0.3)}
+    rec.data[:] = data
+    rec.eff_demagnifications[:] = (1 + rec.shrink_nd) / ns.cp.array(rec.norm_magnifications[None, :])
+    vars_ = {"prb": ns.cp.array(prb), "proj": proj.copy(), "pos": ns.cp.array(pos)}
+    grads = {k: (ns.cp.array(v) if k != "proj" else v.copy()) for k, v in dirs["g"].items()}
+    etas = {k: (ns.cp.array(v) if k != "proj" else v.copy()) for k, v in dirs["e"].items()}
+    Fval = float(ns.cp.asnumpy(rec.min(vars_["prb"], None, vars_["pos"], vars_["proj"])))
+    h_ge = float(rec.hessian_cascade(vars_, grads, etas))
+    h_ee = float(rec.hessian_cascade(vars_, etas, etas))
+    g_out = {"prb": ns.cp.zeros((ndist, n, n), "complex64"), "proj": np.zeros((ntheta, nobj, nobj), "complex64"),
+             "pos": ns.cp.zeros((ntheta, ndist, 2), "float32")}
+    rec.gradients_cascade(vars_, g_out)
+    out.update({
+        "c_dims": np.array([n, ntheta, ndist, nobj]), "c_prb": prb, "c_proj": proj, "c_pos": pos, "c_data": data,
+        "c_F": Fval, "c_h_ge": h_ge, "c_h_ee": h_ee,
+        "c_grad_prb": np.asarray(g_out["prb"]), "c_grad_proj": np.asarray(g_out["proj"]),
+        "c_grad_pos": np.asarray(g_out["pos"]),
+        "c_fker": np.asarray(rec.cl_prop.fker),
+    })
+    for name in ("g", "e"):
+        for k, v in dirs[name].items():
+            out[f"c_{name}_{k}"] = v
+    out["c_norm_mag"] = np.asarray(rec.norm_magnifications)
+    # ---- a short BH run from a synthetic phantom
+    n, ntheta, ndist, nobj, niter = 32, 12, 2, 32, 4
+    rng = np.random.default_rng(7)
+    args = rec_args(n, ntheta, ndist, nobj, niter)
+    rec = ns.rec_mpi.Rec(args)
+    obj = phantom(nobj, rng)
+    prb = (1 + 0.1 * crand(rng, (ndist, n, n))).astype("complex64")
+    pos = frand(rng, (ntheta, ndist, 2), 1.0)
+    pos_err = frand(rng, (ntheta, ndist, 2), 0.2)
+    rec.vars["obj"][:] = obj
+    rec.vars["prb"][:] = ns.cp.array(prb)
+    rec.vars["pos"][:] = ns.cp.array(pos)
+    rec.gen_sqrt_data(rec.vars, rec.data)
+    data = np.array(rec.data)
+    rec.vars["obj"][:] = 0
+    rec.vars["prb"][:] = ns.cp.array(1)
+    rec.vars["pos"][:] = ns.cp.array(pos + pos_err)
+    pairs = []
+    orig = rec.allreduce2
+    rec.allreduce2 = lambda a, b: (pairs.append((float(a), float(b))), orig(a, b))[1]
+    rec.BH()
+    out.update({
+        "bh_dims": np.array([n, ntheta, ndist, nobj, niter]), "bh_obj_true": obj, "bh_prb_true": prb,
+        "bh_pos_true": pos, "bh_pos_err": pos_err, "bh_data": data,
+        "bh_obj": np.array(rec.vars["obj"]), "bh_prb": np.asarray(rec.vars["prb"]),
+        "bh_pos": np.asarray(rec.vars["pos"]), "bh_proj": np.array(rec.vars["proj"]),
+        "bh_topbottom": np.array(pairs, dtype="float64"),
+    })
+    np.savez_compressed(os.path.join(HERE, "rec.npz"), **out)
+
+
+def main():
+    src = sys.argv[1] if len(sys.argv) > 1 else None
+    if src is None:
+        raise SystemExit("usage: make_golden.py <reference src dir>")
+    ns = load_reference(src)
+    which = sys.argv[2:] or ["tomo", "prop", "shift", "rec"]
+    for w in which:
+        {"tomo": tomo_cases, "prop": prop_cases, "shift": shift_cases, "rec": rec_cases}[w](ns)
+        print("wrote", w)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,121 @@
+"""The CPU oracle against the golden vectors made by running the reference's
+own operators (tests/golden/make_golden.py).  FP32 mode must reproduce the
+reference to FP32 rounding; FP64 mode differs by the reference's own FP32
+error (and, for the propagator, by the FP32 rounding of its Fresnel table)."""
+import types
+
+import numpy as np
+import pytest
+
+from conftest import rel_l2
+from oracle import holo_oracle as O
+
+TOL32 = 2e-6      # oracle in FP32 vs reference in FP32
+TOL64 = 1e-5      # FP64 oracle vs FP32 reference (operators other than D/DT)
+TOL64_D = 1e-4    # FP64 oracle (exact Fresnel table) vs FP32 reference table
+
+
+@pytest.mark.parametrize("dt,tol", [("complex64", TOL32), ("complex128", TOL64)])
+@pytest.mark.parametrize("tag", ["a", "b", "c"])
+def test_tomo(golden, tag, dt, tol):
+    g = golden("tomo")
+    n, nz = int(g[f"{tag}_n"]), int(g[f"{tag}_nz"])
+    t = O.Tomo(n, nz, g[f"{tag}_theta"], float(g[f"{tag}_mask_r"]), dt)
+    assert t.m == int(g[f"{tag}_m"])
+    assert rel_l2(t.phi, g[f"{tag}_phi"]) < tol
+    for src, op, key in [("xc", t.R, "Rxc"), ("yc", t.RT, "RTyc"), ("xf", t.R, "Rxf"), ("yf", t.RT, "RTyf")]:
+        out = op(g[f"{tag}_{src}"])
+        assert out.shape == g[f"{tag}_{key}"].shape
+        assert np.iscomplexobj(out) == np.iscomplexobj(g[f"{tag}_{key}"])
+        assert rel_l2(out, g[f"{tag}_{key}"]) < tol
+
+
+@pytest.mark.parametrize("dt,tol", [("complex64", TOL32), ("complex128", TOL64_D)])
+@pytest.mark.parametrize("tag", ["a", "b", "c"])
+def test_propagation(golden, tag, dt, tol):
+    g = golden("prop")
+    n, nz = int(g[f"{tag}_n"]), int(g[f"{tag}_nz"])
+    p = O.Propagation(n, nz, 3, 3, float(g[f"{tag}_wavelength"]), float(g[f"{tag}_voxelsize"]),
+                      g[f"{tag}_distance"], dt)
+    for j in range(3):
+        assert rel_l2(p.D(g[f"{tag}_a"], j), g[f"{tag}_D{j}"]) < tol
+        assert rel_l2(p.DT(g[f"{tag}_b"], j), g[f"{tag}_DT{j}"]) < tol
+    assert p.D(g[f"{tag}_a"][0], 1).shape == g[f"{tag}_D2d"].shape
+
+
+def test_propagation_reference_table(golden):
+    """table='ref32' rebuilds the reference's FP32 Fresnel table bit for bit."""
+    g = golden("prop")
+    for tag in "abc":
+        n, nz = int(g[f"{tag}_n"]), int(g[f"{tag}_nz"])
+        t = O.fresnel_kernel(n, nz, float(g[f"{tag}_wavelength"]), float(g[f"{tag}_voxelsize"]),
+                             g[f"{tag}_distance"], "ref32")
+        np.testing.assert_array_equal(t, g[f"{tag}_fker"])
+
+
+@pytest.mark.parametrize("dt,tol", [("complex64", TOL32), ("complex128", TOL64)])
+@pytest.mark.parametrize("key", ["complex64_a", "complex64_b", "float32_a", "float32_b"])
+def test_shift(golden, key, dt, tol):
+    g = golden("shift")
+    G = lambda k: g[f"{key}_{k}"]
+    n, npsi, nz, nzpsi, nt = [int(v) for v in G("dims")]
+    s = O.Shift(n, npsi, nz, nzpsi, key.split("_")[0], dt)
+    c = s.coeff(G("psi"))
+    assert rel_l2(c, G("coeff")) < tol
+    assert rel_l2(s.S(c, G("r"), G("m")), G("S")) < tol
+    assert rel_l2(s.Sadj(G("g"), G("r"), G("m")), G("Sadj")) < tol
+    assert rel_l2(s.curlyS(G("psi"), G("r"), G("m")), G("curlyS")) < tol
+    assert rel_l2(s.dcurlySc(c, G("r"), G("m"), G("c1"), G("d1")), G("dS")) < tol
+    assert rel_l2(s.d2curlySc(c, G("r"), G("m"), G("c1"), G("d1"), G("c2"), G("d2")), G("d2S")) < tol
+    o1, o2 = s.dcurlySadjc(c, G("r"), G("m"), G("g"))
+    assert rel_l2(o1, G("dSadj1")) < tol
+    assert rel_l2(o2, G("dSadj2")) < tol
+
+
+def rec_args(n, ntheta, ndist, nobj, niter=1):
+    """The solver arguments make_golden.py used."""
+    return types.SimpleNamespace(
+        energy=17.1, detector_pixelsize=1.4760147601476e-6 * 2 * 2048 / n,
+        focustodetectordistance=1.217,
+        z1=(np.array([5.110, 5.464, 6.879, 9.817]) * 1e-3 + 3.135e-3)[:ndist],
+        theta=np.linspace(0, np.pi, ntheta, endpoint=False).astype("float32"),
+        ndist=ndist, ntheta=ntheta, nz=n, n=n, nzobj=nobj, nobj=nobj,
+        obj_dtype="complex64", mask=0.9, lam_prbfit=0.0, rho=[1, 0.05, 0.02],
+        niter=niter, nchunk=max(nobj, ntheta), vis_step=-1, err_step=-1, start_iter=0)
+
+
+@pytest.mark.parametrize("dt,tol", [("complex64", TOL32), ("complex128", TOL64)])
+def test_cascade(golden, dt, tol):
+    g = golden("rec")
+    n, ntheta, ndist, nobj = [int(v) for v in g["c_dims"]]
+    rec = O.Rec(rec_args(n, ntheta, ndist, nobj), dt)
+    rec.data[:] = g["c_data"]
+    rec.eff_demagnifications[:] = (1 + rec.shrink_nd) / rec.norm_magnifications[None, :]
+    v = {"prb": g["c_prb"].astype(rec.cdt), "proj": g["c_proj"].astype(rec.cdt), "pos": g["c_pos"]}
+    gr = {k: g[f"c_g_{k}"] for k in ("prb", "proj", "pos")}
+    et = {k: g[f"c_e_{k}"] for k in ("prb", "proj", "pos")}
+    assert abs(rec.min(v["prb"], None, v["pos"], v["proj"]) / float(g["c_F"]) - 1) < tol
+    assert abs(rec.hessian_cascade(v, gr, et) / float(g["c_h_ge"]) - 1) < tol
+    assert abs(rec.hessian_cascade(v, et, et) / float(g["c_h_ee"]) - 1) < tol
+    out = {k: np.zeros_like(v[k]) for k in v}
+    rec.gradients_cascade(v, out)
+    for k in ("prb", "proj", "pos"):
+        assert rel_l2(out[k], g[f"c_grad_{k}"]) < 5 * tol
+
+
+@pytest.mark.parametrize("dt,tol", [("complex64", 1e-5), ("complex128", 1e-5)])
+def test_bh(golden, dt, tol):
+    g = golden("rec")
+    n, ntheta, ndist, nobj, niter = [int(v) for v in g["bh_dims"]]
+    rec = O.Rec(rec_args(n, ntheta, ndist, nobj, niter), dt)
+    rec.vars["obj"][:] = g["bh_obj_true"]
+    rec.vars["prb"][:] = g["bh_prb_true"]
+    rec.vars["pos"][:] = g["bh_pos_true"]
+    rec.gen_sqrt_data(rec.vars, rec.data)
+    assert rel_l2(rec.data, g["bh_data"]) < 1e-6
+    rec.vars["obj"][:] = 0
+    rec.vars["prb"][:] = 1
+    rec.vars["pos"][:] = g["bh_pos_true"] + g["bh_pos_err"]
+    rec.BH()
+    for k in ("obj", "prb", "pos", "proj"):
+        assert rel_l2(rec.vars[k], g[f"bh_{k}"]) < tol
