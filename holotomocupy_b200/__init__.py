@@ -1,0 +1,10 @@
+"""B200-native operator chain of holotomocupy's Bilinear-Hessian solver.
+
+Drop-in classes with the reference's Python API (CUDA torch tensors in place
+of CuPy arrays): ``Propagation`` (Fresnel D/DT), ``Tomo`` (USFFT R/RT),
+``Shift`` (B-spline shift family) and ``Rec`` (the BH cascade and solver).
+All compute runs in ``lib/libholotomo_b200.so`` (sm_100a).
+"""
+from .propagation import Propagation, fresnel_table  # noqa: F401
+
+__version__ = "0.1.0"

@@ -1,0 +1,74 @@
+"""ctypes binding of ``lib/libholotomo_b200.so`` (declared in include/holotomo_b200.h).
+
+The library is required: importing an operator without it raises at once,
+there is no fallback implementation.
+"""
+import ctypes
+import os
+
+import torch
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "lib", "libholotomo_b200.so")
+
+_c_int, _c_long, _vp = ctypes.c_int, ctypes.c_long, ctypes.c_void_p
+_c_float, _c_double = ctypes.c_float, ctypes.c_double
+
+# name -> argtypes (all return int status unless listed in _RESTYPE)
+SIGNATURES = {
+    "ht_version": [],
+    "ht_last_error": [],
+    "ht_prop_create": [_c_int, _c_int, _c_int, _vp, ctypes.POINTER(_vp)],
+    "ht_prop_destroy": [_vp],
+    "ht_prop_D": [_vp, _vp, _vp, _c_long, _c_int, _vp],
+    "ht_prop_DT": [_vp, _vp, _vp, _c_long, _c_int, _vp],
+}
+_RESTYPE = {"ht_last_error": ctypes.c_char_p}
+
+_lib = None
+
+
+class HoloError(RuntimeError):
+    """A holotomo_b200 entry point returned a non-zero status."""
+
+
+def lib():
+    """Load the shared library once; raise if it is missing."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(
+                f"{LIB_PATH} is missing: build it with `python -m holotomocupy_b200.build` "
+                "(the operators have no CPU fallback)")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, argt in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.argtypes = argt
+            fn.restype = _RESTYPE.get(name, _c_int)
+        _lib = L
+    return _lib
+
+
+def call(name, *args):
+    """Call an entry point and raise HoloError on a non-zero status."""
+    L = lib()
+    st = getattr(L, name)(*args)
+    if st != 0:
+        msg = L.ht_last_error().decode(errors="replace")
+        raise HoloError(f"{name} failed with status {st}: {msg}")
+    return st
+
+
+def stream_ptr(device=None):
+    return _vp(torch.cuda.current_stream(device).cuda_stream)
+
+
+def ptr(t):
+    return _vp(t.data_ptr())
+
+
+def require_cuda(t, name, dtype=None):
+    if not isinstance(t, torch.Tensor) or not t.is_cuda:
+        raise TypeError(f"{name} must be a CUDA torch tensor")
+    if dtype is not None and t.dtype != dtype:
+        raise TypeError(f"{name} must have dtype {dtype}, got {t.dtype}")

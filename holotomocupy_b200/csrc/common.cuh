@@ -1,0 +1,65 @@
+// Shared helpers for the holotomo B200 kernels: complex arithmetic, error
+// reporting, and the per-size twiddle tables.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstdio>
+#include <string>
+
+namespace ht {
+
+// ----------------------------------------------------------------- errors
+// Thread-local last-error message (read through ht_last_error()).
+void set_error(const std::string& msg);
+const char* last_error();
+
+#define HT_CHECK_CUDA(expr)                                                     \
+  do {                                                                          \
+    cudaError_t _e = (expr);                                                    \
+    if (_e != cudaSuccess) {                                                    \
+      ::ht::set_error(std::string(#expr) + ": " + cudaGetErrorString(_e));      \
+      return 2;                                                                 \
+    }                                                                           \
+  } while (0)
+
+#define HT_REQUIRE(cond, msg)                                                   \
+  do {                                                                          \
+    if (!(cond)) {                                                              \
+      ::ht::set_error(msg);                                                     \
+      return 1;                                                                 \
+    }                                                                           \
+  } while (0)
+
+// Status codes returned by every entry point.
+enum Status : int { kOk = 0, kBadArgument = 1, kCudaError = 2, kUnsupported = 3 };
+
+// ------------------------------------------------------------ complex math
+__host__ __device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__host__ __device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__host__ __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+  return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+// a * conj(b)
+__host__ __device__ __forceinline__ float2 cmulc(float2 a, float2 b) {
+  return make_float2(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y);
+}
+__host__ __device__ __forceinline__ float2 cconj(float2 a) { return make_float2(a.x, -a.y); }
+__host__ __device__ __forceinline__ float2 cscale(float2 a, float s) { return make_float2(a.x * s, a.y * s); }
+// multiply by -i (forward sign) or +i (inverse sign)
+template <bool INV>
+__host__ __device__ __forceinline__ float2 rot(float2 a) {
+  return INV ? make_float2(-a.y, a.x) : make_float2(a.y, -a.x);
+}
+__host__ __device__ __forceinline__ float2 cmul_i(float2 a) { return make_float2(-a.y, a.x); }  // i*a
+
+// --------------------------------------------------------- twiddle tables
+// For every supported transform length N the library keeps, per device, a
+// table tw4[m] = exp(-2*pi*i*m/(4N)), m in [0, 4N), computed in double and
+// rounded once.  FFT twiddles W_N^a are tw4[4a]; the DCT pre/post twiddles
+// exp(-i*pi*k/(2N)) are tw4[k].
+const float2* twiddle_table(int N, int device);  // nullptr + error on failure
+
+// Sizes accepted by the line transforms: N = 2^a 3^b from the list below.
+bool fft_size_supported(int N);
+
+}  // namespace ht

@@ -1,0 +1,195 @@
+// Shared-memory Stockham FFT for one line of N complex samples held by a
+// group of T = N/E threads (E samples per thread in registers).
+//
+// Every stage of radix R reads R samples per butterfly from shared memory at
+// stride N/R (coalesced across the group), multiplies by the twiddles
+// W_{P R}^{i j}, runs an R-point DFT in registers and writes the results to
+// their self-sorting positions (b - i) R + i + j P, where P is the product of
+// the radices already applied and i = b mod P.  The result is in natural
+// order, so no bit reversal pass is needed.
+//
+// The line lives in shared memory behind an accessor (row lines are
+// contiguous with one pad slot every 16 samples; column lines of a tile are
+// strided by the tile width), so the same code serves row and column passes.
+#pragma once
+#include "common.cuh"
+
+namespace ht {
+
+// ------------------------------------------------------- small DFT kernels
+template <int R, bool INV>
+struct Dft;
+
+template <bool INV>
+struct Dft<2, INV> {
+  static __device__ __forceinline__ void run(float2* v) {
+    float2 a = v[0], b = v[1];
+    v[0] = cadd(a, b);
+    v[1] = csub(a, b);
+  }
+};
+
+template <bool INV>
+struct Dft<3, INV> {
+  static __device__ __forceinline__ void run(float2* v) {
+    const float s3 = 0.86602540378443864676f;  // sqrt(3)/2
+    float2 a = v[0], b = v[1], c = v[2];
+    float2 t1 = cadd(b, c), t2 = csub(b, c);
+    float2 m1 = make_float2(a.x - 0.5f * t1.x, a.y - 0.5f * t1.y);
+    float2 m2 = rot<INV>(cscale(t2, s3));
+    v[0] = cadd(a, t1);
+    v[1] = cadd(m1, m2);
+    v[2] = csub(m1, m2);
+  }
+};
+
+template <bool INV>
+struct Dft<4, INV> {
+  static __device__ __forceinline__ void run(float2* v) {
+    float2 t0 = cadd(v[0], v[2]), t1 = csub(v[0], v[2]);
+    float2 t2 = cadd(v[1], v[3]), t3 = rot<INV>(csub(v[1], v[3]));
+    v[0] = cadd(t0, t2);
+    v[2] = csub(t0, t2);
+    v[1] = cadd(t1, t3);
+    v[3] = csub(t1, t3);
+  }
+};
+
+template <bool INV>
+struct Dft<8, INV> {
+  static __device__ __forceinline__ void run(float2* v) {
+    const float r = 0.70710678118654752440f;
+    float2 e[4] = {v[0], v[2], v[4], v[6]};
+    float2 o[4] = {v[1], v[3], v[5], v[7]};
+    Dft<4, INV>::run(e);
+    Dft<4, INV>::run(o);
+    // W8^1 = (1 -/+ i)/sqrt2, W8^2 = -/+ i, W8^3 = (-1 -/+ i)/sqrt2
+    float2 o1 = INV ? make_float2(r * (o[1].x - o[1].y), r * (o[1].x + o[1].y))
+                    : make_float2(r * (o[1].x + o[1].y), r * (o[1].y - o[1].x));
+    float2 o2 = rot<INV>(o[2]);
+    float2 o3 = INV ? make_float2(-r * (o[3].x + o[3].y), r * (o[3].x - o[3].y))
+                    : make_float2(r * (o[3].y - o[3].x), -r * (o[3].x + o[3].y));
+    v[0] = cadd(e[0], o[0]);
+    v[4] = csub(e[0], o[0]);
+    v[1] = cadd(e[1], o1);
+    v[5] = csub(e[1], o1);
+    v[2] = cadd(e[2], o2);
+    v[6] = csub(e[2], o2);
+    v[3] = cadd(e[3], o3);
+    v[7] = csub(e[3], o3);
+  }
+};
+
+// ----------------------------------------------------- shared-memory views
+// Row line: contiguous, one pad slot every 16 samples (bank-conflict free for
+// the stride-R writes of the first stages).
+struct SmRow {
+  float2* p;
+  static __host__ __device__ constexpr int padded(int n) { return n + (n >> 4); }
+  __device__ __forceinline__ float2 ld(int k) const { return p[k + (k >> 4)]; }
+  __device__ __forceinline__ void st(int k, float2 v) const { p[k + (k >> 4)] = v; }
+};
+
+// Column line inside a [N][C] tile (row-major, C columns side by side).
+template <int C>
+struct SmCol {
+  float2* p;  // points at column c of row 0
+  __device__ __forceinline__ float2 ld(int k) const { return p[k * C]; }
+  __device__ __forceinline__ void st(int k, float2 v) const { p[k * C] = v; }
+};
+
+// --------------------------------------------------------------- the plan
+template <int... Rs>
+struct Radices {};
+
+// Plan<N>: samples per thread E and the radix sequence (product = N, every
+// radix divides E).
+template <int N>
+struct Plan;
+#define HT_PLAN(NN, EE, ...)                          \
+  template <>                                         \
+  struct Plan<NN> {                                   \
+    static constexpr int E = EE;                      \
+    static constexpr int T = NN / EE;                 \
+    using R = Radices<__VA_ARGS__>;                   \
+  };
+HT_PLAN(18, 6, 2, 3, 3)
+HT_PLAN(24, 12, 4, 3, 2)
+HT_PLAN(32, 8, 8, 4)
+HT_PLAN(36, 12, 4, 3, 3)
+HT_PLAN(48, 12, 4, 4, 3)
+HT_PLAN(64, 8, 8, 8)
+HT_PLAN(96, 24, 8, 4, 3)
+HT_PLAN(128, 8, 8, 4, 4)
+HT_PLAN(192, 24, 8, 8, 3)
+HT_PLAN(256, 8, 8, 8, 4)
+HT_PLAN(384, 24, 8, 8, 3, 2)
+HT_PLAN(512, 8, 8, 8, 8)
+HT_PLAN(768, 24, 8, 8, 4, 3)
+HT_PLAN(1024, 16, 8, 8, 8, 2)
+HT_PLAN(1536, 24, 8, 8, 8, 3)
+HT_PLAN(2048, 16, 8, 8, 8, 4)
+HT_PLAN(3072, 24, 8, 8, 8, 2, 3)
+HT_PLAN(4096, 16, 8, 8, 8, 8)
+#undef HT_PLAN
+
+// ------------------------------------------------------------- one stage
+// tw4: table of exp(-2 pi i m / (4N)); W_N^a = tw4[4a].
+template <int N, int E, int R, int P, bool INV, bool LAST, class SM>
+__device__ __forceinline__ void fft_stage(float2 (&v)[E], const SM& sm, int t,
+                                          const float2* __restrict__ tw4) {
+  constexpr int T = N / E;
+  constexpr int NB = E / R;
+  constexpr int NR = N / R;
+  static_assert(E % R == 0, "radix must divide the samples per thread");
+#pragma unroll
+  for (int s = 0; s < NB; ++s) {
+    const int b = t + s * T;
+#pragma unroll
+    for (int j = 0; j < R; ++j) v[s * R + j] = sm.ld(b + j * NR);
+  }
+#pragma unroll
+  for (int s = 0; s < NB; ++s) {
+    const int b = t + s * T;
+    if constexpr (P > 1) {
+      const int i = b % P;
+#pragma unroll
+      for (int j = 1; j < R; ++j) {
+        float2 w = __ldg(&tw4[4 * (i * j * (N / (P * R)))]);
+        if (INV) w.y = -w.y;
+        v[s * R + j] = cmul(v[s * R + j], w);
+      }
+    }
+    Dft<R, INV>::run(&v[s * R]);
+  }
+  __syncthreads();
+#pragma unroll
+  for (int s = 0; s < NB; ++s) {
+    const int b = t + s * T;
+    const int i = (P > 1) ? (b % P) : 0;
+#pragma unroll
+    for (int j = 0; j < R; ++j) sm.st((b - i) * R + i + j * P, v[s * R + j]);
+  }
+  __syncthreads();
+}
+
+template <int N, int E, int P, bool INV, class SM, int R, int... Rs>
+__device__ __forceinline__ void fft_stages(float2 (&v)[E], const SM& sm, int t,
+                                           const float2* __restrict__ tw4, Radices<R, Rs...>) {
+  constexpr bool LAST = sizeof...(Rs) == 0;
+  fft_stage<N, E, R, P, INV, LAST>(v, sm, t, tw4);
+  if constexpr (!LAST) fft_stages<N, E, P * R, INV>(v, sm, t, tw4, Radices<Rs...>{});
+}
+
+// In-place FFT of the line held in shared memory (natural order in, natural
+// order out).  All T threads of the line must call it; every thread of the
+// block must reach it (it contains __syncthreads).  The caller synchronises
+// before (so the input is complete); the result is complete on return.
+template <int N, bool INV, class SM>
+__device__ __forceinline__ void fft_line(const SM& sm, int t, const float2* __restrict__ tw4) {
+  using PL = Plan<N>;
+  float2 v[PL::E];
+  fft_stages<N, PL::E, 1, INV>(v, sm, t, tw4, typename PL::R{});
+}
+
+}  // namespace ht

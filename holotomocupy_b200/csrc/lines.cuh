@@ -1,0 +1,44 @@
+// Launch helpers shared by the operators: block-shape choices for row and
+// column line transforms, the size dispatch, and dynamic shared memory set-up.
+#pragma once
+#include "fft.cuh"
+
+namespace ht {
+
+// Rows per CTA for a row pass of length N: about 256 threads per CTA.
+template <int N>
+struct RowCfg {
+  static constexpr int T = Plan<N>::T;
+  static constexpr int LINES = (T >= 256) ? 1 : (256 / T);
+  static constexpr int THREADS = LINES * T;
+  static constexpr int SMEM = LINES * SmRow::padded(N) * (int)sizeof(float2);
+};
+
+// Columns per CTA for a column pass of length N (tile N x C in shared memory).
+template <int N>
+struct ColCfg {
+  static constexpr int T = Plan<N>::T;
+  static constexpr int C = (N >= 2048) ? 4 : ((N >= 256) ? 8 : 16);
+  static constexpr int THREADS = C * T;
+  static constexpr int SMEM = N * C * (int)sizeof(float2);
+};
+
+// Set the dynamic shared-memory limit of a kernel once (no-op below 48 KB).
+template <class K>
+inline cudaError_t allow_smem(K kernel, int bytes) {
+  if (bytes <= 48 * 1024) return cudaSuccess;
+  return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+}
+
+// Position of input sample g after the even/odd-reversed reordering used by
+// the DCT-II (v[m] = f[2m], v[N-1-m] = f[2m+1]).
+__device__ __forceinline__ int dct_perm_inv(int g, int N) { return (g & 1) ? (N - 1 - (g >> 1)) : (g >> 1); }
+// Sample of the reordered sequence that lands on output position g.
+__device__ __forceinline__ int dct_perm(int g, int N) { return dct_perm_inv(g, N); }
+
+}  // namespace ht
+
+// Runtime size -> template dispatch over the supported transform lengths.
+#define HT_SIZE_CASES(X) \
+  X(18) X(24) X(32) X(36) X(48) X(64) X(96) X(128) X(192) X(256) X(384) X(512) \
+  X(768) X(1024) X(1536) X(2048) X(3072) X(4096)
