@@ -1,0 +1,370 @@
+#!/usr/bin/env python
+"""Benchmark: Bilinear-Hessian iterations per second for a 512^3 complex
+object, 900 angles, 4 propagation distances and a 512x512 detector (one BH
+iteration = the data-term gradient, the Hessian forms for the step sizes,
+one R and one R^T of the volume, and the variable updates).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+One JSON line on stdout (rank 0).  Under torchrun (N > 1) every rank runs an
+independent reconstruction (the solver does not shard across GPUs: replicas
+only) and `value` is the sum over ranks; time is the max over ranks.
+
+`--impl reference` times the reference algorithm's CPU implementation (the
+NumPy port in oracle/, FP32, all host cores) on a bounded sample of the same
+workload: the per-angle BH cascades (one gradient and three Hessian cascades,
+as rec_mpi.py runs them) for one angle and R + R^T for one slice, scaled to
+900 angles and 512 slices.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "BH iters/s at 512³×900 ang×4 dist (served vs plain); p50/p99 iter latency"
+UNIT = "BH iterations/s"
+DIST = np.array([3e-3, 4e-3, 5e-3, 6e-3])
+WAVELENGTH = 7.3e-11
+VOXEL = 20e-9
+
+
+def workload_args(n, ntheta, ndist, niter=10 ** 6):
+    import types
+    return types.SimpleNamespace(
+        theta=np.linspace(0, np.pi, ntheta, endpoint=False).astype("float32"), ndist=ndist, ntheta=ntheta,
+        nz=n, n=n, nzobj=n, nobj=n, obj_dtype="complex64", mask=0.9, lam_prbfit=0.0, rho=[1, 0.05, 0.02],
+        niter=niter, nchunk=n, vis_step=-1, err_step=-1, start_iter=0, distance=DIST[:ndist],
+        wavelength=WAVELENGTH, voxelsize=VOXEL, norm_magnifications=np.ones(ndist))
+
+
+# ----------------------------------------------------------------- clocks
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = [r.split(",") for r in open(self.path).read().strip().splitlines() if r.strip()]
+        os.unlink(self.path)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            r = [x.strip() for x in r]
+            try:
+                sm.append(float(r[1]))
+                mx = float(r[2])
+            except (ValueError, IndexError):
+                continue
+            for nm, v in zip(names, r[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ----------------------------------------------------------- CPU (oracle)
+def cpu_sample(n, ntheta, ndist, threads):
+    """Seconds per BH iteration of the reference algorithm on the host, from a
+    one-angle cascade sample and a one-slice R/RT sample (scaled)."""
+    os.environ["HOLO_ORACLE_WORKERS"] = str(threads)
+    from oracle import holo_oracle as O
+    O._WORKERS = threads
+    rng = np.random.default_rng(0)
+    a = workload_args(n, 1, ndist)
+    a.theta = a.theta[:1]
+    rec = O.Rec(a, "complex64")
+    rec.eff_demagnifications[:] = 1
+    rec.data[:] = 1.0
+    v = {"prb": np.ones((ndist, n, n), "complex64"), "proj": (0.01 * rng.standard_normal((1, n, n))).astype("complex64"),
+         "pos": rng.uniform(-2, 2, (1, ndist, 2)).astype("float32")}
+    g = {"prb": (0.01 * rng.standard_normal((ndist, n, n))).astype("complex64"),
+         "proj": (0.01 * rng.standard_normal((1, n, n))).astype("complex64"),
+         "pos": rng.uniform(-1, 1, (1, ndist, 2)).astype("float32")}
+    e = {k: x.copy() for k, x in g.items()}
+    tomo = O.Tomo(n, 1, workload_args(n, ntheta, ndist).theta, 0, "complex64")
+    x = (0.01 * rng.standard_normal((1, n, n))).astype("complex64")
+    t0 = time.perf_counter()
+    rec.gradients_cascade(v, g)
+    rec.hessian_cascade(v, g, e)
+    rec.hessian_cascade(v, e, e)
+    rec.hessian_cascade(v, e, e)
+    t1 = time.perf_counter()
+    y = tomo.R(x)
+    tomo.RT(y)
+    t2 = time.perf_counter()
+    per_iter = (t1 - t0) * ntheta + (t2 - t1) * n
+    sample = (f"reference-structure BH cascades (1 gradient + 3 Hessian) for 1 of {ntheta} angles at "
+              f"{n}x{n}x{ndist}, plus R and R^T of 1 of {n} slices, scaled linearly; FP32 NumPy/SciPy oracle")
+    return per_iter, t2 - t0, sample
+
+
+def run_reference(a, rank):
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    n, ntheta, ndist = a.size, a.ntheta, 4
+    for _ in range(a.warmup):
+        cpu_sample(n, ntheta, ndist, threads)
+    per = []
+    for _ in range(a.steps):
+        p, _, sample = cpu_sample(n, ntheta, ndist, threads)
+        per.append(p)
+    ms = float(np.mean(per)) * 1e3
+    value = 1e3 / ms
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup,
+            "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c64",
+            "data": "synthetic", "impl": "reference",
+            "config": {"workload": f"one BH iteration, {n}^3 object, {ntheta} angles, {ndist} distances, {n}^2 detector",
+                       "n": n, "ntheta": ntheta, "ndist": ndist},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------ GPU
+def build_problem(n, ntheta, ndist, seed, device):
+    import torch
+    from holotomocupy_b200 import synthetic
+    from holotomocupy_b200.rec import Rec
+    rec = Rec(workload_args(n, ntheta, ndist))
+    nell = 80 if n >= 512 else 20
+    obj = synthetic.ellipsoid_phantom(n, nell, seed, WAVELENGTH, VOXEL, device=device)
+    prb = synthetic.random_probe(ndist, n, n, seed + 1, device=device)
+    pos = synthetic.random_positions(ntheta, ndist, 2.0, seed + 2, device=device)
+    data = rec.forward_amplitudes(obj, prb, pos)
+    synthetic.noisy_amplitudes(data, 1e4, seed + 3)
+    torch.cuda.synchronize()
+    return rec, obj, prb, pos, data
+
+
+def reset_state(rec, prb0, pos0, data=None):
+    import torch
+    for d in (rec.vars, rec.grads, rec.etas):
+        for v in d.values():
+            v.zero_()
+    for v in rec._c.values():
+        v.zero_()
+    rec.vars["prb"].copy_(prb0)
+    rec.vars["pos"].copy_(pos0)
+    if data is not None:
+        rec.data.copy_(data)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--size", type=int, default=512, help="object/detector size n (the workload is n=512)")
+    ap.add_argument("--ntheta", type=int, default=900)
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--e2e-iters", type=int, default=4)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    a = ap.parse_args()
+    if a.warmup < 3:
+        a.warmup = 3
+
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local = int(os.environ.get("LOCAL_RANK", 0))
+    if a.impl == "reference":
+        run_reference(a, rank)
+        return
+
+    import torch
+    import torch.distributed as dist
+    from holotomocupy_b200 import _lib
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(minutes=10), device_id=device)
+
+    n, ntheta, ndist = a.size, a.ntheta, 4
+    rec, obj_true, prb_true, pos_true, data = build_problem(n, ntheta, ndist, 1234 + rank, device)
+    prb0 = torch.ones_like(prb_true)
+    gen = torch.Generator(device=device).manual_seed(99 + rank)
+    pos0 = pos_true + 0.5 * (2 * torch.rand(pos_true.shape, generator=gen, device=device) - 1)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    # ---- device-resident iterations
+    reset_state(rec, prb0, pos0)
+    rec.bh_setup()
+    it = 0
+    for _ in range(a.warmup):
+        rec.bh_iteration(it)
+        it += 1
+    barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    st = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    lat = []
+    l0 = _lib.lib().ht_launch_count()
+    e0.record(st)
+    for _ in range(a.steps):
+        s0 = torch.cuda.Event(enable_timing=True)
+        s1 = torch.cuda.Event(enable_timing=True)
+        s0.record(st)
+        rec.bh_iteration(it)
+        s1.record(st)
+        lat.append((s0, s1))
+        it += 1
+    e1.record(st)
+    torch.cuda.synchronize()
+    launches = (_lib.lib().ht_launch_count() - l0) / a.steps
+    barrier()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1) / a.steps
+    per_lat = sorted(s.elapsed_time(e) for s, e in lat)
+    if world > 1:
+        t = torch.tensor([ms], device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t)
+    rec.bh_finish()
+    value = world * 1e3 / ms
+
+    # ---- roofline of the dominant kernel family (the propagator passes)
+    roof = roofline(rec, device)
+
+    # ---- end to end through the public API with pinned host buffers
+    e2e = end_to_end(a, rec, obj_true, prb0, pos0, data, device, barrier, world)
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
+        "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c64",
+        "data": "synthetic (seeded ellipsoid phantom, random probe and positions, Poisson noise at 1e4 photons)",
+        "config": {"workload": f"one BH iteration, {n}^3 object, {ntheta} angles, {ndist} distances, {n}^2 detector",
+                   "n": n, "ntheta": ntheta, "ndist": ndist, "parallelism": f"replicas x{world}",
+                   "l2": "inputs larger than L2 (state ~50 GB)", "latency_ms_p50": float(np.percentile(per_lat, 50)),
+                   "latency_ms_p99": float(np.percentile(per_lat, 99))},
+        "gpu_launches": launches,
+        "roofline": roof,
+        "e2e": e2e,
+        "clocks": clk,
+    }
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        per_iter, wall, sample = cpu_sample(n, ntheta, ndist, os.cpu_count() or 1)
+        line["cpu_baseline"] = {"value": 1.0 / per_iter, "unit": UNIT, "cores": os.cpu_count() or 1, "kind": "port",
+                                "sample": sample, "sample_seconds": wall}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def roofline(rec, device):
+    """Time the propagator D over every (angle, distance) image of the
+    workload with CUDA events and report algorithmic bytes / time against the
+    measured HBM copy bandwidth."""
+    import torch
+    from holotomocupy_b200 import _lib
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    peak = float(peaks.get("hbm_gbs", 6650.0))
+    nimg = rec.ntheta * rec.ndist
+    x = torch.empty(nimg, rec.nz, rec.n, dtype=torch.complex64, device=device)
+    x.normal_()
+    y = torch.empty_like(x)
+    st = _lib.stream_ptr()
+    for _ in range(2):
+        _lib.call("ht_prop_D", rec.cl_prop._h, _lib.ptr(x), _lib.ptr(y), nimg, 0, st)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    reps = 5
+    e0.record()
+    for _ in range(reps):
+        _lib.call("ht_prop_D", rec.cl_prop._h, _lib.ptr(x), _lib.ptr(y), nimg, 0, st)
+    e1.record()
+    torch.cuda.synchronize()
+    t = e0.elapsed_time(e1) / reps * 1e-3
+    alg = 16.0 * nimg * rec.nz * rec.n + 32.0 * rec.nz * rec.n
+    achieved = alg / t / 1e9
+    del x, y
+    return {"bound": "hbm", "kernel": "propagator D (row DCT-II, column DCT/table/DCT, row DCT-III) over all images",
+            "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+            "peak_source": "measured" if peaks else "fallback", "launch_ms": t * 1e3}
+
+
+def end_to_end(a, rec, obj_true, prb0, pos0, data, device, barrier, world):
+    """Each step: upload data and the initial state from pinned host memory,
+    run e2e-iters BH iterations through Rec.BH, download obj, prb and pos."""
+    import torch
+    h_data = data.cpu().pin_memory()
+    h_prb = prb0.cpu().pin_memory()
+    h_pos = pos0.cpu().pin_memory()
+    h_obj = torch.zeros(rec.nzobj, rec.nobj, rec.nobj, dtype=torch.complex64).pin_memory()
+    out_obj = torch.empty_like(h_obj).pin_memory()
+    out_prb = torch.empty_like(h_prb).pin_memory()
+    out_pos = torch.empty_like(h_pos).pin_memory()
+    h2d = sum(t.numel() * t.element_size() for t in (h_data, h_prb, h_pos, h_obj))
+    d2h = sum(t.numel() * t.element_size() for t in (out_obj, out_prb, out_pos))
+    times = []
+    for s in range(a.e2e_steps + 1):
+        barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for d in (rec.grads, rec.etas):
+            for v in d.values():
+                v.zero_()
+        rec.data.copy_(h_data, non_blocking=True)
+        rec.vars["obj"].copy_(h_obj, non_blocking=True)
+        rec.vars["prb"].copy_(h_prb, non_blocking=True)
+        rec.vars["pos"].copy_(h_pos, non_blocking=True)
+        rec.BH(niter=a.e2e_iters)
+        out_obj.copy_(rec.vars["obj"], non_blocking=True)
+        out_prb.copy_(rec.vars["prb"], non_blocking=True)
+        out_pos.copy_(rec.vars["pos"], non_blocking=True)
+        e1.record()
+        torch.cuda.synchronize()
+        if s > 0:
+            times.append(e0.elapsed_time(e1))
+    ms = float(np.mean(times))
+    return {"value": world * a.e2e_iters * 1e3 / ms, "unit": UNIT, "h2d_bytes_per_step": h2d,
+            "d2h_bytes_per_step": d2h, "iterations_per_step": a.e2e_iters, "ms_per_step": ms,
+            "step": "upload data + initial obj/prb/pos from pinned host memory, Rec.BH with the iterations, "
+                    "download obj/prb/pos"}
+
+
+if __name__ == "__main__":
+    main()

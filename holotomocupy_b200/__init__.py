@@ -6,5 +6,8 @@ of CuPy arrays): ``Propagation`` (Fresnel D/DT), ``Tomo`` (USFFT R/RT),
 All compute runs in ``lib/libholotomo_b200.so`` (sm_100a).
 """
 from .propagation import Propagation, fresnel_table  # noqa: F401
+from .shift import Shift  # noqa: F401
+from .tomo import Tomo  # noqa: F401
+from .rec import Rec  # noqa: F401
 
 __version__ = "0.1.0"

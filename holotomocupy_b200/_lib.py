@@ -18,12 +18,33 @@ _c_float, _c_double = ctypes.c_float, ctypes.c_double
 SIGNATURES = {
     "ht_version": [],
     "ht_last_error": [],
+    "ht_launch_count": [],
     "ht_prop_create": [_c_int, _c_int, _c_int, _vp, ctypes.POINTER(_vp)],
     "ht_prop_destroy": [_vp],
     "ht_prop_D": [_vp, _vp, _vp, _c_long, _c_int, _vp],
     "ht_prop_DT": [_vp, _vp, _vp, _c_long, _c_int, _vp],
+    "ht_tomo_create": [_c_int, _c_int, _c_int, _vp, _vp, ctypes.POINTER(_vp)],
+    "ht_tomo_destroy": [_vp],
+    "ht_tomo_R": [_vp, _vp, _vp, _c_int, _vp],
+    "ht_tomo_RT": [_vp, _vp, _vp, _c_int, _vp],
+    "ht_shift_create": [_c_int, _c_int, _c_int, _c_int, _c_int, ctypes.POINTER(_vp)],
+    "ht_shift_destroy": [_vp],
+    "ht_shift_coeff": [_vp, _vp, _vp, _c_long, _vp],
+    "ht_shift_S": [_vp, _vp, _vp, _vp, _vp, _c_long, _vp],
+    "ht_shift_Sadj": [_vp, _vp, _vp, _vp, _vp, _c_long, _vp],
+    "ht_shift_dS": [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _c_long, _vp],
+    "ht_shift_d2S": [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _c_long, _vp],
+    "ht_shift_dSadj": [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _c_long, _vp],
+    "ht_filter_rows": [_c_int, _vp, _vp, _c_long, _vp, _vp],
+    "ht_axpby": [_vp, _vp, _c_float, _c_float, _c_long, _vp, _vp],
+    "ht_dot": [_vp, _vp, _c_long, _vp, _vp],
+    "ht_rec_create": [_c_int, _c_int, _c_int, _c_int, _c_int, _c_int, _c_int, _vp, ctypes.POINTER(_vp)],
+    "ht_rec_destroy": [_vp],
+    "ht_rec_forward": [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
+    "ht_rec_gradient": [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
+    "ht_rec_hessian": [_vp, _vp, _vp, _vp, _vp, _vp, _c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
 }
-_RESTYPE = {"ht_last_error": ctypes.c_char_p}
+_RESTYPE = {"ht_last_error": ctypes.c_char_p, "ht_launch_count": ctypes.c_long}
 
 _lib = None
 

@@ -5,3 +5,5 @@
 extern "C" int ht_version(void) { return 100; }
 
 extern "C" const char* ht_last_error(void) { return ht::last_error(); }
+
+extern "C" long ht_launch_count(void) { return ht::launch_count(); }

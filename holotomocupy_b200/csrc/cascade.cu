@@ -1,0 +1,834 @@
+// Fused data-fidelity cascade of the Bilinear-Hessian solver
+// (reference: src/holotomocupy/rec_mpi.py:250-353, 517-813).
+//
+// Forward model per angle theta and distance k (image img = theta*ndist + k):
+//   x22 = S_{pos,mag}(c)            c = coeff(proj[theta]) (the B-spline
+//                                   coefficients, cached by the caller)
+//   x12 = exp(i x22),  x0 = D_k(prb[k] x12),  F = 1/N sum (|x0| - d)^2
+// Gradient (rec_mpi.py:562-813): g0 = 2/N (x0 - d x0/|x0|), G = D_k^H g0,
+//   P = G conj(x12) (cached), Y22 = -i conj(prb[k]) P (the gradient at x22),
+//   grad prb[k] = sum_theta P, grad c[theta] = sum_k S_k^T Y22, and the
+//   position gradient (-Ay, -Ax) with Ax = sum Re<Y22, (dS/dx) c>,
+//   Ay = sum Re<Y22, (dS/dy) c>.
+// Hessian form (rec_mpi.py:250-303).  With the cascade's second-order terms
+// moved onto the gradient quantities, for directions y, z:
+//   H(y, z) = 2/N sum [(1 - d/|x0|) Re(y0 conj z0) + d/|x0| Re(l0* y0) Re(l0* z0)]
+//           + sum Re(conj(P) i (y_prb z22 + z_prb y22))       (second order of F1)
+//           - sum Re(conj(P) prb y22 z22)                      (second order of F2)
+//           + sum Re<Y22, d2S(c; c_y, r_y; c_z, r_z)>          (second order of F3)
+// where y22 = dS(c, c_y, r_y), y0 = D_k(x12 (y_prb + i prb y22)), l0 = x0/|x0|.
+// The F3 term is a bilinear form in the position directions with per-image
+// coefficients Hxx, Hxy, Hyy (from c) and Ax, Ay of the direction's
+// coefficients; the reference's d2s pairs c_y with r_y and c_z with r_z
+// (exact when y = z), which ht_rec_hessian reports as H_ref(y, z) beside the
+// symmetric H_sym(y, z) (c_y with r_z).  One Hessian pass over both
+// directions costs two propagations per image; the reference's three
+// cascades cost ten.
+//
+// Row kernels handle one detector row of one image per line, with the
+// propagator's DCT passes fused in; the column passes are the propagator's.
+#include "dct.cuh"
+#include "holotomo_b200_internal.h"
+
+#include <vector>
+
+namespace ht {
+
+// -------------------------------------------------------------- basics
+__device__ __forceinline__ float bsp0(float t) {
+  if (-2.0f < t && t <= -1.0f) return (t + 2.0f) * (t + 2.0f) * (t + 2.0f);
+  if (-1.0f < t && t <= 1.0f) return 4.0f - 6.0f * t * t + 3.0f * fabsf(t) * t * t;
+  if (1.0f < t && t <= 2.0f) return (2.0f - t) * (2.0f - t) * (2.0f - t);
+  return 0.0f;
+}
+__device__ __forceinline__ float bsp1(float t) {
+  if (-2.0f < t && t <= -1.0f) return 3.0f * (t + 2.0f) * (t + 2.0f);
+  if (-1.0f < t && t <= 1.0f) return -12.0f * t + 9.0f * fabsf(t) * t;
+  if (1.0f < t && t <= 2.0f) return -3.0f * (2.0f - t) * (2.0f - t);
+  return 0.0f;
+}
+__device__ __forceinline__ float bsp2(float t) {
+  if (-2.0f < t && t <= -1.0f) return 6.0f * (t + 2.0f);
+  if (-1.0f < t && t <= 1.0f) return -12.0f + 18.0f * fabsf(t);
+  if (1.0f < t && t <= 2.0f) return 6.0f * (2.0f - t);
+  return 0.0f;
+}
+
+// Object-side element: complex (complex64 objects) or real (float32 objects)
+template <class T>
+struct El;
+template <>
+struct El<float2> {
+  static __device__ __forceinline__ float2 zero() { return make_float2(0.f, 0.f); }
+  static __device__ __forceinline__ void fma(float2& a, float w, float2 v) {
+    a.x += w * v.x;
+    a.y += w * v.y;
+  }
+  static __device__ __forceinline__ float2 cplx(float2 v) { return v; }
+  // projection of a complex gradient onto the element space
+  static __device__ __forceinline__ float2 proj(float2 g) { return g; }
+  static __device__ __forceinline__ float redot(float2 a, float2 b) { return a.x * b.x + a.y * b.y; }
+};
+template <>
+struct El<float> {
+  static __device__ __forceinline__ float zero() { return 0.f; }
+  static __device__ __forceinline__ void fma(float& a, float w, float v) { a += w * v; }
+  static __device__ __forceinline__ float2 cplx(float v) { return make_float2(v, 0.f); }
+  static __device__ __forceinline__ float proj(float2 g) { return g.x; }
+  static __device__ __forceinline__ float redot(float a, float b) { return a * b; }
+};
+
+// exp(i z) for complex z = a + ib: exp(-b) (cos a + i sin a)
+__device__ __forceinline__ float2 cexp_i(float2 z) {
+  float s, c;
+  sincosf(z.x, &s, &c);
+  const float e = expf(-z.y);
+  return make_float2(e * c, e * s);
+}
+
+struct CascDims {
+  int n, nz, nobj, nzobj, ndist;
+  long nimg;  // ntheta * ndist
+};
+
+// Stencil weights at one detector pixel (cuda_kernels.py:177-190).
+struct Taps {
+  int ix, iy;
+  float px[4], py[4], dpx[4], dpy[4], d2px[4], d2py[4];
+};
+
+template <int ORDER>
+__device__ __forceinline__ void taps(const CascDims& D, float mag, float2 r /* (y, x) */, int tx, int ty, Taps& w) {
+  const float half = (mag - 1.0f) / 2.0f;
+  const float x = (mag * (float)(tx - D.n / 2) - r.y + half) + (float)(D.nobj / 2);
+  const float y = (mag * (float)(ty - D.nz / 2) - r.x + half) + (float)(D.nzobj / 2);
+  w.ix = (int)floorf(x);
+  w.iy = (int)floorf(y);
+  const float dx = x - (float)w.ix, dy = y - (float)w.iy;
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const float ux = dx - (float)(j - 1), uy = dy - (float)(j - 1);
+    w.px[j] = bsp0(ux);
+    w.py[j] = bsp0(uy);
+    if (ORDER >= 1) {
+      w.dpx[j] = bsp1(ux);
+      w.dpy[j] = bsp1(uy);
+    }
+    if (ORDER >= 2) {
+      w.d2px[j] = bsp2(ux);
+      w.d2py[j] = bsp2(uy);
+    }
+  }
+}
+
+// sum over the 4x4 taps of weight(jy, jx) * c[...], zero outside
+#define HT_TAP_LOOP(D, w, cbase, BODY)                                  \
+  _Pragma("unroll") for (int jy = 0; jy < 4; ++jy) {                    \
+    const int yy = w.iy + jy - 1;                                       \
+    if (yy < 0 || yy >= D.nzobj) continue;                              \
+    _Pragma("unroll") for (int jx = 0; jx < 4; ++jx) {                  \
+      const int xx = w.ix + jx - 1;                                     \
+      if (xx < 0 || xx >= D.nobj) continue;                             \
+      const long ci = (long)yy * D.nobj + xx;                           \
+      BODY                                                              \
+    }                                                                   \
+  }
+
+__device__ __forceinline__ float2 ld_pos(const float* pos, long img) {
+  return make_float2(pos[2 * img + 0], pos[2 * img + 1]);
+}
+
+// Per-image accumulator slots
+enum Acc : int { kAx = 0, kAy, kHxx, kHxy, kHyy, kAyx, kAyy, kAzx, kAzy, kNAcc };
+// Global accumulator slots
+enum Glob : int { kF = 0, kQ0, kQ1, kQ2, kL10, kL11, kL12, kL20, kL21, kL22, kNGlob };
+
+// ================================================= forward row pass
+// u = prb[k] exp(i S(c)) -> row DCT-II -> tmp
+template <int N, class T>
+__global__ void __launch_bounds__(RowCfg<N>::THREADS)
+k_casc_fwd(const T* __restrict__ c, const float* __restrict__ pos, const float* __restrict__ mag,
+           const float2* __restrict__ prb, float2* __restrict__ tmp, CascDims D, const float2* __restrict__ tw4) {
+  constexpr int TT = RowCfg<N>::T;
+  extern __shared__ float2 smem[];
+  const int line = threadIdx.x / TT, t = threadIdx.x % TT;
+  const long row = (long)blockIdx.x * RowCfg<N>::LINES + line;  // img * nz + ty
+  const bool valid = row < D.nimg * D.nz;
+  const long img = valid ? row / D.nz : 0;
+  const int ty = valid ? (int)(row % D.nz) : 0;
+  const int k = (int)(img % D.ndist);
+  const long th = img / D.ndist;
+  SmRow sm{smem + line * SmRow::padded(N)};
+  const T* cb = c + th * (long)D.nzobj * D.nobj;
+  const float m0 = valid ? mag[img] : 1.f;
+  const float2 r = valid ? ld_pos(pos, img) : make_float2(0.f, 0.f);
+  for (int tx = t; tx < N; tx += TT) {
+    float2 u = make_float2(0.f, 0.f);
+    if (valid) {
+      Taps w;
+      taps<0>(D, m0, r, tx, ty, w);
+      T x22 = El<T>::zero();
+      HT_TAP_LOOP(D, w, cb, El<T>::fma(x22, w.px[jx] * w.py[jy], __ldg(&cb[ci]));)
+      u = cmul(prb[((long)k * D.nz + ty) * N + tx], cexp_i(El<T>::cplx(x22)));
+    }
+    dct2_put<N>(sm, tx, u);
+  }
+  __syncthreads();
+  dct2_finish<N, TT>(sm, t, tw4, tmp + row * N, valid);
+}
+
+// ======================================== residual row pass
+// tmp holds the column-processed spectrum of u.  MODE 0: x0 -> cache,
+// F, g0 -> DCT-II -> tmp.  MODE 1: F only.  MODE 2: out = |x0| (float).
+template <int N, int MODE>
+__global__ void __launch_bounds__(RowCfg<N>::THREADS)
+k_casc_resid(float2* __restrict__ tmp, float2* __restrict__ x0c, const float* __restrict__ data,
+             float* __restrict__ amp, double* __restrict__ glob, float scale, CascDims D,
+             const float2* __restrict__ tw4) {
+  constexpr int TT = RowCfg<N>::T;
+  constexpr int E = Plan<N>::E;
+  extern __shared__ float2 smem[];
+  double* red = reinterpret_cast<double*>(smem + RowCfg<N>::LINES * SmRow::padded(N));
+  const int line = threadIdx.x / TT, t = threadIdx.x % TT;
+  const long row = (long)blockIdx.x * RowCfg<N>::LINES + line;
+  const bool valid = row < D.nimg * D.nz;
+  SmRow sm{smem + line * SmRow::padded(N)};
+  dct3_start<N, TT>(sm, t, tw4, tmp + row * N, valid);
+  float2 g0[E];
+  double acc[1] = {0.0};
+  float facc = 0.f;
+#pragma unroll
+  for (int i = 0; i < E; ++i) {
+    const int tx = t + i * TT;
+    g0[i] = make_float2(0.f, 0.f);
+    if (valid) {
+      const float2 x0 = sm.ld(dct_perm(tx, N));
+      const float a = sqrtf(x0.x * x0.x + x0.y * x0.y);
+      if (MODE == 2) {
+        amp[row * N + tx] = a;
+      } else {
+        const float d = data[row * N + tx];
+        const float e = a - d;
+        facc += e * e;
+        if (MODE == 0) {
+          x0c[row * N + tx] = x0;
+          // rec_mpi.py:557-559: scale * (x - y * (x / |x|))
+          const float2 l = make_float2(x0.x / a, x0.y / a);
+          g0[i] = make_float2(scale * (x0.x - d * l.x), scale * (x0.y - d * l.y));
+        }
+      }
+    }
+  }
+  if (MODE != 2) {
+    acc[0] = facc;
+    line_sums<TT, 1>(acc, red, line, t);
+    if (t == 0 && valid) atomicAdd(&glob[kF], acc[0]);
+  }
+  if (MODE != 0) return;
+  __syncthreads();
+#pragma unroll
+  for (int i = 0; i < E; ++i) dct2_put<N>(sm, t + i * TT, g0[i]);
+  __syncthreads();
+  dct2_finish<N, TT>(sm, t, tw4, tmp + row * N, valid);
+}
+
+// ============================================== adjoint row pass
+// tmp holds the column-processed spectrum of g0.  G = DCT-III; recompute
+// x12; P = G conj(x12) -> cache; Y22 = -i conj(prb) P; per-image sums
+// Ax, Ay, Hxx, Hxy, Hyy.
+template <int N, class T>
+__global__ void __launch_bounds__(RowCfg<N>::THREADS)
+k_casc_adj(const float2* __restrict__ tmp, float2* __restrict__ Pc, const T* __restrict__ c,
+           const float* __restrict__ pos, const float* __restrict__ mag, const float2* __restrict__ prb,
+           double* __restrict__ acc_img, CascDims D, const float2* __restrict__ tw4) {
+  constexpr int TT = RowCfg<N>::T;
+  extern __shared__ float2 smem[];
+  double* red = reinterpret_cast<double*>(smem + RowCfg<N>::LINES * SmRow::padded(N));
+  const int line = threadIdx.x / TT, t = threadIdx.x % TT;
+  const long row = (long)blockIdx.x * RowCfg<N>::LINES + line;
+  const bool valid = row < D.nimg * D.nz;
+  const long img = valid ? row / D.nz : 0;
+  const int ty = valid ? (int)(row % D.nz) : 0;
+  const int k = (int)(img % D.ndist);
+  const long th = img / D.ndist;
+  SmRow sm{smem + line * SmRow::padded(N)};
+  dct3_start<N, TT>(sm, t, tw4, tmp + row * N, valid);
+  const T* cb = c + th * (long)D.nzobj * D.nobj;
+  const float m0 = valid ? mag[img] : 1.f;
+  const float2 r = valid ? ld_pos(pos, img) : make_float2(0.f, 0.f);
+  float s[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
+  for (int tx = t; tx < N; tx += TT) {
+    if (!valid) break;
+    const float2 G = sm.ld(dct_perm(tx, N));
+    Taps w;
+    taps<2>(D, m0, r, tx, ty, w);
+    T x22 = El<T>::zero(), ax = El<T>::zero(), ay = El<T>::zero(), hxx = El<T>::zero(), hxy = El<T>::zero(),
+      hyy = El<T>::zero();
+    HT_TAP_LOOP(D, w, cb, {
+      const T cv = __ldg(&cb[ci]);
+      El<T>::fma(x22, w.px[jx] * w.py[jy], cv);
+      El<T>::fma(ax, w.dpx[jx] * w.py[jy], cv);
+      El<T>::fma(ay, w.px[jx] * w.dpy[jy], cv);
+      El<T>::fma(hxx, w.d2px[jx] * w.py[jy], cv);
+      El<T>::fma(hxy, w.dpx[jx] * w.dpy[jy], cv);
+      El<T>::fma(hyy, w.px[jx] * w.d2py[jy], cv);
+    })
+    const float2 x12 = cexp_i(El<T>::cplx(x22));
+    const float2 P = cmulc(G, x12);
+    Pc[row * N + tx] = P;
+    const float2 pr = prb[((long)k * D.nz + ty) * N + tx];
+    // Y22 = -i conj(pr) P  (rec_mpi.py:706-707, .real for float32 objects)
+    const T Y = El<T>::proj(rot<false>(cmulc(P, pr)));
+    s[0] += El<T>::redot(Y, ax);
+    s[1] += El<T>::redot(Y, ay);
+    s[2] += El<T>::redot(Y, hxx);
+    s[3] += El<T>::redot(Y, hxy);
+    s[4] += El<T>::redot(Y, hyy);
+  }
+  double v[5];
+#pragma unroll
+  for (int i = 0; i < 5; ++i) v[i] = s[i];
+  line_sums<TT, 5>(v, red, line, t);
+  if (t == 0 && valid) {
+#pragma unroll
+    for (int i = 0; i < 5; ++i) atomicAdd(&acc_img[img * kNAcc + kAx + i], v[i]);
+  }
+}
+
+// ================================================= probe gradient
+// gprb[k, p] = sum_theta P[theta, k, p]  (gF1, rec_mpi.py:641)
+__global__ void k_sum_theta(const float2* __restrict__ Pc, float2* __restrict__ gprb, long ntheta, int ndist,
+                            long npix) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;  // k * npix + p
+  if (i >= (long)ndist * npix) return;
+  const int k = (int)(i / npix);
+  const long p = i % npix;
+  double sx = 0.0, sy = 0.0;
+  for (long th = 0; th < ntheta; ++th) {
+    const float2 v = Pc[(th * ndist + k) * npix + p];
+    sx += v.x;
+    sy += v.y;
+  }
+  gprb[i] = make_float2((float)sx, (float)sy);
+}
+
+// ================================================= object gradient
+// gc[theta, iy, ix] = sum_k S_k^T(Y22[theta, k]) (gF3, rec_mpi.py:802-808),
+// gathered from the detector pixels whose 4x4 footprint holds (iy, ix).
+__device__ __forceinline__ void cand(float m0, float C0, int i, int nhalf, int nmax, int& lo, int& hi) {
+  if (!(fabsf(m0) > 1e-3f)) {
+    lo = 0;
+    hi = nmax - 1;
+    return;
+  }
+  const float a = ((float)(i - 2) - C0) / m0 + (float)nhalf;
+  const float b = ((float)(i + 2) - C0) / m0 + (float)nhalf;
+  const float l = fminf(fmaxf(fminf(a, b), -1e7f), 1e7f);
+  const float h = fminf(fmaxf(fmaxf(a, b), -1e7f), 1e7f);
+  lo = max(0, (int)floorf(l) - 1);
+  hi = min(nmax - 1, (int)ceilf(h) + 1);
+}
+
+template <class T>
+__global__ void __launch_bounds__(256)
+k_casc_sadj(T* __restrict__ gc, const float2* __restrict__ Pc, const float2* __restrict__ prb,
+            const float* __restrict__ pos, const float* __restrict__ mag, CascDims D) {
+  const int ix = blockIdx.x * blockDim.x + threadIdx.x;
+  const int iy = blockIdx.y * blockDim.y + threadIdx.y;
+  const long th = blockIdx.z;
+  if (ix >= D.nobj || iy >= D.nzobj) return;
+  T acc = El<T>::zero();
+  for (int k = 0; k < D.ndist; ++k) {
+    const long img = th * D.ndist + k;
+    const float m0 = mag[img];
+    const float ry = pos[2 * img + 0], rx = pos[2 * img + 1];
+    const float half = (m0 - 1.0f) / 2.0f;
+    int tx0, tx1, ty0, ty1;
+    cand(m0, -rx + half + (float)(D.nobj / 2), ix, D.n / 2, D.n, tx0, tx1);
+    cand(m0, -ry + half + (float)(D.nzobj / 2), iy, D.nz / 2, D.nz, ty0, ty1);
+    const float2* Pi = Pc + img * (long)D.nz * D.n;
+    const float2* pk = prb + (long)k * D.nz * D.n;
+    for (int ty = ty0; ty <= ty1; ++ty) {
+      const float y = (m0 * (float)(ty - D.nz / 2) - ry + half) + (float)(D.nzobj / 2);
+      const int jy = iy - (int)floorf(y);
+      if (jy < -1 || jy > 2) continue;
+      const float wy = bsp0(y - floorf(y) - (float)jy);
+      T racc = El<T>::zero();
+      for (int tx = tx0; tx <= tx1; ++tx) {
+        const float x = (m0 * (float)(tx - D.n / 2) - rx + half) + (float)(D.nobj / 2);
+        const int jx = ix - (int)floorf(x);
+        if (jx < -1 || jx > 2) continue;
+        const long p = (long)ty * D.n + tx;
+        const T Y = El<T>::proj(rot<false>(cmulc(__ldg(&Pi[p]), __ldg(&pk[p]))));
+        El<T>::fma(racc, bsp0(x - floorf(x) - (float)jx), Y);
+      }
+      El<T>::fma(acc, wy, racc);
+    }
+  }
+  gc[(th * D.nzobj + iy) * D.nobj + ix] = acc;
+}
+
+// gpos[img] = (-Ay, -Ax)  (dsadj, cuda_kernels.py:744-761 with redot)
+__global__ void k_casc_gpos(const double* __restrict__ acc_img, float* __restrict__ gpos, long nimg) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nimg) return;
+  gpos[2 * i + 0] = (float)(-acc_img[i * kNAcc + kAy]);
+  gpos[2 * i + 1] = (float)(-acc_img[i * kNAcc + kAx]);
+}
+
+// ================================================ Hessian row pass
+// For NDIR directions d: y22_d = dS(c, c_d, r_d);  v_d = x12 (prb_d + i prb y22_d)
+// -> row DCT-II -> tmp[d];  plus the pointwise second-order sums L1, L2
+// (pairs 00, 01, 11) and the per-image Ax(c_d), Ay(c_d).
+template <int N, class T, int NDIR>
+__global__ void __launch_bounds__(RowCfg<N>::THREADS)
+k_casc_hess_fwd(const T* __restrict__ c, const float* __restrict__ pos, const float* __restrict__ mag,
+                const float2* __restrict__ prb, const float2* __restrict__ Pc, const T* __restrict__ c0,
+                const float* __restrict__ pos0, const float2* __restrict__ prb0, const T* __restrict__ c1,
+                const float* __restrict__ pos1, const float2* __restrict__ prb1, float2* __restrict__ tmp,
+                double* __restrict__ acc_img, double* __restrict__ glob, CascDims D,
+                const float2* __restrict__ tw4) {
+  constexpr int TT = RowCfg<N>::T;
+  constexpr int LINES = RowCfg<N>::LINES;
+  extern __shared__ float2 smem[];
+  double* red = reinterpret_cast<double*>(smem + NDIR * LINES * SmRow::padded(N));
+  const int line = threadIdx.x / TT, t = threadIdx.x % TT;
+  const long row = (long)blockIdx.x * LINES + line;
+  const bool valid = row < D.nimg * D.nz;
+  const long img = valid ? row / D.nz : 0;
+  const int ty = valid ? (int)(row % D.nz) : 0;
+  const int k = (int)(img % D.ndist);
+  const long th = img / D.ndist;
+  SmRow sm0{smem + line * SmRow::padded(N)};
+  SmRow sm1{smem + (LINES + line) * SmRow::padded(N)};
+  const long coff = th * (long)D.nzobj * D.nobj;
+  const T* cb = c + coff;
+  const float m0 = valid ? mag[img] : 1.f;
+  const float2 r = valid ? ld_pos(pos, img) : make_float2(0.f, 0.f);
+  const float2 rd0 = valid ? ld_pos(pos0, img) : make_float2(0.f, 0.f);
+  const float2 rd1 = (valid && NDIR == 2) ? ld_pos(pos1, img) : make_float2(0.f, 0.f);
+  // sums: L1 00,01,11 ; L2 00,01,11 ; A: ax0, ay0, ax1, ay1
+  float s[10] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+  for (int tx = t; tx < N; tx += TT) {
+    float2 v0 = make_float2(0.f, 0.f), v1 = make_float2(0.f, 0.f);
+    if (valid) {
+      Taps w;
+      taps<1>(D, m0, r, tx, ty, w);
+      T x22 = El<T>::zero(), dxc = El<T>::zero(), dyc = El<T>::zero();
+      T s0 = El<T>::zero(), ax0 = El<T>::zero(), ay0 = El<T>::zero();
+      T s1 = El<T>::zero(), ax1 = El<T>::zero(), ay1 = El<T>::zero();
+      const T* cb0 = c0 + coff;
+      const T* cb1 = (NDIR == 2) ? c1 + coff : c0 + coff;
+      HT_TAP_LOOP(D, w, cb, {
+        const float pp = w.px[jx] * w.py[jy];
+        const float dxw = w.dpx[jx] * w.py[jy];
+        const float dyw = w.px[jx] * w.dpy[jy];
+        const T cv = __ldg(&cb[ci]);
+        El<T>::fma(x22, pp, cv);
+        El<T>::fma(dxc, dxw, cv);
+        El<T>::fma(dyc, dyw, cv);
+        const T a0 = __ldg(&cb0[ci]);
+        El<T>::fma(s0, pp, a0);
+        El<T>::fma(ax0, dxw, a0);
+        El<T>::fma(ay0, dyw, a0);
+        if (NDIR == 2) {
+          const T a1 = __ldg(&cb1[ci]);
+          El<T>::fma(s1, pp, a1);
+          El<T>::fma(ax1, dxw, a1);
+          El<T>::fma(ay1, dyw, a1);
+        }
+      })
+      // dS (rec_mpi.py:757; cuda_kernels.py:600-609): sum phi phi c_d - (dphi_x phi_y r_dx + phi_x dphi_y r_dy) c
+      T y0 = s0, y1 = s1;
+      El<T>::fma(y0, -rd0.y, dxc);
+      El<T>::fma(y0, -rd0.x, dyc);
+      if (NDIR == 2) {
+        El<T>::fma(y1, -rd1.y, dxc);
+        El<T>::fma(y1, -rd1.x, dyc);
+      }
+      const float2 x12 = cexp_i(El<T>::cplx(x22));
+      const long p = ((long)k * D.nz + ty) * N + tx;
+      const float2 pr = prb[p];
+      const float2 P = Pc[row * N + tx];
+      const T Y = El<T>::proj(rot<false>(cmulc(P, pr)));
+      const float2 Y0 = El<T>::cplx(y0), Y1 = El<T>::cplx(y1);
+      const float2 q0 = prb0[p];
+      const float2 q1 = (NDIR == 2) ? prb1[p] : make_float2(0.f, 0.f);
+      // v_d = x12 (prb_d + i prb y22_d)   (dF2 then dF1, rec_mpi.py:591, 664)
+      v0 = cmul(x12, cadd(q0, cmul_i(cmul(pr, Y0))));
+      if (NDIR == 2) v1 = cmul(x12, cadd(q1, cmul_i(cmul(pr, Y1))));
+      // L1(a,b) = Re(conj(P) i (q_a y22_b + q_b y22_a));  L2(a,b) = -Re(conj(P) prb y22_a y22_b)
+      const float2 cP = cconj(P);
+      s[0] += cmul(cP, cmul_i(cscale(cmul(q0, Y0), 2.f))).x;
+      s[3] += -cmul(cP, cmul(pr, cmul(Y0, Y0))).x;
+      s[6] += El<T>::redot(Y, ax0);
+      s[7] += El<T>::redot(Y, ay0);
+      if (NDIR == 2) {
+        s[1] += cmul(cP, cmul_i(cadd(cmul(q0, Y1), cmul(q1, Y0)))).x;
+        s[2] += cmul(cP, cmul_i(cscale(cmul(q1, Y1), 2.f))).x;
+        s[4] += -cmul(cP, cmul(pr, cmul(Y0, Y1))).x;
+        s[5] += -cmul(cP, cmul(pr, cmul(Y1, Y1))).x;
+        s[8] += El<T>::redot(Y, ax1);
+        s[9] += El<T>::redot(Y, ay1);
+      }
+    }
+    dct2_put<N>(sm0, tx, v0);
+    if (NDIR == 2) dct2_put<N>(sm1, tx, v1);
+  }
+  double v[10];
+#pragma unroll
+  for (int i = 0; i < 10; ++i) v[i] = s[i];
+  line_sums<TT, 10>(v, red, line, t);
+  if (t == 0 && valid) {
+    atomicAdd(&glob[kL10], v[0]);
+    atomicAdd(&glob[kL20], v[3]);
+    atomicAdd(&acc_img[img * kNAcc + kAyx], v[6]);
+    atomicAdd(&acc_img[img * kNAcc + kAyy], v[7]);
+    if (NDIR == 2) {
+      atomicAdd(&glob[kL11], v[1]);
+      atomicAdd(&glob[kL12], v[2]);
+      atomicAdd(&glob[kL21], v[4]);
+      atomicAdd(&glob[kL22], v[5]);
+      atomicAdd(&acc_img[img * kNAcc + kAzx], v[8]);
+      atomicAdd(&acc_img[img * kNAcc + kAzy], v[9]);
+    }
+  }
+  __syncthreads();
+  const long nrow = D.nimg * D.nz;
+  dct2_finish<N, TT>(sm0, t, tw4, tmp + row * N, valid);
+  if (NDIR == 2) dct2_finish<N, TT>(sm1, t, tw4, tmp + (nrow + row) * N, valid);
+}
+
+// ======================================== Hessian quadratic terms
+// y0_d = DCT-III rows of tmp[d];  Q pairs with x0 and the data.
+template <int N, int NDIR>
+__global__ void __launch_bounds__(RowCfg<N>::THREADS)
+k_casc_hess_q(const float2* __restrict__ tmp, const float2* __restrict__ x0c, const float* __restrict__ data,
+              double* __restrict__ glob, CascDims D, const float2* __restrict__ tw4) {
+  constexpr int TT = RowCfg<N>::T;
+  constexpr int LINES = RowCfg<N>::LINES;
+  extern __shared__ float2 smem[];
+  double* red = reinterpret_cast<double*>(smem + NDIR * LINES * SmRow::padded(N));
+  const int line = threadIdx.x / TT, t = threadIdx.x % TT;
+  const long row = (long)blockIdx.x * LINES + line;
+  const bool valid = row < D.nimg * D.nz;
+  const long nrow = D.nimg * D.nz;
+  SmRow sm0{smem + line * SmRow::padded(N)};
+  SmRow sm1{smem + (LINES + line) * SmRow::padded(N)};
+  dct3_start<N, TT>(sm0, t, tw4, tmp + row * N, valid);
+  if (NDIR == 2) dct3_start<N, TT>(sm1, t, tw4, tmp + (nrow + row) * N, valid);
+  float s[3] = {0.f, 0.f, 0.f};
+  for (int tx = t; tx < N; tx += TT) {
+    if (!valid) break;
+    const float2 x0 = x0c[row * N + tx];
+    const float d = data[row * N + tx];
+    const float a = sqrtf(x0.x * x0.x + x0.y * x0.y);
+    const float2 l0 = make_float2(x0.x / a, x0.y / a);
+    const float d0 = d / a;
+    const float2 y0 = sm0.ld(dct_perm(tx, N));
+    const float ly = l0.x * y0.x + l0.y * y0.y;  // Re(conj(l0) y0)
+    s[0] += (1.f - d0) * (y0.x * y0.x + y0.y * y0.y) + d0 * ly * ly;
+    if (NDIR == 2) {
+      const float2 y1 = sm1.ld(dct_perm(tx, N));
+      const float lz = l0.x * y1.x + l0.y * y1.y;
+      s[1] += (1.f - d0) * (y0.x * y1.x + y0.y * y1.y) + d0 * ly * lz;
+      s[2] += (1.f - d0) * (y1.x * y1.x + y1.y * y1.y) + d0 * lz * lz;
+    }
+  }
+  double v[3] = {s[0], s[1], s[2]};
+  line_sums<TT, 3>(v, red, line, t);
+  if (t == 0 && valid) {
+    atomicAdd(&glob[kQ0], v[0]);
+    if (NDIR == 2) {
+      atomicAdd(&glob[kQ1], v[1]);
+      atomicAdd(&glob[kQ2], v[2]);
+    }
+  }
+}
+
+// ============================================ Hessian combination
+// out[0] = H(y,y), out[1] = H_ref(y,z), out[2] = H(z,z), out[3] = H_sym(y,z)
+__global__ void k_casc_hess_combine(const double* __restrict__ acc_img, const double* __restrict__ glob,
+                                    const float* __restrict__ posy, const float* __restrict__ posz, int ndir,
+                                    long nimg, double qscale, double* __restrict__ out) {
+  double b00 = 0, b01 = 0, b11 = 0, ayy = 0, azz = 0, ayz = 0, azy = 0;
+  for (long i = threadIdx.x; i < nimg; i += blockDim.x) {
+    const double* a = acc_img + i * kNAcc;
+    const double yx = posy[2 * i + 1], yy = posy[2 * i + 0];
+    b00 += yx * yx * a[kHxx] + 2.0 * yx * yy * a[kHxy] + yy * yy * a[kHyy];
+    ayy += -(yx * a[kAyx] + yy * a[kAyy]);
+    if (ndir == 2) {
+      const double zx = posz[2 * i + 1], zy = posz[2 * i + 0];
+      b01 += yx * zx * a[kHxx] + (yx * zy + yy * zx) * a[kHxy] + yy * zy * a[kHyy];
+      b11 += zx * zx * a[kHxx] + 2.0 * zx * zy * a[kHxy] + zy * zy * a[kHyy];
+      azz += -(zx * a[kAzx] + zy * a[kAzy]);
+      ayz += -(zx * a[kAyx] + zy * a[kAyy]);  // c_y with r_z
+      azy += -(yx * a[kAzx] + yy * a[kAzy]);  // c_z with r_y
+    }
+  }
+  __shared__ double red[7][256];
+  double vals[7] = {b00, b01, b11, ayy, azz, ayz, azy};
+  for (int j = 0; j < 7; ++j) red[j][threadIdx.x] = vals[j];
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s)
+      for (int j = 0; j < 7; ++j) red[j][threadIdx.x] += red[j][threadIdx.x + s];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    b00 = red[0][0];
+    b01 = red[1][0];
+    b11 = red[2][0];
+    ayy = red[3][0];
+    azz = red[4][0];
+    ayz = red[5][0];
+    azy = red[6][0];
+    out[0] = qscale * glob[kQ0] + glob[kL10] + glob[kL20] + b00 + 2.0 * ayy;
+    if (ndir == 2) {
+      const double common = qscale * glob[kQ1] + glob[kL11] + glob[kL21] + b01;
+      out[1] = common + ayy + azz;
+      out[2] = qscale * glob[kQ2] + glob[kL12] + glob[kL22] + b11 + 2.0 * azz;
+      out[3] = common + ayz + azy;
+    } else {
+      out[1] = out[2] = out[3] = 0.0;
+    }
+  }
+}
+
+}  // namespace ht
+
+#define HT_REC_SIZES(X) X(32) X(64) X(128) X(256) X(384) X(512) X(768) X(1024) X(2048)
+
+// ================================================================= C ABI
+struct ht_rec_s {
+  ht::CascDims D;
+  int ntheta, is_complex, device;
+  const ht_prop_s* prop;
+  float2* x0;      // [nimg, nz, n]
+  float2* P;       // [nimg, nz, n]
+  float2* tmp;     // [2, nimg, nz, n]
+  double* acc_img; // [nimg, kNAcc]
+  double* glob;    // [kNGlob]
+};
+
+extern "C" int ht_rec_create(int n, int nz, int nobj, int nzobj, int ntheta, int ndist, int is_complex,
+                             ht_prop_s* prop, ht_rec_s** out) {
+  using namespace ht;
+  HT_REQUIRE(out && prop, "ht_rec_create: null pointer");
+  HT_REQUIRE(n > 0 && nz > 0 && nobj > 0 && nzobj > 0 && ntheta > 0 && ndist > 0, "ht_rec_create: bad sizes");
+  int pn, pnz, pnd;
+  prop_dims(prop, &pn, &pnz, &pnd);
+  HT_REQUIRE(pn == n && pnz == nz && pnd == ndist, "ht_rec_create: propagator sizes differ");
+  bool n_ok = false;
+#define X(S) n_ok = n_ok || (n == S);
+  HT_REC_SIZES(X)
+#undef X
+  if (!n_ok) {
+    set_error("ht_rec_create: n must be one of 32, 64, 128, 256, 384, 512, 768, 1024, 2048");
+    return kUnsupported;
+  }
+  ht_rec_s* r = new ht_rec_s{};
+  r->D = CascDims{n, nz, nobj, nzobj, ndist, (long)ntheta * ndist};
+  r->ntheta = ntheta;
+  r->is_complex = is_complex ? 1 : 0;
+  r->prop = prop;
+  cudaGetDevice(&r->device);
+  const size_t img = (size_t)ntheta * ndist * nz * n;
+  cudaError_t e = cudaMalloc(&r->x0, sizeof(float2) * img);
+  if (e == cudaSuccess) e = cudaMalloc(&r->P, sizeof(float2) * img);
+  if (e == cudaSuccess) e = cudaMalloc(&r->tmp, sizeof(float2) * 2 * img);
+  if (e == cudaSuccess) e = cudaMalloc(&r->acc_img, sizeof(double) * (size_t)ntheta * ndist * kNAcc);
+  if (e == cudaSuccess) e = cudaMalloc(&r->glob, sizeof(double) * kNGlob);
+  if (e != cudaSuccess) {
+    set_error(std::string("ht_rec_create: ") + cudaGetErrorString(e));
+    cudaFree(r->x0);
+    cudaFree(r->P);
+    cudaFree(r->tmp);
+    cudaFree(r->acc_img);
+    cudaFree(r->glob);
+    delete r;
+    return kCudaError;
+  }
+  *out = r;
+  return kOk;
+}
+
+extern "C" int ht_rec_destroy(ht_rec_s* r) {
+  if (!r) return ht::kOk;
+  cudaFree(r->x0);
+  cudaFree(r->P);
+  cudaFree(r->tmp);
+  cudaFree(r->acc_img);
+  cudaFree(r->glob);
+  delete r;
+  return ht::kOk;
+}
+
+namespace ht {
+#define HT_ROWS_GRID(N, nrows) (unsigned)(((nrows) + RowCfg<N>::LINES - 1) / RowCfg<N>::LINES)
+
+template <int N, class T>
+static cudaError_t fwd_pass(ht_rec_s* r, const void* c, const float* pos, const float* mag, const float2* prb,
+                            const float2* hw, const float2* twn, const float2* twz, cudaStream_t st) {
+  using CF = RowCfg<N>;
+  const long nrows = r->D.nimg * r->D.nz;
+  cudaError_t e = allow_smem(k_casc_fwd<N, T>, CF::SMEM);
+  if (e != cudaSuccess) return e;
+  k_casc_fwd<N, T><<<HT_ROWS_GRID(N, nrows), CF::THREADS, CF::SMEM, st>>>((const T*)c, pos, mag, prb, r->tmp, r->D,
+                                                                           twn); ::ht::count_launch();
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  return dct_cols(r->D.nz, false, r->tmp, r->D.nimg, N, hw, r->D.ndist, twz, st);
+}
+
+template <int N, int MODE>
+static cudaError_t resid_pass(ht_rec_s* r, const float* data, float* amp, float scale, const float2* twn,
+                              cudaStream_t st) {
+  using CF = RowCfg<N>;
+  const int smem = CF::SMEM + CF::THREADS * (int)sizeof(double);
+  cudaError_t e = allow_smem(k_casc_resid<N, MODE>, smem);
+  if (e != cudaSuccess) return e;
+  const long nrows = r->D.nimg * r->D.nz;
+  k_casc_resid<N, MODE><<<HT_ROWS_GRID(N, nrows), CF::THREADS, smem, st>>>(r->tmp, r->x0, data, amp, r->glob, scale,
+                                                                           r->D, twn); ::ht::count_launch();
+  return cudaGetLastError();
+}
+
+template <int N, class T>
+static cudaError_t grad_impl(ht_rec_s* r, const void* c, const float* pos, const float* mag, const float2* prb,
+                             const float* data, void* gc, float* gpos, float2* gprb, float scale, cudaStream_t st) {
+  const float2 *hw, *twn, *twz;
+  prop_tables(r->prop, &hw, &twn, &twz);
+  cudaError_t e = fwd_pass<N, T>(r, c, pos, mag, prb, hw, twn, twz, st);
+  if (e != cudaSuccess) return e;
+  if ((e = resid_pass<N, 0>(r, data, nullptr, scale, twn, st)) != cudaSuccess) return e;
+  if ((e = dct_cols(r->D.nz, true, r->tmp, r->D.nimg, N, hw, r->D.ndist, twz, st)) != cudaSuccess) return e;
+  using CF = RowCfg<N>;
+  const long nrows = r->D.nimg * r->D.nz;
+  const int smem = CF::SMEM + 5 * CF::THREADS * (int)sizeof(double);
+  if ((e = allow_smem(k_casc_adj<N, T>, smem)) != cudaSuccess) return e;
+  k_casc_adj<N, T><<<HT_ROWS_GRID(N, nrows), CF::THREADS, smem, st>>>(r->tmp, r->P, (const T*)c, pos, mag, prb,
+                                                                      r->acc_img, r->D, twn); ::ht::count_launch();
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  const long npix = (long)r->D.nz * N;
+  k_sum_theta<<<(unsigned)((r->D.ndist * npix + 255) / 256), 256, 0, st>>>(r->P, gprb, r->ntheta, r->D.ndist, npix); ::ht::count_launch();
+  dim3 g2((r->D.nobj + 31) / 32, (r->D.nzobj + 7) / 8, r->ntheta);
+  k_casc_sadj<T><<<g2, dim3(32, 8), 0, st>>>((T*)gc, r->P, prb, pos, mag, r->D); ::ht::count_launch();
+  k_casc_gpos<<<(unsigned)((r->D.nimg + 255) / 256), 256, 0, st>>>(r->acc_img, gpos, r->D.nimg); ::ht::count_launch();
+  return cudaGetLastError();
+}
+
+template <int N, class T, int NDIR>
+static cudaError_t hess_impl(ht_rec_s* r, const void* c, const float* pos, const float* mag, const float2* prb,
+                             const float* data, const void* c0, const float* p0, const float2* q0, const void* c1,
+                             const float* p1, const float2* q1, cudaStream_t st) {
+  const float2 *hw, *twn, *twz;
+  prop_tables(r->prop, &hw, &twn, &twz);
+  using CF = RowCfg<N>;
+  const long nrows = r->D.nimg * r->D.nz;
+  const int smem = NDIR * CF::SMEM + 10 * CF::THREADS * (int)sizeof(double);
+  cudaError_t e = allow_smem(k_casc_hess_fwd<N, T, NDIR>, smem);
+  if (e != cudaSuccess) return e;
+  k_casc_hess_fwd<N, T, NDIR><<<HT_ROWS_GRID(N, nrows), CF::THREADS, smem, st>>>(
+      (const T*)c, pos, mag, prb, r->P, (const T*)c0, p0, q0, (const T*)c1, p1, q1, r->tmp, r->acc_img, r->glob,
+      r->D, twn); ::ht::count_launch();
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  if ((e = dct_cols(r->D.nz, false, r->tmp, NDIR * r->D.nimg, N, hw, r->D.ndist, twz, st)) != cudaSuccess) return e;
+  const int smq = NDIR * CF::SMEM + 3 * CF::THREADS * (int)sizeof(double);
+  if ((e = allow_smem(k_casc_hess_q<N, NDIR>, smq)) != cudaSuccess) return e;
+  k_casc_hess_q<N, NDIR><<<HT_ROWS_GRID(N, nrows), CF::THREADS, smq, st>>>(r->tmp, r->x0, data, r->glob, r->D, twn); ::ht::count_launch();
+  return cudaGetLastError();
+}
+
+
+}  // namespace ht
+
+extern "C" int ht_rec_forward(ht_rec_s* r, const void* c, const float* pos, const float* mag, const void* prb,
+                              const float* data, float* amp, double* fval, void* stream) {
+  using namespace ht;
+  HT_REQUIRE(r && c && pos && mag && prb, "ht_rec_forward: null pointer");
+  HT_REQUIRE(amp || (data && fval), "ht_rec_forward: need data and fval, or amp");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const float2 *hw, *twn, *twz;
+  prop_tables(r->prop, &hw, &twn, &twz);
+  HT_CHECK_CUDA(cudaMemsetAsync(r->glob, 0, sizeof(double) * kNGlob, st));
+  cudaError_t e = cudaErrorInvalidValue;
+  switch (r->D.n) {
+#define X(S)                                                                                                  \
+  case S:                                                                                                     \
+    e = r->is_complex ? fwd_pass<S, float2>(r, c, pos, mag, (const float2*)prb, hw, twn, twz, st)              \
+                      : fwd_pass<S, float>(r, c, pos, mag, (const float2*)prb, hw, twn, twz, st);              \
+    if (e == cudaSuccess)                                                                                     \
+      e = amp ? resid_pass<S, 2>(r, data, amp, 0.f, twn, st) : resid_pass<S, 1>(r, data, nullptr, 0.f, twn, st); \
+    break;
+    HT_REC_SIZES(X)
+#undef X
+    default:
+      break;
+  }
+  HT_CHECK_CUDA(e);
+  if (fval) HT_CHECK_CUDA(cudaMemcpyAsync(fval, r->glob + kF, sizeof(double), cudaMemcpyDeviceToDevice, st));
+  return kOk;
+}
+
+extern "C" int ht_rec_gradient(ht_rec_s* r, const void* c, const float* pos, const float* mag, const void* prb,
+                               const float* data, void* gc, float* gpos, void* gprb, double* fval, void* stream) {
+  using namespace ht;
+  HT_REQUIRE(r && c && pos && mag && prb && data && gc && gpos && gprb, "ht_rec_gradient: null pointer");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  HT_CHECK_CUDA(cudaMemsetAsync(r->glob, 0, sizeof(double) * kNGlob, st));
+  HT_CHECK_CUDA(cudaMemsetAsync(r->acc_img, 0, sizeof(double) * r->D.nimg * kNAcc, st));
+  // rec_mpi.py:569: np.float32(2 / data_size)
+  const float scale = (float)(2.0 / ((double)r->ntheta * r->D.ndist * r->D.nz * r->D.n));
+  cudaError_t e = cudaErrorInvalidValue;
+  switch (r->D.n) {
+#define X(S)                                                                                                     \
+  case S:                                                                                                        \
+    e = r->is_complex ? grad_impl<S, float2>(r, c, pos, mag, (const float2*)prb, data, gc, gpos, (float2*)gprb,    \
+                                             scale, st)                                                          \
+                      : grad_impl<S, float>(r, c, pos, mag, (const float2*)prb, data, gc, gpos, (float2*)gprb,     \
+                                            scale, st);                                                          \
+    break;
+    HT_REC_SIZES(X)
+#undef X
+    default:
+      break;
+  }
+  HT_CHECK_CUDA(e);
+  if (fval) HT_CHECK_CUDA(cudaMemcpyAsync(fval, r->glob + kF, sizeof(double), cudaMemcpyDeviceToDevice, st));
+  return kOk;
+}
+
+extern "C" int ht_rec_hessian(ht_rec_s* r, const void* c, const float* pos, const float* mag, const void* prb,
+                              const float* data, int ndir, const void* cy, const float* posy, const void* prby,
+                              const void* cz, const float* posz, const void* prbz, double* out, void* stream) {
+  using namespace ht;
+  HT_REQUIRE(r && c && pos && mag && prb && data && cy && posy && prby && out, "ht_rec_hessian: null pointer");
+  HT_REQUIRE(ndir == 1 || (ndir == 2 && cz && posz && prbz), "ht_rec_hessian: ndir must be 1, or 2 with z given");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  // clear the Hessian slots only: the gradient pass's per-image terms stay
+  HT_CHECK_CUDA(cudaMemsetAsync(r->glob + kQ0, 0, sizeof(double) * (kNGlob - kQ0), st));
+  HT_CHECK_CUDA(cudaMemset2DAsync(r->acc_img + kAyx, sizeof(double) * kNAcc, 0, sizeof(double) * 4, r->D.nimg, st));
+  cudaError_t e = cudaErrorInvalidValue;
+  const float2 *q0 = (const float2*)prby, *q1 = (const float2*)prbz;
+  switch (r->D.n) {
+#define X(S)                                                                                                      \
+  case S:                                                                                                         \
+    if (r->is_complex)                                                                                            \
+      e = ndir == 2 ? hess_impl<S, float2, 2>(r, c, pos, mag, (const float2*)prb, data, cy, posy, q0, cz, posz, q1, st) \
+                    : hess_impl<S, float2, 1>(r, c, pos, mag, (const float2*)prb, data, cy, posy, q0, cy, posy, q0, st); \
+    else                                                                                                          \
+      e = ndir == 2 ? hess_impl<S, float, 2>(r, c, pos, mag, (const float2*)prb, data, cy, posy, q0, cz, posz, q1, st)  \
+                    : hess_impl<S, float, 1>(r, c, pos, mag, (const float2*)prb, data, cy, posy, q0, cy, posy, q0, st);  \
+    break;
+    HT_REC_SIZES(X)
+#undef X
+    default:
+      break;
+  }
+  HT_CHECK_CUDA(e);
+  const double qscale = 2.0 / ((double)r->ntheta * r->D.ndist * r->D.nz * r->D.n);
+  k_casc_hess_combine<<<1, 256, 0, st>>>(r->acc_img, r->glob, posy, ndir == 2 ? posz : posy, ndir, r->D.nimg, qscale,
+                                         out); ::ht::count_launch();
+  HT_CHECK_CUDA(cudaGetLastError());
+  return kOk;
+}

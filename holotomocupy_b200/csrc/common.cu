@@ -1,6 +1,7 @@
 // Error state and twiddle tables shared by all operators.
 #include "common.cuh"
 
+#include <atomic>
 #include <cmath>
 #include <map>
 #include <mutex>
@@ -15,6 +16,10 @@ std::map<std::pair<int, int>, float2*> g_tw;  // (device, N) -> table
 const int kSizes[] = {18, 24, 32, 36, 48, 64, 96, 128, 192, 256, 384, 512,
                       768, 1024, 1536, 2048, 3072, 4096};
 }  // namespace
+
+std::atomic<long> g_launches{0};
+void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+long launch_count() { return g_launches.load(std::memory_order_relaxed); }
 
 void set_error(const std::string& msg) { g_last_error = msg; }
 const char* last_error() { return g_last_error.c_str(); }

@@ -59,6 +59,10 @@ __host__ __device__ __forceinline__ float2 cmul_i(float2 a) { return make_float2
 // exp(-i*pi*k/(2N)) are tw4[k].
 const float2* twiddle_table(int N, int device);  // nullptr + error on failure
 
+// Number of kernels this library has launched (read through ht_launch_count()).
+void count_launch();
+long launch_count();
+
 // Sizes accepted by the line transforms: N = 2^a 3^b from the list below.
 bool fft_size_supported(int N);
 

@@ -90,7 +90,9 @@ k_dct3_rows(const float2* in, float2* out, long nrows, const float2* __restrict_
 // data: [nimg, NZ, n] in place; H: [NZ, n] (the j-th distance's Hw).
 template <int NZ, bool CONJ>
 __global__ void __launch_bounds__(ColCfg<NZ>::THREADS)
-k_dct_cols(float2* data, int n, const float2* __restrict__ H, const float2* __restrict__ tw4) {
+k_dct_cols(float2* data, int n, const float2* __restrict__ Hall, int ntab, const float2* __restrict__ tw4) {
+  // image blockIdx.y uses table (blockIdx.y % ntab) of Hall [ntab, NZ, n]
+  const float2* __restrict__ H = Hall + (long)(blockIdx.y % ntab) * NZ * n;
   constexpr int C = ColCfg<NZ>::C;
   constexpr int T = ColCfg<NZ>::T;
   extern __shared__ float2 tile[];
@@ -143,28 +145,28 @@ static cudaError_t launch_dct_rows(bool inverse, const float2* in, float2* out, 
   if (inverse) {
     cudaError_t e = allow_smem(k_dct3_rows<N>, CF::SMEM);
     if (e != cudaSuccess) return e;
-    k_dct3_rows<N><<<(unsigned)grid, CF::THREADS, CF::SMEM, st>>>(in, out, nrows, tw4);
+    k_dct3_rows<N><<<(unsigned)grid, CF::THREADS, CF::SMEM, st>>>(in, out, nrows, tw4); ::ht::count_launch();
   } else {
     cudaError_t e = allow_smem(k_dct2_rows<N>, CF::SMEM);
     if (e != cudaSuccess) return e;
-    k_dct2_rows<N><<<(unsigned)grid, CF::THREADS, CF::SMEM, st>>>(in, out, nrows, tw4);
+    k_dct2_rows<N><<<(unsigned)grid, CF::THREADS, CF::SMEM, st>>>(in, out, nrows, tw4); ::ht::count_launch();
   }
   return cudaGetLastError();
 }
 
 template <int NZ>
-static cudaError_t launch_dct_cols(bool conj, float2* data, long nimg, int n, const float2* H,
+static cudaError_t launch_dct_cols(bool conj, float2* data, long nimg, int n, const float2* H, int ntab,
                                    const float2* tw4, cudaStream_t st) {
   using CF = ColCfg<NZ>;
   dim3 grid((n + CF::C - 1) / CF::C, (unsigned)nimg);
   if (conj) {
     cudaError_t e = allow_smem(k_dct_cols<NZ, true>, CF::SMEM);
     if (e != cudaSuccess) return e;
-    k_dct_cols<NZ, true><<<grid, CF::THREADS, CF::SMEM, st>>>(data, n, H, tw4);
+    k_dct_cols<NZ, true><<<grid, CF::THREADS, CF::SMEM, st>>>(data, n, H, ntab, tw4); ::ht::count_launch();
   } else {
     cudaError_t e = allow_smem(k_dct_cols<NZ, false>, CF::SMEM);
     if (e != cudaSuccess) return e;
-    k_dct_cols<NZ, false><<<grid, CF::THREADS, CF::SMEM, st>>>(data, n, H, tw4);
+    k_dct_cols<NZ, false><<<grid, CF::THREADS, CF::SMEM, st>>>(data, n, H, ntab, tw4); ::ht::count_launch();
   }
   return cudaGetLastError();
 }
@@ -182,12 +184,12 @@ cudaError_t dct_rows(int N, bool inverse, const float2* in, float2* out, long nr
   }
 }
 
-cudaError_t dct_cols(int NZ, bool conj, float2* data, long nimg, int n, const float2* H, const float2* tw4,
-                     cudaStream_t st) {
+cudaError_t dct_cols(int NZ, bool conj, float2* data, long nimg, int n, const float2* H, int ntab,
+                     const float2* tw4, cudaStream_t st) {
   switch (NZ) {
 #define X(S) \
   case S:    \
-    return launch_dct_cols<S>(conj, data, nimg, n, H, tw4, st);
+    return launch_dct_cols<S>(conj, data, nimg, n, H, ntab, tw4, st);
     HT_SIZE_CASES(X)
 #undef X
     default:
@@ -253,6 +255,18 @@ extern "C" int ht_prop_destroy(ht_prop_s* p) {
 }
 
 namespace ht {
+void prop_dims(const ht_prop_s* p, int* n, int* nz, int* ndist) {
+  *n = p->n;
+  *nz = p->nz;
+  *ndist = p->ndist;
+}
+
+void prop_tables(const ht_prop_s* p, const float2** hw, const float2** twn, const float2** twz) {
+  *hw = p->hw;
+  *twn = p->tw_n;
+  *twz = p->tw_nz;
+}
+
 int prop_apply(ht_prop_s* p, const void* in, void* out, long batch, int j, bool adjoint, cudaStream_t st) {
   HT_REQUIRE(p != nullptr, "propagator handle is null");
   HT_REQUIRE(in != nullptr && out != nullptr, "propagator: null data pointer");
@@ -263,7 +277,7 @@ int prop_apply(ht_prop_s* p, const void* in, void* out, long batch, int j, bool 
   float2* dst = static_cast<float2*>(out);
   const float2* H = p->hw + (size_t)j * p->nz * p->n;
   HT_CHECK_CUDA(dct_rows(p->n, false, src, dst, batch * p->nz, p->tw_n, st));
-  HT_CHECK_CUDA(dct_cols(p->nz, adjoint, dst, batch, p->n, H, p->tw_nz, st));
+  HT_CHECK_CUDA(dct_cols(p->nz, adjoint, dst, batch, p->n, H, 1, p->tw_nz, st));
   HT_CHECK_CUDA(dct_rows(p->n, true, dst, dst, batch * p->nz, p->tw_n, st));
   return kOk;
 }

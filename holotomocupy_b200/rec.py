@@ -1,0 +1,530 @@
+"""Bilinear-Hessian holotomography solver on the B200 (drop-in for holotomocupy's Rec).
+
+Reference: ``src/holotomocupy/rec_mpi.py:21-902`` (single rank).  Same
+constructor ``Rec(args)`` with the reference's argument keys, the same
+``vars`` / ``grads`` / ``etas`` dictionaries (CUDA torch tensors, resident on
+the device instead of pinned host arrays), the cascade functions ``F*``,
+``dF*``, ``d2F_dF*``, ``gF*`` (operator-by-operator, for derivative checks),
+and ``gradients``, ``hessian``, ``BH``, ``min``, ``gen_sqrt_data``,
+``gen_sqrt_ref``.
+
+The solver itself runs the fused cascade of ``libholotomo_b200.so``
+(``ht_rec_gradient`` / ``ht_rec_hessian``): one gradient pass and one Hessian
+pass per iteration evaluate every quadratic form the reference's three
+Hessian cascades produce, with the B-spline coefficients of vars/grads/etas
+``proj`` kept alongside ``proj`` (the prefilter is linear, so the BH updates
+apply to them directly).  Inner products, quadratic forms and the step sizes
+are accumulated in float64.
+
+Optional argument keys beyond the reference's: ``distance``, ``wavelength``,
+``voxelsize`` and ``norm_magnifications`` give the propagation geometry
+directly instead of deriving it from ``z1``/``energy`` (rec_mpi.py:55-60).
+"""
+import ctypes
+import math
+import time
+
+import numpy as np
+import torch
+
+from . import _lib
+from .propagation import Propagation
+from .shift import Shift
+from .tomo import Tomo
+
+
+def _t(x, device, dtype=None):
+    if isinstance(x, torch.Tensor):
+        return x.to(device=device, dtype=dtype or x.dtype)
+    return torch.as_tensor(np.asarray(x), device=device, dtype=dtype)
+
+
+def reprod(a, b):
+    """utils.py:96-97"""
+    if a.is_complex() or b.is_complex():
+        a = a if a.is_complex() else torch.complex(a, torch.zeros_like(a))
+        b = b if b.is_complex() else torch.complex(b, torch.zeros_like(b))
+        return a.real * b.real + a.imag * b.imag
+    return a * b
+
+
+def redot(a, b):
+    """utils.py:100-103, accumulated in float64."""
+    return float(torch.sum(reprod(a, b).double()))
+
+
+class Rec:
+    """BH reconstruction (rec_mpi.py:21)."""
+
+    def __init__(self, args):
+        for key, value in vars(args).items():
+            setattr(self, key, value)
+        if not hasattr(self, "lam_laplacian"):
+            self.lam_laplacian = 0
+        if not hasattr(self, "lam_prbfit"):
+            self.lam_prbfit = 0
+        if self.lam_laplacian != 0:
+            raise NotImplementedError("lam_laplacian != 0: the Laplacian regulariser is not built yet")
+        self.device = torch.device("cuda", torch.cuda.current_device())
+        dev = self.device
+        self.F = [self.F0, self.F1, self.F2, self.F3]
+        self.gF = [self.gF0, self.gF1, self.gF2, self.gF3]
+        self.dF = [self.dF0, self.dF1, self.dF2, self.dF3]
+        self.d2F_dF = [self.d2F_dF0, self.d2F_dF1, self.d2F_dF2, self.d2F_dF3]
+        if getattr(self, "distance", None) is None:                      # rec_mpi.py:55-60
+            wavelength = 1.24e-09 / self.energy
+            z1 = np.asarray(self.z1)
+            z2 = self.focustodetectordistance - z1
+            magnifications = self.focustodetectordistance / z1
+            norm_magnifications = magnifications / magnifications[0]
+            distance = (z1 * z2) / self.focustodetectordistance * norm_magnifications ** 2
+            voxelsize = self.detector_pixelsize / magnifications[0]
+        else:
+            wavelength, voxelsize, distance = self.wavelength, self.voxelsize, np.asarray(self.distance)
+            norm_magnifications = np.asarray(getattr(self, "norm_magnifications", np.ones(self.ndist)))
+        self.rho_sq = {"obj": args.rho[0] ** 2, "prb": args.rho[1] ** 2, "pos": args.rho[2] ** 2}
+        self.complex_obj = self.obj_dtype == "complex64"
+        self.odt = torch.complex64 if self.complex_obj else torch.float32
+        theta = np.asarray(self.theta.cpu() if isinstance(self.theta, torch.Tensor) else self.theta)
+        self.cl_tomo = Tomo(self.nobj, self.nzobj, theta, self.mask)
+        self.cl_prop = Propagation(self.n, self.nz, self.ntheta, self.ndist, wavelength, voxelsize, distance)
+        self.cl_shift = Shift(self.n, self.nobj, self.nz, self.nzobj, self.obj_dtype)
+        self.norm_const = float(np.float32(np.sqrt(self.nobj / self.ntheta)))   # rec_mpi.py:88
+        self.norm_magnifications = norm_magnifications
+        self.data_size = self.ntheta * self.ndist * self.nz * self.n
+        self.prb_size = self.ndist * self.nz * self.n
+        self.obj_size = self.nzobj * self.nobj ** 2
+        self.table = []
+        self.alloc_arrays()
+        h = ctypes.c_void_p()
+        _lib.call("ht_rec_create", self.n, self.nz, self.nobj, self.nzobj, self.ntheta, self.ndist,
+                  1 if self.complex_obj else 0, self.cl_prop._h, ctypes.byref(h))
+        self._h = h
+        self._scal = torch.zeros(8, dtype=torch.float64, device=dev)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            try:
+                _lib.lib().ht_rec_destroy(h)
+            except Exception:
+                pass
+            self._h = None
+
+    # ------------------------------------------------------------ state
+    def alloc_arrays(self):
+        """rec_mpi.py:105-136 (device-resident, zero-initialised)."""
+        dev, odt = self.device, self.odt
+        prb_shape = (self.ndist, self.nz, self.n)
+        z = lambda *s, dt=odt: torch.zeros(*s, dtype=dt, device=dev)
+        self.vars = {"obj": z(self.nzobj, self.nobj, self.nobj), "pos": z(self.ntheta, self.ndist, 2, dt=torch.float32),
+                     "prb": z(*prb_shape, dt=torch.complex64), "proj": z(self.ntheta, self.nzobj, self.nobj)}
+        self.data = z(self.ntheta, self.ndist, self.nz, self.n, dt=torch.float32)
+        self.ref = z(*prb_shape, dt=torch.float32)
+        self.grads, self.etas = {}, {}
+        for ge in (self.grads, self.etas):
+            ge["obj"] = z(self.nzobj, self.nobj, self.nobj)
+            ge["pos"] = z(self.ntheta, self.ndist, 2, dt=torch.float32)
+            ge["proj"] = z(self.ntheta, self.nzobj, self.nobj)
+            ge["prb"] = z(*prb_shape, dt=torch.complex64)
+        # rec_mpi.py:135-136: one array, zero until BH() sets it (rec_mpi.py:146)
+        self.shrink_nd = z(self.ntheta, self.ndist, dt=torch.float32)
+        self.eff_demagnifications = self.shrink_nd
+        # B-spline coefficients of vars/grads/etas proj
+        self._c = {"vars": z(self.ntheta, self.nzobj, self.nobj), "grads": z(self.ntheta, self.nzobj, self.nobj),
+                   "etas": z(self.ntheta, self.nzobj, self.nobj)}
+
+    def _coeff_into(self, src, dst):
+        """dst = coeff(src) (shift.py:74-82) for a [ntheta, nzobj, nobj] array."""
+        if self.complex_obj:
+            _lib.call("ht_shift_coeff", self.cl_shift._hc, _lib.ptr(src), _lib.ptr(dst), src.shape[0],
+                      _lib.stream_ptr())
+        else:
+            dst.copy_(self.cl_shift.coeff(src))
+        return dst
+
+    def _axpby(self, x, y, a, b, dot=None):
+        n = x.numel() * (2 if x.is_complex() else 1)
+        _lib.call("ht_axpby", _lib.ptr(x), _lib.ptr(y), float(a), float(b), n,
+                  _lib.ptr(dot) if dot is not None else None, _lib.stream_ptr())
+
+    # -------------------------------------------------- fused cascade
+    def _gradient_pass(self, c, pos, prb):
+        """Fused gF0..gF3 (rec_mpi.py:327-353): returns (sum_k S^T Y22, gpos, gprb), F in _scal[0]."""
+        gc = torch.empty_like(c)
+        gpos = torch.empty(self.ntheta, self.ndist, 2, dtype=torch.float32, device=self.device)
+        gprb = torch.empty(self.ndist, self.nz, self.n, dtype=torch.complex64, device=self.device)
+        _lib.call("ht_rec_gradient", self._h, _lib.ptr(c), _lib.ptr(pos), _lib.ptr(self.eff_demagnifications),
+                  _lib.ptr(prb), _lib.ptr(self.data), _lib.ptr(gc), _lib.ptr(gpos), _lib.ptr(gprb),
+                  _lib.ptr(self._scal), _lib.stream_ptr())
+        return gc, gpos, gprb
+
+    def _hessian_pass(self, c, pos, prb, y, z=None):
+        """Fused Hessian forms; y, z = (coefficients, pos, prb) of the directions.
+        Returns float64 tensor [H(y,y), H_ref(y,z), H(z,z), H_sym(y,z)]."""
+        out = torch.zeros(4, dtype=torch.float64, device=self.device)
+        zz = z if z is not None else (None, None, None)
+        _lib.call("ht_rec_hessian", self._h, _lib.ptr(c), _lib.ptr(pos), _lib.ptr(self.eff_demagnifications),
+                  _lib.ptr(prb), _lib.ptr(self.data), 2 if z is not None else 1, _lib.ptr(y[0]), _lib.ptr(y[1]),
+                  _lib.ptr(y[2]), _lib.ptr(zz[0]) if z is not None else None,
+                  _lib.ptr(zz[1]) if z is not None else None, _lib.ptr(zz[2]) if z is not None else None,
+                  _lib.ptr(out), _lib.stream_ptr())
+        return out
+
+    def _contig(self, d):
+        return {k: v.contiguous() for k, v in d.items()}
+
+    def gradients_cascade(self, vars, grads):
+        """rec_mpi.py:327-353 (data term; writes grads prb/proj/pos)."""
+        v = self._contig(vars)
+        c = self._coeff_into(v["proj"], torch.empty_like(v["proj"]))
+        gc, gpos, gprb = self._gradient_pass(c, v["pos"], v["prb"])
+        grads["prb"][:] = gprb * self.rho_sq["prb"]
+        grads["proj"][:] = self.cl_shift.coeff(gc) * self.rho_sq["obj"]
+        grads["pos"][:] = gpos * self.rho_sq["pos"]
+
+    def hessian_cascade(self, vars, grads, etas):
+        """rec_mpi.py:250-303: the data-term Hessian form at vars for (grads, etas)."""
+        v = self._contig(vars)
+        c = self._coeff_into(v["proj"], torch.empty_like(v["proj"]))
+        self._gradient_pass(c, v["pos"], v["prb"])
+        y_is_z = grads["prb"] is etas["prb"]
+        g, e = self._contig(grads), self._contig(etas)
+        cy = self._coeff_into(g["proj"], torch.empty_like(g["proj"]))
+        y = (cy, g["pos"], g["prb"])
+        if y_is_z:
+            return float(self._hessian_pass(c, v["pos"], v["prb"], y)[0])
+        cz = self._coeff_into(e["proj"], torch.empty_like(e["proj"]))
+        return float(self._hessian_pass(c, v["pos"], v["prb"], y, (cz, e["pos"], e["prb"]))[1])
+
+    # ------------------------------------------------- probe-fit term
+    def gradient_prbfit(self, grad_prb, prb):
+        """rec_mpi.py:365-377"""
+        if self.lam_prbfit == 0:
+            return
+        for j in range(self.ndist):
+            tmp = self.cl_prop.D(prb[j: j + 1].contiguous(), j)
+            td = self.ref[j: j + 1] * (tmp / torch.abs(tmp))
+            td = self.lam_prbfit / self.prb_size * self.cl_prop.DT(2 * (tmp - td), j)
+            grad_prb[j: j + 1] += td * self.rho_sq["prb"]
+
+    def _prbfit_forms(self, prb, d1, d2):
+        """hessian_prbfit (rec_mpi.py:379-398) for the pairs (d1,d1), (d1,d2), (d2,d2)."""
+        if self.lam_prbfit == 0:
+            return 0.0, 0.0, 0.0
+        out = [0.0, 0.0, 0.0]
+        for j in range(self.ndist):
+            Dp = self.cl_prop.D(prb[j: j + 1].contiguous(), j)
+            Da = self.cl_prop.D(d1[j: j + 1].contiguous(), j)
+            Db = self.cl_prop.D(d2[j: j + 1].contiguous(), j) if d2 is not None else Da
+            l0 = Dp / torch.abs(Dp)
+            d0 = self.ref[j: j + 1] / torch.abs(Dp)
+            for i, (u, w) in enumerate(((Da, Da), (Da, Db), (Db, Db))):
+                v1 = torch.sum(((1 - d0) * reprod(u, w)).double())
+                v2 = torch.sum((d0 * reprod(l0, u) * reprod(l0, w)).double())
+                out[i] += float(2 * (v1 + v2))
+        s = self.lam_prbfit / self.prb_size
+        return out[0] * s, out[1] * s, out[2] * s
+
+    # ----------------------------------------------------- forward use
+    def fwd_tomo(self, obj, out=None):
+        """rec_mpi.py:498-507"""
+        return self.cl_tomo.R(obj, out=out)
+
+    def min(self, prb, obj, pos, proj):
+        """rec_mpi.py:815-835: data term + probe-fit term."""
+        c = self._coeff_into(proj.contiguous(), torch.empty_like(proj))
+        _lib.call("ht_rec_forward", self._h, _lib.ptr(c), _lib.ptr(pos.contiguous()),
+                  _lib.ptr(self.eff_demagnifications), _lib.ptr(prb.contiguous()), _lib.ptr(self.data), None,
+                  _lib.ptr(self._scal), _lib.stream_ptr())
+        out = float(self._scal[0]) / self.data_size
+        if self.lam_prbfit != 0:
+            for j in range(self.ndist):
+                Dprb = self.cl_prop.D(prb[j: j + 1].contiguous(), j)[0]
+                out += self.lam_prbfit / self.prb_size * float(torch.linalg.norm(torch.abs(Dprb) - self.ref[j])) ** 2
+        return out
+
+    def gen_sqrt_data(self, vars, out):
+        """rec_mpi.py:882-897 (note: before the first BH() call the reference's
+        eff_demagnifications is still zero, rec_mpi.py:135-136, and so is it here)."""
+        vars["obj"] /= self.norm_const
+        self.fwd_tomo(vars["obj"], out=vars["proj"])
+        c = self._coeff_into(vars["proj"], torch.empty_like(vars["proj"]))
+        _lib.call("ht_rec_forward", self._h, _lib.ptr(c), _lib.ptr(vars["pos"]), _lib.ptr(self.eff_demagnifications),
+                  _lib.ptr(vars["prb"]), None, _lib.ptr(out), None, _lib.stream_ptr())
+        vars["obj"] *= self.norm_const
+
+    def forward_amplitudes(self, obj, prb, pos, out=None):
+        """|F1(F2(F3(prb, R(obj / norm_const), pos)))| with the physical
+        magnifications 1 / norm_magnifications: the synthetic-data forward model
+        (gen_sqrt_data without the zero-magnification start state)."""
+        eff = torch.empty(self.ntheta, self.ndist, dtype=torch.float32, device=self.device)
+        eff[:] = _t(1.0 / np.asarray(self.norm_magnifications, dtype=np.float64)[None, :], self.device, torch.float32)
+        proj = self.fwd_tomo((obj / self.norm_const).to(self.odt).contiguous())
+        c = self._coeff_into(proj, torch.empty_like(proj))
+        del proj
+        if out is None:
+            out = torch.empty(self.ntheta, self.ndist, self.nz, self.n, dtype=torch.float32, device=self.device)
+        _lib.call("ht_rec_forward", self._h, _lib.ptr(c), _lib.ptr(pos.contiguous()), _lib.ptr(eff),
+                  _lib.ptr(prb.contiguous()), None, _lib.ptr(out), None, _lib.stream_ptr())
+        return out
+
+    def gen_sqrt_ref(self, prb, out):
+        """rec_mpi.py:899-902"""
+        for j in range(self.ndist):
+            out[j] = torch.abs(self.cl_prop.D(prb[j: j + 1].contiguous(), j)[0])
+
+    # ------------------------------------------------------------ BH
+    def BH(self, writer=None, niter=None, record=None):
+        """rec_mpi.py:138-232.  ``record`` (a list) receives (iteration, alpha, beta)."""
+        self.bh_setup()
+        niter = self.niter if niter is None else niter
+        for i in range(self.start_iter, niter):
+            a, b = self.bh_iteration(i)
+            if record is not None:
+                record.append((i, a, b))
+            self.error_debug(self.vars, i)
+        return self.bh_finish()
+
+    def bh_setup(self):
+        """Start of BH (rec_mpi.py:139-162): magnifications, normalisation, mask,
+        proj = R(obj) and its B-spline coefficients."""
+        vars, C = self.vars, self._c
+        self.eff_demagnifications[:] = (1 + self.shrink_nd) / _t(self.norm_magnifications[None, :], self.device,
+                                                                 torch.float32)
+        vars["obj"] /= self.norm_const
+        if self.start_iter == 0:
+            vars["obj"] *= self.cl_tomo.mask
+        self.fwd_tomo(vars["obj"], out=vars["proj"])
+        self._coeff_into(vars["proj"], C["vars"])
+        self.error_debug(vars, -1)
+        self.time_start = time.time()
+        if not hasattr(self, "_dots"):
+            self._dots = torch.zeros(4, dtype=torch.float64, device=self.device)
+
+    def bh_finish(self):
+        """End of BH (rec_mpi.py:229-232)."""
+        self.vars["obj"] *= self.norm_const
+        return self.vars
+
+    def bh_iteration(self, i):
+        """One BH iteration (rec_mpi.py:163-227); returns (alpha, beta)."""
+        vars, grads, etas, C = self.vars, self.grads, self.etas, self._c
+        rho = self.rho_sq
+        dots = self._dots
+        # ---- gradients (rec_mpi.py:305-325)
+        gc, gpos, gprb = self._gradient_pass(C["vars"], vars["pos"], vars["prb"])
+        torch.mul(gprb, rho["prb"], out=grads["prb"])
+        torch.mul(gpos, rho["pos"], out=grads["pos"])
+        self._coeff_into(gc, grads["proj"])
+        grads["proj"] *= rho["obj"]
+        self.cl_tomo.RT(grads["proj"], out=grads["obj"])               # gF4
+        self.gradient_prbfit(grads["prb"], vars["prb"])
+        self.fwd_tomo(grads["obj"], out=grads["proj"])
+        self._coeff_into(grads["proj"], C["grads"])
+        # ---- Hessian forms (rec_mpi.py:180-213)
+        y = (C["grads"], grads["pos"], grads["prb"])
+        if i == self.start_iter:
+            beta = 0.0
+            H = self._hessian_pass(C["vars"], vars["pos"], vars["prb"], y).cpu().numpy()
+            pf = self._prbfit_forms(vars["prb"], grads["prb"], None)
+            Hgg = H[0] + pf[0]
+        else:
+            z = (C["etas"], etas["pos"], etas["prb"])
+            H = self._hessian_pass(C["vars"], vars["pos"], vars["prb"], y, z).cpu().numpy()
+            pf = self._prbfit_forms(vars["prb"], grads["prb"], etas["prb"])
+            Hgg, Hge, Hee, Hge_sym = H[0] + pf[0], H[1] + pf[1], H[2] + pf[2], H[3] + pf[1]
+            beta = Hge / Hee
+        # ---- conjugate direction and step (rec_mpi.py:196-218)
+        dots.zero_()
+        self._axpby(etas["obj"], grads["obj"], beta, -1, dots[0:1])
+        self._axpby(etas["pos"], grads["pos"], beta, -1, dots[1:2])
+        self._axpby(etas["prb"], grads["prb"], beta, -1, dots[2:3])
+        self._axpby(etas["proj"], grads["proj"], beta, -1)
+        self._axpby(C["etas"], C["grads"], beta, -1)
+        d = dots.cpu().numpy()
+        top = -(d[0] / rho["obj"] + d[1] / rho["pos"] + d[2] / rho["prb"])
+        bottom = Hgg if i == self.start_iter else beta * beta * Hee - 2 * beta * Hge_sym + Hgg
+        alpha = top / bottom
+        for v in ("obj", "prb", "pos", "proj"):
+            self._axpby(vars[v], etas[v], 1, alpha)
+        self._axpby(C["vars"], C["etas"], 1, alpha)
+        return float(alpha), float(beta)
+
+    def error_debug(self, vars, i):
+        """rec_mpi.py:862-880 (the convergence table is kept in self.table)."""
+        if self.err_step == -1 or i % self.err_step != 0:
+            return
+        err = self.min(vars["prb"], vars["obj"], vars["pos"], vars["proj"])
+        self.table.append((i, err, time.time() - self.time_start if i >= 0 else 0.0))
+        self.time_start = time.time()
+
+    def gradients(self, vars, grads):
+        """rec_mpi.py:305-325"""
+        self.gradients_cascade(vars, grads)
+        self.cl_tomo.RT(grads["proj"].contiguous(), out=grads["obj"])
+        self.gradient_prbfit(grads["prb"], vars["prb"])
+
+    def hessian(self, vars, grads, etas):
+        """rec_mpi.py:234-248"""
+        w = self.hessian_cascade(vars, grads, etas)
+        if self.lam_prbfit != 0:
+            w += self._prbfit_forms(vars["prb"], grads["prb"], etas["prb"])[1]
+        return w
+
+    # ====================== cascade functions, operator by operator
+    # (rec_mpi.py:517-813; used for derivative checks, not by BH())
+    def F0(self, x, d):
+        t = torch.abs(x) - d
+        return float(torch.sum((t * t).double())) / self.data_size
+
+    def dF0(self, x, y, d, return_x=False):
+        return 2 / self.data_size * redot(x - d * (x / torch.abs(x)), y)
+
+    def d2F_dF0(self, x, y, z, w, d):
+        absval = torch.abs(x)
+        l0 = x / absval
+        d0 = d / absval
+        v = (1 - d0) * reprod(y, z) + d0 * reprod(l0, y) * reprod(l0, z)
+        if w is not None:
+            v = v + reprod(x - d * l0, w)
+        return 2 / self.data_size * float(torch.sum(v.double()))
+
+    def gF0(self, x, y):
+        for i in range(1, 4)[::-1]:
+            x = self.F[i](x)
+        return np.float32(2 / self.data_size) * (x - y * (x / torch.abs(x)))
+
+    def _D(self, a, j, adj=False):
+        a = a.contiguous()
+        return self.cl_prop.DT(a, j) if adj else self.cl_prop.D(a, j)
+
+    def F1(self, x):
+        x11, x12 = x
+        x0 = torch.empty(x12.shape[0], self.ndist, self.nz, self.n, dtype=torch.complex64, device=x12.device)
+        for j in range(self.ndist):
+            x0[:, j] = self._D(x11[j] * x12[:, j], j)
+        return x0
+
+    def dF1(self, x, y, return_x=True):
+        x11, x12 = x
+        y11, y12 = y
+        y0 = (y11[None] * x12 + x11[None] * y12).to(torch.complex64)
+        for j in range(self.ndist):
+            y0[:, j] = self._D(y0[:, j], j)
+        if return_x:
+            return self.F1(x), y0
+        return y0
+
+    def d2F_dF1(self, x, y, z, w):
+        x11, x12 = x
+        y11, y12 = y
+        z11, z12 = z
+        w11, w12 = w
+        y0 = 2 * y11[None] * y12 if y12 is z12 else y11[None] * z12 + z11[None] * y12
+        if w11 is not None:
+            y0 = y0 + w11[None] * x12
+        if w12 is not None:
+            y0 = y0 + x11[None] * w12
+        y0 = y0.to(torch.complex64)
+        for j in range(self.ndist):
+            y0[:, j] = self._D(y0[:, j], j)
+        return y0
+
+    def gF1(self, x, y):
+        y0 = y
+        for i in range(2, 4)[::-1]:
+            x = self.F[i](x)
+        x11, x12 = x
+        y12 = torch.empty(y0.shape[0], self.ndist, self.nz, self.n, dtype=torch.complex64, device=y0.device)
+        for j in range(self.ndist):
+            y12[:, j] = self._D(y0[:, j], j, adj=True)
+        y11 = torch.sum(y12 * torch.conj(x12), dim=0)
+        y12 = y12 * torch.conj(x11[None])
+        return y11, y12
+
+    @staticmethod
+    def _cexp(x22):
+        return torch.exp(1j * x22.to(torch.complex64))
+
+    def F2(self, x):
+        x21, x22 = x
+        return x21, self._cexp(x22)
+
+    def dF2(self, x, y, return_x=True):
+        x21, x22 = x
+        y21, y22 = y
+        x12 = self._cexp(x22)
+        y12 = x12 * 1j * y22
+        return ([x21, x12], [y21, y12]) if return_x else [y21, y12]
+
+    def d2F_dF2(self, x, y, z, w):
+        x21, x22 = x
+        y21, y22 = y
+        z21, z22 = z
+        w21, w22 = w
+        e = self._cexp(x22)
+        y12 = e * (-y22 * z22)
+        if w22 is not None:
+            y12 = y12 + e * 1j * w22
+        return [w21, y12]
+
+    def gF2(self, x, y):
+        y11, y12 = y
+        x21, x22 = self.F3(x)
+        y22 = (-1j) * y12 * torch.conj(self._cexp(x22))
+        y22 = y22.real if not self.complex_obj else y22
+        return [y11, y22]
+
+    def _eff(self, k):
+        return self.eff_demagnifications[:, k].contiguous()
+
+    def F3(self, x):
+        x31, x32, x33 = x
+        x22 = torch.empty(len(x33), self.ndist, self.nz, self.n, dtype=self.odt, device=x32.device)
+        c = self.cl_shift.coeff(x32)
+        for k in range(self.ndist):
+            x22[:, k] = self.cl_shift.curlySc(c, x33[:, k], self._eff(k))
+        return [x31, x22]
+
+    def dF3(self, x, y, return_x=True):
+        x31, x32, x33 = x
+        y31, y32, y33 = y
+        y22 = torch.zeros(len(y32), self.ndist, self.nz, self.n, dtype=self.odt, device=y32.device)
+        c = self.cl_shift.coeff(x32)
+        c1 = self.cl_shift.coeff(y32)
+        for k in range(self.ndist):
+            y22[:, k] = self.cl_shift.dcurlySc(c, x33[:, k], self._eff(k), c1, y33[:, k])
+        if return_x:
+            return self.F3(x), [y31, y22]
+        return [y31, y22]
+
+    def d2F_dF3(self, x, y, z, w):
+        x31, x32, x33 = x
+        y31, y32, y33 = y
+        z31, z32, z33 = z
+        w31, w32, w33 = w
+        y22 = torch.zeros(len(y32), self.ndist, self.nz, self.n, dtype=self.odt, device=y32.device)
+        c = self.cl_shift.coeff(x32)
+        cy = self.cl_shift.coeff(y32)
+        cz = self.cl_shift.coeff(z32)
+        for k in range(self.ndist):
+            y22[:, k] = self.cl_shift.d2curlySc(c, x33[:, k], self._eff(k), cy, y33[:, k], cz, z33[:, k])
+        if w32 is not None:
+            cw = self.cl_shift.coeff(w32)
+            for k in range(self.ndist):
+                y22[:, k] += self.cl_shift.dcurlySc(c, x33[:, k], self._eff(k), cw, w33[:, k])
+        return [w31, y22]
+
+    def gF3(self, x, y):
+        y21, y22 = y
+        x31, x32, x33 = x
+        y32 = torch.zeros(y22.shape[0], self.nzobj, self.nobj, dtype=self.odt, device=y22.device)
+        y33 = torch.empty(y22.shape[0], self.ndist, 2, dtype=torch.float32, device=y22.device)
+        c = self.cl_shift.coeff(x32)
+        for k in range(self.ndist):
+            dpsi, dr = self.cl_shift.dcurlySadjc(c, x33[:, k], self._eff(k), y22[:, k].contiguous())
+            y32 += dpsi
+            y33[:, k] = dr
+        y32 = self.cl_shift.coeff(y32)
+        return [y21, y32, y33]

@@ -27,6 +27,10 @@ int ht_version(void);
 /* Message of the calling thread's last failed call ("" if none). */
 const char* ht_last_error(void);
 
+/* Number of CUDA kernels the library has launched in this process (all
+ * threads); no counterpart in the reference. */
+long ht_launch_count(void);
+
 /* ------------------------------------------------------------------------
  * Fresnel propagator.  Replaces Propagation.__init__/D/DT
  * (src/holotomocupy/propagation.py:14-44, 70-89, 91-112) and the cuFFTDx
@@ -47,6 +51,127 @@ int ht_prop_D(ht_prop_s* p, const void* in, void* out, long batch, int j, void* 
 
 /* out[b] = D_j^H(in[b]) (propagation.py:91-112); same layout rules as D. */
 int ht_prop_DT(ht_prop_s* p, const void* in, void* out, long batch, int j, void* stream);
+
+/* ------------------------------------------------------------------------
+ * USFFT Radon transform.  Replaces Tomo.__init__/R/RT
+ * (src/holotomocupy/tomo.py:12-54, 56-86, 88-116) and the gather kernel
+ * (src/holotomocupy/cuda_kernels.py:3-76).
+ * --------------------------------------------------------------------- */
+typedef struct ht_tomo_s ht_tomo_s;
+
+/* n: object width (= detector width); nz: slice capacity of one call;
+ * theta_host: host float32 [ntheta]; phi_host: host float32 [n, n], the
+ * reference's deapodisation factor already multiplied by the support mask
+ * and 1/(n sqrt(n ntheta)) (tomo.py:19-21, 34-47).  The handle owns a
+ * workspace of nz*(6n^2) + ntheta*nz*n complex64 samples. */
+int ht_tomo_create(int n, int nz, int ntheta, const float* theta_host, const float* phi_host, ht_tomo_s** out);
+int ht_tomo_destroy(ht_tomo_s* t);
+
+/* sino[ntheta, nz, n] = R(obj[nz, n, n]), complex64 (tomo.py:56-86). */
+int ht_tomo_R(ht_tomo_s* t, const void* obj, void* sino, int nz, void* stream);
+
+/* obj[nz, n, n] = R^T(sino[ntheta, nz, n]), complex64 (tomo.py:88-116). */
+int ht_tomo_RT(ht_tomo_s* t, const void* sino, void* obj, int nz, void* stream);
+
+/* ------------------------------------------------------------------------
+ * Cubic B-spline shift family.  Replaces Shift.__init__/coeff/S/Sadj/
+ * dcurlySc/dcurlySadjc/d2curlySc (src/holotomocupy/shift.py:18-48, 74-82,
+ * 102-122, 170-221) and the kernels s/sf, ds/dsf, d2s/d2sf, dsadj/dsadjf
+ * (src/holotomocupy/cuda_kernels.py:161-290, 377-843).
+ * Shapes: coefficients [batch, nzpsi, npsi]; shifted images [batch, nz, n];
+ * r, dr: float32 [batch, 2] as (y, x) shifts in pixels; mag: float32 [batch].
+ * is_complex = 1: complex64 elements; 0: float32 elements.
+ * --------------------------------------------------------------------- */
+typedef struct ht_shift_s ht_shift_s;
+
+int ht_shift_create(int n, int npsi, int nz, int nzpsi, int is_complex, ht_shift_s** out);
+int ht_shift_destroy(ht_shift_s* s);
+
+/* out = ifft2(fft2(psi) / B3): the B-spline prefilter (shift.py:74-82);
+ * complex64 [batch, nzpsi, npsi]; out may alias psi. */
+int ht_shift_coeff(ht_shift_s* s, const void* psi, void* out, long batch, void* stream);
+
+/* out = S_{r,mag}(c) (shift.py:102-111; cuda_kernels.py:161-227). */
+int ht_shift_S(ht_shift_s* s, const void* c, const float* r, const float* mag, void* out, long batch, void* stream);
+
+/* out = S_{r,mag}^T(g) (shift.py:113-122), deterministic gather form. */
+int ht_shift_Sadj(ht_shift_s* s, const void* g, const float* r, const float* mag, void* out, long batch,
+                  void* stream);
+
+/* First derivative: S(c1) - (dS/dr . dr)(c) (shift.py:170-183; cuda_kernels.py:547-617). */
+int ht_shift_dS(ht_shift_s* s, const void* c, const float* r, const float* mag, const void* c1, const float* dr,
+                void* out, long batch, void* stream);
+
+/* Second-order term with the reference's pairing of (c1, dr1) and (c2, dr2)
+ * (shift.py:206-221; cuda_kernels.py:377-459). */
+int ht_shift_d2S(ht_shift_s* s, const void* c, const float* r, const float* mag, const void* c1, const float* dr1,
+                 const void* c2, const float* dr2, void* out, long batch, void* stream);
+
+/* Adjoint of the derivative (shift.py:185-204; cuda_kernels.py:690-766):
+ * out1 = S^T(g) [batch, nzpsi, npsi]; out2 = double [batch, 2] with
+ * out2[b,0] = Re<g, -phi'_y phi_x c>, out2[b,1] = Re<g, -phi'_x phi_y c>,
+ * reduced in double precision (the reference returns float32). */
+int ht_shift_dSadj(ht_shift_s* s, const void* c, const float* r, const float* mag, const void* g, void* out1,
+                   double* out2, long batch, void* stream);
+
+/* ------------------------------------------------------------------------
+ * Fused BH data-fidelity cascade.  Replaces Rec.gradients_cascade,
+ * Rec.hessian_cascade and the forward model of Rec.min/gen_sqrt_data
+ * (src/holotomocupy/rec_mpi.py:250-353, 498-507, 517-813, 815-835,
+ * 882-897) with its F0..F3 / dF / d2F_dF / gF chain.
+ * Shapes (nimg = ntheta*ndist): c [ntheta, nzobj, nobj] B-spline
+ * coefficients of proj (complex64, or float32 when is_complex = 0);
+ * pos [ntheta, ndist, 2] float32 (y, x); mag [ntheta, ndist] float32;
+ * prb [ndist, nz, n] complex64; data [ntheta, ndist, nz, n] float32
+ * amplitudes.  The handle owns 4*nimg*nz*n complex64 samples of workspace:
+ * caches of the last gradient call that ht_rec_hessian reads, so call
+ * ht_rec_gradient first with the same state.
+ * --------------------------------------------------------------------- */
+typedef struct ht_rec_s ht_rec_s;
+
+int ht_rec_create(int n, int nz, int nobj, int nzobj, int ntheta, int ndist, int is_complex, ht_prop_s* prop,
+                  ht_rec_s** out);
+int ht_rec_destroy(ht_rec_s* r);
+
+/* Forward model.  With amp != NULL: amp[ntheta, ndist, nz, n] = |x0|
+ * (gen_sqrt_data, rec_mpi.py:882-897).  Otherwise *fval (device double) =
+ * 1/N sum (|x0| - data)^2 (F0 of min, rec_mpi.py:517-527, 815-835). */
+int ht_rec_forward(ht_rec_s* r, const void* c, const float* pos, const float* mag, const void* prb, const float* data,
+                   float* amp, double* fval, void* stream);
+
+/* Gradient of the data term (gF0..gF3, rec_mpi.py:327-353, 562-813), unscaled:
+ * gc [ntheta, nzobj, nobj] = sum_k S_k^T(Y22) (apply coeff() for the proj
+ * gradient), gpos [ntheta, ndist, 2] float32, gprb [ndist, nz, n] complex64,
+ * *fval (device double) = the objective at the same point. */
+int ht_rec_gradient(ht_rec_s* r, const void* c, const float* pos, const float* mag, const void* prb,
+                    const float* data, void* gc, float* gpos, void* gprb, double* fval, void* stream);
+
+/* Hessian forms at the state of the last ht_rec_gradient call
+ * (hessian_cascade, rec_mpi.py:250-303) for directions y (and z when
+ * ndir = 2), each given as (coefficients of its proj, its pos, its prb).
+ * out (device double[4]) = {H(y,y), H(y,z) as the reference evaluates it
+ * (its d2s pairs c_y with r_y and c_z with r_z), H(z,z), the symmetric
+ * H(y,z)}. */
+int ht_rec_hessian(ht_rec_s* r, const void* c, const float* pos, const float* mag, const void* prb,
+                   const float* data, int ndir, const void* cy, const float* posy, const void* prby, const void* cz,
+                   const float* posz, const void* prbz, double* out, void* stream);
+
+/* ------------------------------------------------------------------------
+ * BLAS-1 on float32 vectors (complex64 arrays as interleaved pairs, n =
+ * number of floats), inner products accumulated in double.  Replaces
+ * Chunking.linear_batch / linear_redot_batch / redot_batch
+ * (src/holotomocupy/chunking.py:235-290) and utils.redot (utils.py:100-103).
+ * --------------------------------------------------------------------- */
+/* x = a*x + b*y; if dot != NULL: *dot += sum(y * x_new) (device double). */
+int ht_axpby(void* x, const void* y, float a, float b, long n, double* dot, void* stream);
+/* *dot += sum(x * y) (device double). */
+int ht_dot(const void* x, const void* y, long n, double* dot, void* stream);
+
+/* Row filter: out[r] = IFFT(sym * FFT(in[r])) for each of nrows rows of
+ * length N (complex64); sym: device float32 [N] in FFT order, carrying the
+ * 1/N of the inverse transform.  Serves Tomo._filter_sino
+ * (src/holotomocupy/tomo.py:118-161). */
+int ht_filter_rows(int N, const void* in, void* out, long nrows, const float* sym, void* stream);
 
 #ifdef __cplusplus
 }

@@ -74,7 +74,7 @@ def prop_cases(ns):
 def shift_cases(ns):
     out = {}
     for dt in ("complex64", "float32"):
-        for (n, npsi, nz, nzpsi, ntheta, tag) in [(24, 32, 20, 28, 3, "a"), (32, 32, 32, 32, 2, "b")]:
+        for (n, npsi, nz, nzpsi, ntheta, tag) in [(24, 32, 20, 24, 3, "a"), (32, 32, 32, 32, 2, "b")]:
             key = f"{dt}_{tag}"
             rng = np.random.default_rng(300 + n + len(dt))
             s = ns.shift.Shift(n, npsi, nz, nzpsi, dt)

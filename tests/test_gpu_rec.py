@@ -1,0 +1,171 @@
+"""The BH cascade and solver on the GPU against the reference (golden vectors
+from its own rec_mpi.py), plus derivative (Taylor) checks of the cascade
+functions, as in the reference's tests/holotomo3d/test_approximation.ipynb.
+
+Bounds: cascade values rel <= 1e-5 against the reference; BH state after 4
+iterations rel L2 <= 1e-5."""
+import types
+
+import numpy as np
+import pytest
+import torch
+
+from conftest import rel_l2
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-5
+
+
+def rec_args(n, ntheta, ndist, nobj, niter=1):
+    return types.SimpleNamespace(
+        energy=17.1, detector_pixelsize=1.4760147601476e-6 * 2 * 2048 / n,
+        focustodetectordistance=1.217,
+        z1=(np.array([5.110, 5.464, 6.879, 9.817]) * 1e-3 + 3.135e-3)[:ndist],
+        theta=np.linspace(0, np.pi, ntheta, endpoint=False).astype("float32"),
+        ndist=ndist, ntheta=ntheta, nz=n, n=n, nzobj=nobj, nobj=nobj,
+        obj_dtype="complex64", mask=0.9, lam_prbfit=0.0, rho=[1, 0.05, 0.02],
+        niter=niter, nchunk=max(nobj, ntheta), vis_step=-1, err_step=-1, start_iter=0)
+
+
+def cuda(a):
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+def _cascade_setup(g):
+    from holotomocupy_b200.rec import Rec
+    n, ntheta, ndist, nobj = [int(v) for v in g["c_dims"]]
+    rec = Rec(rec_args(n, ntheta, ndist, nobj))
+    np.testing.assert_array_equal(rec.cl_prop.fker.cpu().numpy(), g["c_fker"])
+    rec.data[:] = cuda(g["c_data"])
+    rec.eff_demagnifications[:] = (1 + rec.shrink_nd) / cuda(rec.norm_magnifications[None, :].astype("float32"))
+    v = {"prb": cuda(g["c_prb"]), "proj": cuda(g["c_proj"]), "pos": cuda(g["c_pos"])}
+    gr = {k: cuda(g[f"c_g_{k}"]) for k in ("prb", "proj", "pos")}
+    et = {k: cuda(g[f"c_e_{k}"]) for k in ("prb", "proj", "pos")}
+    return rec, v, gr, et
+
+
+def test_cascade_matches_reference(golden):
+    g = golden("rec")
+    rec, v, gr, et = _cascade_setup(g)
+    assert abs(rec.min(v["prb"], None, v["pos"], v["proj"]) / float(g["c_F"]) - 1) < TOL
+    assert abs(rec.hessian_cascade(v, gr, et) / float(g["c_h_ge"]) - 1) < TOL
+    assert abs(rec.hessian_cascade(v, et, et) / float(g["c_h_ee"]) - 1) < TOL
+    out = {k: torch.zeros_like(v[k]) for k in v}
+    rec.gradients_cascade(v, out)
+    for k in ("prb", "proj", "pos"):
+        assert rel_l2(out[k].cpu().numpy(), g[f"c_grad_{k}"]) < TOL, k
+
+
+def test_cascade_functions_match_reference(golden):
+    """The operator-by-operator F/gF chain gives the same gradient as the fused pass."""
+    g = golden("rec")
+    rec, v, gr, et = _cascade_setup(g)
+    x = [v["prb"], v["proj"], v["pos"]]
+    y = rec.data
+    for f in rec.gF:
+        y = f(x, y)
+    assert rel_l2((y[0] * rec.rho_sq["prb"]).cpu().numpy(), g["c_grad_prb"]) < TOL
+    assert rel_l2((y[1] * rec.rho_sq["obj"]).cpu().numpy(), g["c_grad_proj"]) < TOL
+    assert rel_l2((y[2] * rec.rho_sq["pos"]).cpu().numpy(), g["c_grad_pos"]) < TOL
+
+
+def test_symmetric_hessian_is_the_polarised_quadratic_form(golden):
+    g = golden("rec")
+    rec, v, gr, et = _cascade_setup(g)
+    c = rec._coeff_into(v["proj"], torch.empty_like(v["proj"]))
+    rec._gradient_pass(c, v["pos"], v["prb"])
+    co = lambda p: rec._coeff_into(p.contiguous(), torch.empty_like(p))
+    y = (co(gr["proj"]), gr["pos"], gr["prb"])
+    z = (co(et["proj"]), et["pos"], et["prb"])
+    H = rec._hessian_pass(c, v["pos"], v["prb"], y, z).cpu().numpy()
+    s = tuple((a + b).contiguous() for a, b in zip(y, z))
+    d = tuple((a - b).contiguous() for a, b in zip(y, z))
+    Hs = float(rec._hessian_pass(c, v["pos"], v["prb"], s)[0])
+    Hd = float(rec._hessian_pass(c, v["pos"], v["prb"], d)[0])
+    assert abs(H[3] - (Hs - Hd) / 4) <= 1e-4 * (abs(Hs) + abs(Hd))
+    Hyy = float(rec._hessian_pass(c, v["pos"], v["prb"], y)[0])
+    assert abs(H[0] / Hyy - 1) < 1e-6
+
+
+def test_bh_matches_reference(golden):
+    from holotomocupy_b200.rec import Rec
+    g = golden("rec")
+    n, ntheta, ndist, nobj, niter = [int(v) for v in g["bh_dims"]]
+    rec = Rec(rec_args(n, ntheta, ndist, nobj, niter))
+    rec.vars["obj"][:] = cuda(g["bh_obj_true"])
+    rec.vars["prb"][:] = cuda(g["bh_prb_true"])
+    rec.vars["pos"][:] = cuda(g["bh_pos_true"])
+    rec.gen_sqrt_data(rec.vars, rec.data)
+    assert rel_l2(rec.data.cpu().numpy(), g["bh_data"]) < TOL
+    rec.vars["obj"][:] = 0
+    rec.vars["prb"][:] = 1
+    rec.vars["pos"][:] = cuda(g["bh_pos_true"] + g["bh_pos_err"])
+    record = []
+    rec.BH(record=record)
+    tb = g["bh_topbottom"]
+    ref_alpha = [tb[0, 0] / tb[0, 1]] + [tb[2 * i, 0] / tb[2 * i, 1] for i in range(1, niter)]
+    ref_beta = [0.0] + [tb[2 * i - 1, 0] / tb[2 * i - 1, 1] for i in range(1, niter)]
+    for (i, a, b), ra, rb in zip(record, ref_alpha, ref_beta):
+        assert abs(a / ra - 1) < 1e-4, (i, a, ra)
+        if rb:
+            assert abs(b / rb - 1) < 1e-4, (i, b, rb)
+    for k in ("obj", "prb", "pos", "proj"):
+        assert rel_l2(rec.vars[k].cpu().numpy(), g[f"bh_{k}"]) < TOL, k
+
+
+def _taylor(f_w, f_at, df, d2f, L):
+    e1, e2, e3 = [], [], []
+    for l in L:
+        a = f_at(l)
+        e1.append(float(torch.linalg.norm(f_w - a)) if torch.is_tensor(a) else abs(f_w - a))
+        e2.append(float(torch.linalg.norm(f_w + df(l) - a)) if torch.is_tensor(a) else abs(f_w + df(l) - a))
+        e3.append(float(torch.linalg.norm(f_w + df(l) + 0.5 * d2f(l) - a)) if torch.is_tensor(a)
+                  else abs(f_w + df(l) + 0.5 * d2f(l) - a))
+    return np.array(e1), np.array(e2), np.array(e3)
+
+
+def test_taylor_orders():
+    """tests/holotomo3d/test_approximation.ipynb cells 4-10 of the reference, asserted:
+    halving the step divides the first-order residual by ~4 and the
+    second-order residual by ~8."""
+    from holotomocupy_b200.rec import Rec
+    n, ntheta, ndist = 64, 4, 2
+    args = rec_args(n, ntheta, ndist, n)
+    args.theta = np.linspace(0, np.pi, ntheta).astype("float32")
+    rec = Rec(args)
+    rec.eff_demagnifications[:] = 1.0
+    rng = np.random.default_rng(42)
+    rc = lambda s, sc=1.0: cuda(((rng.standard_normal(s) + 1j * rng.standard_normal(s)) * sc).astype("complex64"))
+    rf = lambda s, sc=1.0: cuda((rng.standard_normal(s) * sc).astype("float32"))
+    prb, proj, pos = rc((ndist, n, n)), rf((ntheta, n, n), 0.1).to(torch.complex64), rf((ntheta, ndist, 2), 0.5)
+    dprb, dproj, dpos = rc((ndist, n, n)), rf((ntheta, n, n), 0.1).to(torch.complex64), rf((ntheta, ndist, 2), 0.5)
+    L = [0.08, 0.04]   # the reference notebook reads its ratios at steps 0.05-0.08
+    # F3
+    x3, dx3 = [prb, proj, pos], [dprb, dproj, dpos]
+    sc = lambda l: [l * v for v in dx3]
+    e1, e2, e3 = _taylor(rec.F3(x3)[1], lambda l: rec.F3([v + d for v, d in zip(x3, sc(l))])[1],
+                         lambda l: rec.dF3(x3, sc(l), return_x=False)[1],
+                         lambda l: rec.d2F_dF3(x3, sc(l), sc(l), [None] * 3)[1], L)
+    assert 3.0 < e2[0] / e2[1] < 5.0 and 6.0 < e3[0] / e3[1] < 10.0
+    # F2
+    x22, dx22 = rf((ntheta, ndist, n, n), 0.1), rf((ntheta, ndist, n, n), 0.1)
+    x2, dx2 = [prb, x22], [dprb, dx22]
+    sc = lambda l: [l * v for v in dx2]
+    e1, e2, e3 = _taylor(rec.F2(x2)[1], lambda l: rec.F2([v + d for v, d in zip(x2, sc(l))])[1],
+                         lambda l: rec.dF2(x2, sc(l), return_x=False)[1],
+                         lambda l: rec.d2F_dF2(x2, sc(l), sc(l), [None, None])[1], L)
+    assert 3.0 < e2[0] / e2[1] < 5.0 and 6.0 < e3[0] / e3[1] < 10.0
+    # F1 (bilinear: the second-order expansion is exact)
+    x1 = [rc((ndist, n, n)), rc((ntheta, ndist, n, n))]
+    dx1 = [rc((ndist, n, n)), rc((ntheta, ndist, n, n), 0.1)]
+    sc = lambda l: [l * v for v in dx1]
+    e1, e2, e3 = _taylor(rec.F1(x1), lambda l: rec.F1([v + d for v, d in zip(x1, sc(l))]),
+                         lambda l: rec.dF1(x1, sc(l), return_x=False),
+                         lambda l: rec.d2F_dF1(x1, sc(l), sc(l), [None, None]), L)
+    assert 3.0 < e2[0] / e2[1] < 5.0 and e3[0] < 1e-5 * e1[0]
+    # F0
+    data = torch.abs(rf((ntheta, ndist, n, n))) + 0.1
+    x0, dx0 = rc((ntheta, ndist, n, n)), rc((ntheta, ndist, n, n), 0.1)
+    e1, e2, e3 = _taylor(rec.F0(x0, data), lambda l: rec.F0(x0 + l * dx0, data),
+                         lambda l: rec.dF0(x0, l * dx0, data), lambda l: rec.d2F_dF0(x0, l * dx0, l * dx0, None, data), L)
+    assert 3.0 < e2[0] / e2[1] < 5.0 and 6.0 < e3[0] / e3[1] < 10.0

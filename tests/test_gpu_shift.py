@@ -1,0 +1,74 @@
+"""B-spline shift family on the GPU against the reference (golden vectors from
+its own shift.py) and the oracle.  Bound: rel L2 <= 1e-5."""
+import numpy as np
+import pytest
+import torch
+
+from conftest import rel_l2
+from oracle import holo_oracle as O
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-5
+
+
+@pytest.mark.parametrize("key", ["complex64_a", "complex64_b", "float32_a", "float32_b"])
+def test_shift_family_matches_reference(golden, key):
+    from holotomocupy_b200 import Shift
+    g = golden("shift")
+    G = lambda k: torch.from_numpy(g[f"{key}_{k}"]).cuda()
+    R = lambda k: g[f"{key}_{k}"]
+    n, npsi, nz, nzpsi, nt = [int(v) for v in g[f"{key}_dims"]]
+    s = Shift(n, npsi, nz, nzpsi, key.split("_")[0])
+    c = s.coeff(G("psi"))
+    assert rel_l2(c.cpu().numpy(), R("coeff")) < TOL
+    c = torch.from_numpy(R("coeff")).cuda()   # isolate each operator from coeff's rounding
+    checks = {
+        "S": s.S(c, G("r"), G("m")),
+        "Sadj": s.Sadj(G("g"), G("r"), G("m")),
+        "curlyS": s.curlyS(G("psi"), G("r"), G("m")),
+        "dS": s.dcurlySc(c, G("r"), G("m"), G("c1"), G("d1")),
+        "d2S": s.d2curlySc(c, G("r"), G("m"), G("c1"), G("d1"), G("c2"), G("d2")),
+    }
+    o1, o2 = s.dcurlySadjc(c, G("r"), G("m"), G("g"))
+    checks["dSadj1"], checks["dSadj2"] = o1, o2
+    for k, v in checks.items():
+        v = v.cpu().numpy()
+        assert v.shape == R(k).shape and v.dtype == R(k).dtype, k
+        assert rel_l2(v, R(k)) < TOL, (k, rel_l2(v, R(k)))
+
+
+@pytest.mark.parametrize("mag", [1.0, 0.8, 1.25, 0.0])
+def test_adjoint_and_oracle(mag):
+    from holotomocupy_b200 import Shift
+    n = nz = 96
+    npsi = nzpsi = 128
+    nt = 3
+    rng = np.random.default_rng(int(mag * 100))
+    s = Shift(n, npsi, nz, nzpsi, "complex64")
+    o = O.Shift(n, npsi, nz, nzpsi, "complex64", "complex64")
+    c = (rng.standard_normal((nt, nzpsi, npsi)) + 1j * rng.standard_normal((nt, nzpsi, npsi))).astype("complex64")
+    gimg = (rng.standard_normal((nt, nz, n)) + 1j * rng.standard_normal((nt, nz, n))).astype("complex64")
+    r = rng.uniform(-5, 5, (nt, 2)).astype("float32")
+    m = np.full(nt, mag, "float32")
+    ct, gt = torch.from_numpy(c).cuda(), torch.from_numpy(gimg).cuda()
+    Sc = s.S(ct, torch.from_numpy(r).cuda(), torch.from_numpy(m).cuda())
+    STg = s.Sadj(gt, torch.from_numpy(r).cuda(), torch.from_numpy(m).cuda())
+    assert rel_l2(Sc.cpu().numpy(), o.S(c, r, m)) < TOL
+    assert rel_l2(STg.cpu().numpy(), o.Sadj(gimg, r, m)) < TOL
+    lhs = np.vdot(gimg.astype(np.complex128), Sc.cpu().numpy().astype(np.complex128))
+    rhs = np.vdot(STg.cpu().numpy().astype(np.complex128), c.astype(np.complex128))
+    assert abs(lhs - rhs) / abs(lhs) < 1e-5
+    o1, o2 = s.dcurlySadjc(ct, torch.from_numpy(r).cuda(), torch.from_numpy(m).cuda(), gt)
+    p1, p2 = o.dcurlySadjc(c, r, m, gimg)
+    assert rel_l2(o1.cpu().numpy(), p1) < TOL
+    assert rel_l2(o2.cpu().numpy(), p2) < TOL
+
+
+def test_coeff_large_against_fp64():
+    from holotomocupy_b200 import Shift
+    n = 512
+    rng = np.random.default_rng(1)
+    psi = (rng.standard_normal((2, n, n)) + 1j * rng.standard_normal((2, n, n))).astype("complex64")
+    s = Shift(n, n, n, n, "complex64")
+    o = O.Shift(n, n, n, n, "complex64", "complex128")
+    assert rel_l2(s.coeff(torch.from_numpy(psi).cuda()).cpu().numpy(), o.coeff(psi.astype(np.complex128))) < TOL

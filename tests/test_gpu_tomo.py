@@ -1,0 +1,83 @@
+"""USFFT Radon transform on the GPU against the reference (golden vectors from
+its own tomo.py) and the oracle.  Bound: rel L2 <= 1e-5 against the reference
+and the FP32 oracle; the FP64 oracle is reported with a 1e-4 bound."""
+import numpy as np
+import pytest
+import torch
+
+from conftest import rel_l2
+from oracle import holo_oracle as O
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-5
+
+
+@pytest.mark.parametrize("tag", ["a", "b", "c"])
+def test_R_RT_match_reference(golden, tag):
+    from holotomocupy_b200 import Tomo
+    g = golden("tomo")
+    n, nz = int(g[f"{tag}_n"]), int(g[f"{tag}_nz"])
+    t = Tomo(n, nz, g[f"{tag}_theta"], float(g[f"{tag}_mask_r"]))
+    assert t.pars[0] == int(g[f"{tag}_m"])
+    np.testing.assert_array_equal(t.pars[2].cpu().numpy(), g[f"{tag}_phi"])
+    for src, op, key in [("xc", t.R, "Rxc"), ("yc", t.RT, "RTyc"), ("xf", t.R, "Rxf"), ("yf", t.RT, "RTyf")]:
+        out = op(torch.from_numpy(g[f"{tag}_{src}"]).cuda()).cpu().numpy()
+        ref = g[f"{tag}_{key}"]
+        assert out.shape == ref.shape and out.dtype == ref.dtype
+        assert rel_l2(out, ref) < TOL, (key, rel_l2(out, ref))
+
+
+@pytest.mark.parametrize("n,ntheta,nz", [(128, 180, 3), (256, 96, 2)])
+def test_R_RT_against_oracle(n, ntheta, nz):
+    from holotomocupy_b200 import Tomo
+    rng = np.random.default_rng(n)
+    theta = np.linspace(0, np.pi, ntheta, endpoint=False).astype("float32")
+    t = Tomo(n, nz, theta, 0.9)
+    o32 = O.Tomo(n, nz, theta, 0.9, "complex64")
+    o64 = O.Tomo(n, nz, theta, 0.9, "complex128")
+    x = (rng.standard_normal((nz, n, n)) + 1j * rng.standard_normal((nz, n, n))).astype("complex64")
+    y = (rng.standard_normal((ntheta, nz, n)) + 1j * rng.standard_normal((ntheta, nz, n))).astype("complex64")
+    Rx = t.R(torch.from_numpy(x).cuda()).cpu().numpy()
+    RTy = t.RT(torch.from_numpy(y).cuda()).cpu().numpy()
+    assert rel_l2(Rx, o32.R(x)) < TOL
+    assert rel_l2(RTy, o32.RT(y)) < TOL
+    assert rel_l2(Rx, o64.R(x.astype(np.complex128))) < 1e-4
+    assert rel_l2(RTy, o64.RT(y.astype(np.complex128))) < 1e-4
+
+
+def test_adjoint_float32():
+    """tests/tomo/test_tomo.ipynb cell 15 of the reference, asserted."""
+    from holotomocupy_b200 import Tomo
+    n, nz, ntheta = 256, 16, 1024
+    theta = np.linspace(0, np.pi, ntheta, endpoint=False).astype("float32")
+    t = Tomo(n, nz, theta, 1)
+    rng = np.random.default_rng(42)
+    x = torch.from_numpy(rng.standard_normal((nz, n, n)).astype("float32")).cuda()
+    y = torch.from_numpy(rng.standard_normal((ntheta, nz, n)).astype("float32")).cuda()
+    Rx, RTy = t.R(x), t.RT(y)
+    assert Rx.dtype == torch.float32 and tuple(Rx.shape) == (ntheta, nz, n)
+    lhs = torch.sum(Rx.double() * y.double()).item()
+    rhs = torch.sum(x.double() * RTy.double()).item()
+    assert abs(lhs - rhs) / abs(lhs) < 1e-5
+
+
+def test_fbp_matches_oracle():
+    from holotomocupy_b200 import Tomo
+    n, nz, ntheta = 64, 2, 96
+    theta = np.linspace(0, np.pi, ntheta, endpoint=False).astype("float32")
+    rng = np.random.default_rng(3)
+    d = rng.standard_normal((ntheta, nz, n)).astype("float32")
+    t = Tomo(n, nz, theta, 1)
+    o = O.Tomo(n, nz, theta, 1, "complex128")
+    for f in ("ramp", "shepp", "parzen"):
+        got = t.fbp(torch.from_numpy(d).cuda(), f).cpu().numpy()
+        assert rel_l2(got, o.fbp(d.astype(np.float64), f)) < 1e-5
+    with pytest.raises(ValueError):
+        t.fbp(torch.from_numpy(d).cuda(), "hann")
+
+
+def test_slice_capacity_is_enforced():
+    from holotomocupy_b200 import Tomo
+    t = Tomo(32, 2, np.linspace(0, np.pi, 8, endpoint=False), 0)
+    with pytest.raises(ValueError):
+        t.R(torch.zeros(3, 32, 32, dtype=torch.complex64, device="cuda"))
