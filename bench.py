@@ -192,6 +192,8 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--e2e-iters", type=int, default=4)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile", action="store_true",
+                    help="time the device iterations only (no roofline, e2e or CPU legs): for ncu launch lists")
     a = ap.parse_args()
     if a.warmup < 3:
         a.warmup = 3
@@ -261,10 +263,10 @@ def main():
     value = world * 1e3 / ms
 
     # ---- roofline of the dominant kernel family (the propagator passes)
-    roof = roofline(rec, device)
+    roof = None if a.profile else roofline(rec, device)
 
     # ---- end to end through the public API with pinned host buffers
-    e2e = end_to_end(a, rec, obj_true, prb0, pos0, data, device, barrier, world)
+    e2e = None if a.profile else end_to_end(a, rec, obj_true, prb0, pos0, data, device, barrier, world)
 
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
@@ -279,7 +281,7 @@ def main():
         "e2e": e2e,
         "clocks": clk,
     }
-    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+    if rank == 0 and world == 1 and not (a.no_cpu_baseline or a.profile):
         per_iter, wall, sample = cpu_sample(n, ntheta, ndist, os.cpu_count() or 1)
         line["cpu_baseline"] = {"value": 1.0 / per_iter, "unit": UNIT, "cores": os.cpu_count() or 1, "kind": "port",
                                 "sample": sample, "sample_seconds": wall}

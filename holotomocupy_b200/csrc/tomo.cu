@@ -3,18 +3,24 @@
 //
 // R(obj)[theta, z, :] = crop . IFFT_n . gather_theta . FFT2_2n . embed(obj * phi)
 // with the reference's fftshift-by-sign multiplications folded into the
-// passes:
-//   1. row pass (length 2n) over the n non-zero rows of each padded slice:
-//      embed obj*phi, pre-sign (-1)^(row+col), FFT, post column sign (-1)^kx;
-//   2. column pass (length 2n): only rows n/2..3n/2 are non-zero; FFT, post
-//      row sign (-1)^ky -> the centred spectrum fde[z] (2n x 2n);
-//   3. gather + detector IFFT: for each (theta, z) the n polar samples are
-//      81-tap Gaussian-weighted sums of fde[z] (m = 4 at every supported
-//      size), then sign, IFFT_n, sign, /4, in one kernel.
-// RT runs the exact adjoint: detector FFT with signs; a tiled scatter that
-// accumulates each 32x32 tile of fde in shared memory over the polar samples
-// whose windows reach it (no global atomics); column IFFT keeping only the
-// central rows; row IFFT, crop, * phi.
+// passes.  Slices are processed Z at a time in "Z-interleaved" layouts (the Z
+// samples of consecutive slices stored together), so every spectral access
+// is one Z*8-byte vector and each Gaussian window serves Z slices:
+//   1. row pass (length 2n) over the n non-zero rows of the padded slice:
+//      embed obj*phi, pre-sign (-1)^(row+col), FFT, post column sign (-1)^kx
+//      -> fa  [zb][n][2n][Z];
+//   2. column pass (length 2n, rows outside n/2..3n/2 are zero): FFT, post
+//      row sign (-1)^ky -> the centred spectrum fde [zb][2n][2n][Z];
+//   3. gather + detector IFFT: for each (theta, slice batch) the n polar
+//      samples are 81-tap Gaussian-weighted sums of fde (m = 4 at every
+//      supported size), then sign, IFFT_n, sign, /4.
+// RT runs the exact adjoint: detector FFT with signs -> gs [zb][theta][n][Z];
+// a per-cell gather replaces the reference's atomic scatter: every spectral
+// cell visits only the angles whose line passes within 7.5 cells of it
+// (binary search in the sorted angles) and the few radial samples near it,
+// and re-checks window membership with the forward's own formulas, so R^T is
+// the exact transpose of R and deterministic; then column IFFT keeping the
+// central rows, row IFFT, crop, * phi.
 //
 // Angle cosines and sines come from a table computed in double precision on
 // the host (the reference's __cosf/__sinf error of ~5e-7 moves R by up to
@@ -22,80 +28,40 @@
 #include "lines.cuh"
 #include "holotomo_b200_internal.h"
 
+#include <algorithm>
 #include <cmath>
+#include <numeric>
 #include <vector>
 
 namespace ht {
 
 struct GatherGeom {
   int n, ntheta, m;
-  float coeff0, coeff1;  // pi/mu, -pi^2/mu
-  const float2* cs;      // [ntheta] (cos theta, sin theta)
+  float coeff0, coeff1;   // pi/mu, -pi^2/mu
+  const float2* cs;       // [ntheta] (cos theta, sin theta)
+  const float* th_sorted; // [ntheta] theta mod pi, ascending
+  const int* th_index;    // [ntheta] original index of th_sorted[i]
 };
 
-// ------------------------------------------------------ pass 1: rows (R)
-// obj [nz, n, n] -> fa [nz, n, 2n]
+// Slices per batch for padded size N2 = 2n.
 template <int N2>
-__global__ void __launch_bounds__(RowCfg<N2>::THREADS)
-k_tomo_rows_fwd(const float2* __restrict__ obj, const float* __restrict__ phi, float2* __restrict__ fa,
-                long nrows, const float2* __restrict__ tw4) {
-  constexpr int T = RowCfg<N2>::T;
-  constexpr int n = N2 / 2;
-  extern __shared__ float2 smem[];
-  const int line = threadIdx.x / T, t = threadIdx.x % T;
-  const long row = (long)blockIdx.x * RowCfg<N2>::LINES + line;  // z*n + r
-  const bool valid = row < nrows;
-  SmRow sm{smem + line * SmRow::padded(N2)};
-  const int r = valid ? (int)(row % n) : 0;
-  const int pr = r + n / 2;
-  for (int q = t; q < N2; q += T) {
-    float2 v = make_float2(0.f, 0.f);
-    if (valid && q >= n / 2 && q < 3 * n / 2) {
-      const float2 o = obj[row * n + (q - n / 2)];
-      float s = phi[r * n + (q - n / 2)];
-      if ((pr + q) & 1) s = -s;
-      v = cscale(o, s);
-    }
-    sm.st(q, v);
-  }
-  __syncthreads();
-  fft_line<N2, false>(sm, t, tw4);
-  if (!valid) return;
-  for (int k = t; k < N2; k += T) {
-    float2 v = sm.ld(k);
-    if (k & 1) v = make_float2(-v.x, -v.y);
-    fa[row * N2 + k] = v;
-  }
-}
+struct TZ {
+  static constexpr int Z = (N2 <= 1024) ? 8 : ((N2 == 2048) ? 4 : 2);
+};
 
-// --------------------------------------------------- pass 2: columns (R)
-// fa [nz, n, 2n] -> fde [nz, 2n, 2n]
-template <int N2>
-__global__ void __launch_bounds__(ColCfg<N2>::THREADS)
-k_tomo_cols_fwd(const float2* __restrict__ fa, float2* __restrict__ fde, const float2* __restrict__ tw4) {
-  constexpr int C = ColCfg<N2>::C;
-  constexpr int T = ColCfg<N2>::T;
-  constexpr int n = N2 / 2;
-  extern __shared__ float2 tile[];
-  const int c = threadIdx.x % C, t = threadIdx.x / C;
-  const int col0 = blockIdx.x * C;
-  const long z = blockIdx.y;
-  const float2* src = fa + z * n * N2;
-  for (int idx = threadIdx.x; idx < N2 * C; idx += blockDim.x) {
-    const int pr = idx / C, cc = idx % C;
-    const bool in = pr >= n / 2 && pr < 3 * n / 2 && col0 + cc < N2;
-    tile[idx] = in ? src[(long)(pr - n / 2) * N2 + col0 + cc] : make_float2(0.f, 0.f);
-  }
-  __syncthreads();
-  fft_line<N2, false>(SmCol<C>{tile + c}, t, tw4);
-  float2* dst = fde + z * N2 * N2;
-  for (int idx = threadIdx.x; idx < N2 * C; idx += blockDim.x) {
-    const int ky = idx / C, cc = idx % C;
-    if (col0 + cc >= N2) continue;
-    float2 v = tile[idx];
-    if (ky & 1) v = make_float2(-v.x, -v.y);
-    dst[(long)ky * N2 + col0 + cc] = v;
-  }
+// Z lines of length N per CTA; line stride odd in float2 units so that
+// reading one position of all lines is bank-conflict free.
+template <int N, int Z>
+struct ZCfg {
+  static constexpr int T = Plan<N>::T;
+  static constexpr int THREADS = Z * T;
+  static constexpr int LS = SmRow::padded(N) + 1;
+  static constexpr int SMEM = Z * LS * (int)sizeof(float2);
+};
+
+template <int N, int Z>
+__device__ __forceinline__ SmRow zline(float2* smem, int l) {
+  return SmRow{smem + l * ZCfg<N, Z>::LS};
 }
 
 // ---------------------------------------------- the 9x9 Gaussian window
@@ -103,288 +69,403 @@ k_tomo_cols_fwd(const float2* __restrict__ fa, float2* __restrict__ fde, const f
 // (cuda_kernels.py:22-45).  x0 = (tx - n/2)/n cos(th), y0 = -(tx - n/2)/n sin(th).
 struct Window {
   int bx, by;
-  float ex[9], ey[9];
+  float x0, y0;
 };
 
-__device__ __forceinline__ void make_window(const GatherGeom& G, int tx, float2 cs, Window& w) {
+__device__ __forceinline__ void window_base(const GatherGeom& G, int tx, float2 cs, Window& w) {
   const int n = G.n;
   const float twon = (float)(2 * n);
-  const float inv_twon = 1.0f / twon;
   const float rho = (float)(tx - n / 2) / (float)n;
-  const float x0 = rho * cs.x;
-  const float y0 = -rho * cs.y;
-  w.bx = (int)floorf(twon * x0) - G.m;
-  w.by = (int)floorf(twon * y0) - G.m;
+  w.x0 = rho * cs.x;
+  w.y0 = -rho * cs.y;
+  w.bx = (int)floorf(twon * w.x0) - G.m;
+  w.by = (int)floorf(twon * w.y0) - G.m;
+}
+__device__ __forceinline__ float wx_tap(const GatherGeom& G, const Window& w, int i) {
+  const float inv_twon = 1.0f / (float)(2 * G.n);
+  const float w0 = (float)(w.bx + i) * inv_twon - w.x0;
+  return __expf(G.coeff1 * w0 * w0);
+}
+__device__ __forceinline__ float wy_tap(const GatherGeom& G, const Window& w, int i) {
+  const float inv_twon = 1.0f / (float)(2 * G.n);
+  const float w1 = (float)(w.by + i) * inv_twon - w.y0;
+  return G.coeff0 * __expf(G.coeff1 * w1 * w1);
+}
+
+// acc[l] += w * p[l] for Z complex samples read as Z/2 float4
+template <int Z>
+__device__ __forceinline__ void zload_fma(float2 (&acc)[Z], float w, const float2* __restrict__ p) {
+  const float4* q = reinterpret_cast<const float4*>(p);
 #pragma unroll
-  for (int i = 0; i < 9; ++i) {
-    const float w0 = (float)(w.bx + i) * inv_twon - x0;
-    w.ex[i] = __expf(G.coeff1 * w0 * w0);
-    const float w1 = (float)(w.by + i) * inv_twon - y0;
-    w.ey[i] = G.coeff0 * __expf(G.coeff1 * w1 * w1);
+  for (int i = 0; i < Z / 2; ++i) {
+    const float4 v = __ldg(&q[i]);
+    acc[2 * i].x += w * v.x;
+    acc[2 * i].y += w * v.y;
+    acc[2 * i + 1].x += w * v.z;
+    acc[2 * i + 1].y += w * v.w;
   }
 }
 
-// --------------------------------- pass 3: gather + detector IFFT (R)
-// fde [nz, 2n, 2n] -> sino [ntheta, nz, n]; one line per (theta, z),
-// lines ordered z-major so consecutive CTAs share the same fde slice.
-template <int N>
-__global__ void __launch_bounds__(RowCfg<N>::THREADS)
-k_gather_ifft(const float2* __restrict__ fde, float2* __restrict__ sino, GatherGeom G, int nz,
-              const float2* __restrict__ tw4) {
-  constexpr int T = RowCfg<N>::T;
-  constexpr int twon = 2 * N;
+// ------------------------------------------------------ 1: rows (R)
+// obj [nz, n, n] -> fa [zb][n][2n][Z];  grid (n, nzb)
+template <int N2>
+__global__ void __launch_bounds__(ZCfg<N2, TZ<N2>::Z>::THREADS)
+k_trow_fwd(const float2* __restrict__ obj, const float* __restrict__ phi, float2* __restrict__ fa, int nz,
+           const float2* __restrict__ tw4) {
+  constexpr int Z = TZ<N2>::Z;
+  constexpr int T = ZCfg<N2, Z>::T;
+  constexpr int n = N2 / 2;
   extern __shared__ float2 smem[];
-  const int line = threadIdx.x / T, t = threadIdx.x % T;
-  const long L = (long)blockIdx.x * RowCfg<N>::LINES + line;
-  const bool valid = L < (long)nz * G.ntheta;
-  const int z = valid ? (int)(L / G.ntheta) : 0;
-  const int th = valid ? (int)(L % G.ntheta) : 0;
-  SmRow sm{smem + line * SmRow::padded(N)};
-  const float2 cs = G.cs[th];
-  const float2* f = fde + (long)z * twon * twon;
-  for (int tx = t; tx < N; tx += T) {
-    float2 acc = make_float2(0.f, 0.f);
-    if (valid) {
-      Window w;
-      make_window(G, tx, cs, w);
-#pragma unroll
-      for (int i1 = 0; i1 < 9; ++i1) {
-        const int row = (N + w.by + i1 + twon) % twon;
-        const float2* frow = f + (long)row * twon;
-        float2 ra = make_float2(0.f, 0.f);
-#pragma unroll
-        for (int i0 = 0; i0 < 9; ++i0) {
-          const float2 v = __ldg(&frow[(N + w.bx + i0 + twon) % twon]);
-          ra.x += w.ex[i0] * v.x;
-          ra.y += w.ex[i0] * v.y;
-        }
-        acc.x += w.ey[i1] * ra.x;
-        acc.y += w.ey[i1] * ra.y;
-      }
-      // /n of the gather, (-1)^tx sign before the IFFT
-      const float s = ((tx & 1) ? -1.f : 1.f) / (float)N;
-      acc = cscale(acc, s);
+  const int l = threadIdx.x / T, t = threadIdx.x % T;
+  const int r = blockIdx.x, zb = blockIdx.y;
+  const int z = zb * Z + l;
+  const bool valid = z < nz;
+  const int pr = r + n / 2;
+  SmRow sm = zline<N2, Z>(smem, l);
+  for (int q = t; q < N2; q += T) {
+    float2 v = make_float2(0.f, 0.f);
+    if (valid && q >= n / 2 && q < 3 * n / 2) {
+      float s = phi[r * n + (q - n / 2)];
+      if ((pr + q) & 1) s = -s;
+      v = cscale(obj[((long)z * n + r) * n + (q - n / 2)], s);
     }
-    sm.st(tx, acc);
+    sm.st(q, v);
   }
   __syncthreads();
-  fft_line<N, true>(sm, t, tw4);
-  if (!valid) return;
+  fft_line<N2, false>(sm, t, tw4);
+  float2* dst = fa + ((long)zb * n + r) * N2 * Z;
+  for (int idx = threadIdx.x; idx < N2 * Z; idx += blockDim.x) {
+    const int kx = idx / Z, ll = idx % Z;
+    float2 v = zline<N2, Z>(smem, ll).ld(kx);
+    if (kx & 1) v = make_float2(-v.x, -v.y);
+    dst[idx] = v;
+  }
+}
+
+// --------------------------------------------------- 2: columns (R)
+// fa [zb][n][2n][Z] -> fde [zb][2n][2n][Z];  grid (2n, nzb)
+template <int N2>
+__global__ void __launch_bounds__(ZCfg<N2, TZ<N2>::Z>::THREADS)
+k_tcol_fwd(const float2* __restrict__ fa, float2* __restrict__ fde, const float2* __restrict__ tw4) {
+  constexpr int Z = TZ<N2>::Z;
+  constexpr int T = ZCfg<N2, Z>::T;
+  constexpr int n = N2 / 2;
+  extern __shared__ float2 smem[];
+  const int l = threadIdx.x / T, t = threadIdx.x % T;
+  const int kx = blockIdx.x, zb = blockIdx.y;
+  const float2* src = fa + (long)zb * n * N2 * Z + (long)kx * Z;
+  for (int idx = threadIdx.x; idx < N2 * Z; idx += blockDim.x) {
+    const int pr = idx / Z, ll = idx % Z;
+    const float2 v = (pr >= n / 2 && pr < 3 * n / 2) ? src[(long)(pr - n / 2) * N2 * Z + ll] : make_float2(0.f, 0.f);
+    zline<N2, Z>(smem, ll).st(pr, v);
+  }
+  __syncthreads();
+  fft_line<N2, false>(zline<N2, Z>(smem, l), t, tw4);
+  float2* dst = fde + (long)zb * N2 * N2 * Z + (long)kx * Z;
+  for (int idx = threadIdx.x; idx < N2 * Z; idx += blockDim.x) {
+    const int ky = idx / Z, ll = idx % Z;
+    float2 v = zline<N2, Z>(smem, ll).ld(ky);
+    if (ky & 1) v = make_float2(-v.x, -v.y);
+    dst[(long)ky * N2 * Z + ll] = v;
+  }
+}
+
+// ------------------------------------- 3: gather + detector IFFT (R)
+// fde [zb][2n][2n][Z] -> sino [ntheta, nz, n];  grid (ntheta, nzb)
+template <int N>
+__global__ void __launch_bounds__(ZCfg<N, TZ<2 * N>::Z>::THREADS)
+k_tgather(const float2* __restrict__ fde, float2* __restrict__ sino, GatherGeom G, int nz,
+          const float2* __restrict__ tw4) {
+  constexpr int Z = TZ<2 * N>::Z;
+  constexpr int T = ZCfg<N, Z>::T;
+  constexpr int twon = 2 * N;
+  extern __shared__ float2 smem[];
+  const int th = blockIdx.x, zb = blockIdx.y;
+  const float2 cs = G.cs[th];
+  const float2* f = fde + (long)zb * twon * twon * Z;
+  for (int tx = threadIdx.x; tx < N; tx += blockDim.x) {
+    Window w;
+    window_base(G, tx, cs, w);
+    float ex[9];
+    int cols[9];
+#pragma unroll
+    for (int i = 0; i < 9; ++i) {
+      ex[i] = wx_tap(G, w, i);
+      cols[i] = (N + w.bx + i + twon) % twon;
+    }
+    float2 acc[Z];
+#pragma unroll
+    for (int l = 0; l < Z; ++l) acc[l] = make_float2(0.f, 0.f);
+#pragma unroll
+    for (int i1 = 0; i1 < 9; ++i1) {
+      const int row = (N + w.by + i1 + twon) % twon;
+      const float ey = wy_tap(G, w, i1);
+      const float2* frow = f + (long)row * twon * Z;
+      float2 ra[Z];
+#pragma unroll
+      for (int l = 0; l < Z; ++l) ra[l] = make_float2(0.f, 0.f);
+#pragma unroll
+      for (int i0 = 0; i0 < 9; ++i0) zload_fma<Z>(ra, ex[i0], frow + (long)cols[i0] * Z);
+#pragma unroll
+      for (int l = 0; l < Z; ++l) {
+        acc[l].x += ey * ra[l].x;
+        acc[l].y += ey * ra[l].y;
+      }
+    }
+    // /n of the gather, (-1)^tx before the IFFT
+    const float s = ((tx & 1) ? -1.f : 1.f) / (float)N;
+#pragma unroll
+    for (int l = 0; l < Z; ++l) zline<N, Z>(smem, l).st(tx, cscale(acc[l], s));
+  }
+  __syncthreads();
+  const int l = threadIdx.x / T, t = threadIdx.x % T;
+  fft_line<N, true>(zline<N, Z>(smem, l), t, tw4);
+  const int z = zb * Z + l;
+  if (z >= nz) return;
   float2* dst = sino + ((long)th * nz + z) * N;
+  SmRow sm = zline<N, Z>(smem, l);
   for (int k = t; k < N; k += T) {
-    // ifft 1/n, (-1)^k sign, /4
-    const float s = ((k & 1) ? -1.f : 1.f) / (4.f * (float)N);
+    const float s = ((k & 1) ? -1.f : 1.f) / (4.f * (float)N);  // ifft 1/n, (-1)^k, /4
     dst[k] = cscale(sm.ld(k), s);
   }
 }
 
-// --------------------------------------- RT pass 1: detector FFT rows
-// sino [ntheta, nz, n] -> G [ntheta, nz, n]:  G = c1d * FFT(c1d * sino)
+// ------------------------------------- RT 1: detector FFT with signs
+// sino [ntheta, nz, n] -> gs [zb][ntheta][n][Z];  grid (ntheta, nzb)
 template <int N>
-__global__ void __launch_bounds__(RowCfg<N>::THREADS)
-k_sino_fft(const float2* __restrict__ sino, float2* __restrict__ out, long nrows, const float2* __restrict__ tw4) {
-  constexpr int T = RowCfg<N>::T;
+__global__ void __launch_bounds__(ZCfg<N, TZ<2 * N>::Z>::THREADS)
+k_tsino_fft(const float2* __restrict__ sino, float2* __restrict__ gs, int ntheta, int nz,
+            const float2* __restrict__ tw4) {
+  constexpr int Z = TZ<2 * N>::Z;
+  constexpr int T = ZCfg<N, Z>::T;
   extern __shared__ float2 smem[];
-  const int line = threadIdx.x / T, t = threadIdx.x % T;
-  const long row = (long)blockIdx.x * RowCfg<N>::LINES + line;
-  const bool valid = row < nrows;
-  SmRow sm{smem + line * SmRow::padded(N)};
+  const int l = threadIdx.x / T, t = threadIdx.x % T;
+  const int th = blockIdx.x, zb = blockIdx.y;
+  const int z = zb * Z + l;
+  SmRow sm = zline<N, Z>(smem, l);
   for (int k = t; k < N; k += T) {
-    float2 v = valid ? sino[row * N + k] : make_float2(0.f, 0.f);
+    float2 v = (z < nz) ? sino[((long)th * nz + z) * N + k] : make_float2(0.f, 0.f);
     if (k & 1) v = make_float2(-v.x, -v.y);
     sm.st(k, v);
   }
   __syncthreads();
   fft_line<N, false>(sm, t, tw4);
-  if (!valid) return;
-  for (int k = t; k < N; k += T) {
-    float2 v = sm.ld(k);
-    if (k & 1) v = make_float2(-v.x, -v.y);
-    out[row * N + k] = v;
+  float2* dst = gs + ((long)zb * ntheta + th) * N * Z;
+  for (int idx = threadIdx.x; idx < N * Z; idx += blockDim.x) {
+    const int tx = idx / Z, ll = idx % Z;
+    float2 v = zline<N, Z>(smem, ll).ld(tx);
+    if (tx & 1) v = make_float2(-v.x, -v.y);
+    dst[idx] = v;
   }
 }
 
-// ----------------------------------------- RT pass 2: tiled scatter
-// G [ntheta, nz, n] -> fde [nz, 2n, 2n]; CTA = one TSxTS tile of one slice.
-constexpr int kTile = 32;
-constexpr int kScatterWarps = 8;
+// -------------------------------------------- RT 2: per-cell gather
+// gs [zb][ntheta][n][Z] -> fde [zb][2n][2n][Z];  grid (2n/16, 2n/16, nzb), block 16x16
+constexpr float kLineReach = 7.5f;  // window cells lie within 5 sqrt(2) of the sample centre
 
-__global__ void __launch_bounds__(kScatterWarps * 32)
-k_scatter_tiles(const float2* __restrict__ Gs, float2* __restrict__ fde, GatherGeom G, int nz) {
-  __shared__ float2 acc[kTile * kTile];
+__device__ __forceinline__ int lower_bound_f(const float* a, int n, float v) {
+  int lo = 0, hi = n;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (a[mid] < v)
+      lo = mid + 1;
+    else
+      hi = mid;
+  }
+  return lo;
+}
+
+template <int Z>
+__device__ __forceinline__ void cell_angle(const GatherGeom& G, int j, float px, float py, int X, int Y,
+                                           const float2* __restrict__ g, float2 (&acc)[Z]) {
   const int n = G.n, twon = 2 * n;
-  const int X0 = blockIdx.x * kTile, Y0 = blockIdx.y * kTile;
-  const int z = blockIdx.z;
-  for (int i = threadIdx.x; i < kTile * kTile; i += blockDim.x) acc[i] = make_float2(0.f, 0.f);
-  __syncthreads();
-  const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
-  const float mrg = (float)(G.m + 2);
-  for (int th = warp; th < G.ntheta; th += kScatterWarps) {
-    const float2 cs = G.cs[th];
-    // sample centre in window-base units: cx = 2 rho cos, cy = -2 rho sin, rho = tx - n/2;
-    // grid column X = (n + ell) mod 2n.  Check the 3x3 periodic images.
-    for (int sy = -1; sy <= 1; ++sy) {
-      for (int sx = -1; sx <= 1; ++sx) {
-        const float xlo = (float)(X0 - n + sx * twon) - mrg, xhi = (float)(X0 - n + kTile + sx * twon) + mrg;
-        const float ylo = (float)(Y0 - n + sy * twon) - mrg, yhi = (float)(Y0 - n + kTile + sy * twon) + mrg;
-        float rlo = -(float)(n / 2), rhi = (float)(n / 2);
-        const float c2 = 2.f * cs.x, s2 = -2.f * cs.y;
-        if (fabsf(c2) > 1e-12f) {
-          float a = xlo / c2, b = xhi / c2;
-          rlo = fmaxf(rlo, fminf(a, b));
-          rhi = fminf(rhi, fmaxf(a, b));
-        } else if (xlo > 0.f || xhi < 0.f) {
-          continue;
-        }
-        if (fabsf(s2) > 1e-12f) {
-          float a = ylo / s2, b = yhi / s2;
-          rlo = fmaxf(rlo, fminf(a, b));
-          rhi = fminf(rhi, fmaxf(a, b));
-        } else if (ylo > 0.f || yhi < 0.f) {
-          continue;
-        }
-        if (rlo > rhi) continue;
-        const int t0 = max(0, (int)floorf(rlo) + n / 2 - 1);
-        const int t1 = min(n - 1, (int)ceilf(rhi) + n / 2 + 1);
-        for (int tx = t0 + lane; tx <= t1; tx += 32) {
-          Window w;
-          make_window(G, tx, cs, w);
-          const float2 g = Gs[((long)th * nz + z) * n + tx];
+  const float2 cs = G.cs[j];
+  const float s = px * cs.x - py * cs.y;  // projection onto (cos, -sin)
+  const int t0 = max(0, (int)ceilf((s - kLineReach) * 0.5f) + n / 2);
+  const int t1 = min(n - 1, (int)floorf((s + kLineReach) * 0.5f) + n / 2);
+  for (int tx = t0; tx <= t1; ++tx) {
+    Window w;
+    window_base(G, tx, cs, w);
+    int i0 = (X - n - w.bx) % twon;
+    if (i0 < 0) i0 += twon;
+    if (i0 > 8) continue;
+    int i1 = (Y - n - w.by) % twon;
+    if (i1 < 0) i1 += twon;
+    if (i1 > 8) continue;
+    const float wt = wx_tap(G, w, i0) * wy_tap(G, w, i1);
+    zload_fma<Z>(acc, wt, g + ((long)j * n + tx) * Z);
+  }
+}
+
+template <int Z>
+__global__ void __launch_bounds__(256)
+k_tcell(const float2* __restrict__ gs, float2* __restrict__ fde, GatherGeom G) {
+  const int n = G.n, twon = 2 * n;
+  const int X = blockIdx.x * 16 + threadIdx.x;
+  const int Y = blockIdx.y * 16 + threadIdx.y;
+  const int zb = blockIdx.z;
+  if (X >= twon || Y >= twon) return;
+  const float2* g = gs + (long)zb * G.ntheta * n * Z;
+  float2 acc[Z];
 #pragma unroll
-          for (int i1 = 0; i1 < 9; ++i1) {
-            const int row = (n + w.by + i1 + twon) % twon - Y0;
-            if (row < 0 || row >= kTile) continue;
-#pragma unroll
-            for (int i0 = 0; i0 < 9; ++i0) {
-              const int col = (n + w.bx + i0 + twon) % twon - X0;
-              if (col < 0 || col >= kTile) continue;
-              const float wt = w.ex[i0] * w.ey[i1];
-              atomicAdd(&acc[row * kTile + col].x, wt * g.x);
-              atomicAdd(&acc[row * kTile + col].y, wt * g.y);
-            }
-          }
-        }
+  for (int l = 0; l < Z; ++l) acc[l] = make_float2(0.f, 0.f);
+  const float PI = 3.14159265358979f;
+  const float lim = (float)n + 9.0f;
+  for (int oy = -1; oy <= 1; ++oy) {
+    for (int ox = -1; ox <= 1; ++ox) {
+      // the cell and its periodic images within reach of the sample disc
+      const float px = (float)(X - n + ox * twon), py = (float)(Y - n + oy * twon);
+      if (fabsf(px) > lim || fabsf(py) > lim) continue;
+      const float R = sqrtf(px * px + py * py);
+      if (R <= kLineReach) {
+        for (int j = 0; j < G.ntheta; ++j) cell_angle<Z>(G, j, px, py, X, Y, g, acc);
+        continue;
       }
+      // angles with R |sin(theta + phi)| <= reach, theta taken mod pi
+      const float dlt = asinf(fminf(1.0f, kLineReach / R)) + 1e-4f;
+      float c = -atan2f(py, px);
+      c = c - PI * floorf(c / PI);
+      const float a = c - dlt, b = c + dlt;
+      float ia[2], ib[2];
+      int ni = 0;
+      if (a < 0.f) {
+        ia[ni] = 0.f;
+        ib[ni++] = b;
+        ia[ni] = a + PI;
+        ib[ni++] = PI;
+      } else if (b >= PI) {
+        ia[ni] = a;
+        ib[ni++] = PI;
+        ia[ni] = 0.f;
+        ib[ni++] = b - PI;
+      } else {
+        ia[ni] = a;
+        ib[ni++] = b;
+      }
+      for (int q = 0; q < ni; ++q)
+        for (int i = lower_bound_f(G.th_sorted, G.ntheta, ia[q]); i < G.ntheta && G.th_sorted[i] <= ib[q]; ++i)
+          cell_angle<Z>(G, G.th_index[i], px, py, X, Y, g, acc);
     }
   }
-  __syncthreads();
-  float2* dst = fde + (long)z * twon * twon;
-  for (int i = threadIdx.x; i < kTile * kTile; i += blockDim.x) {
-    const int r = i / kTile, c = i % kTile;
-    if (Y0 + r < twon && X0 + c < twon) dst[(long)(Y0 + r) * twon + X0 + c] = acc[i];
-  }
+  float4* dst = reinterpret_cast<float4*>(fde + (((long)zb * twon + Y) * twon + X) * Z);
+#pragma unroll
+  for (int i = 0; i < Z / 2; ++i)
+    dst[i] = make_float4(acc[2 * i].x, acc[2 * i].y, acc[2 * i + 1].x, acc[2 * i + 1].y);
 }
 
-// ------------------------------------------ RT pass 3: column IFFT
-// fde [nz, 2n, 2n] -> fb [nz, n, 2n] (central rows only)
+// ------------------------------------------- RT 3: column IFFT
+// fde [zb][2n][2n][Z] -> fb [zb][n][2n][Z] (central rows);  grid (2n, nzb)
 template <int N2>
-__global__ void __launch_bounds__(ColCfg<N2>::THREADS)
-k_tomo_cols_adj(const float2* __restrict__ fde, float2* __restrict__ fb, const float2* __restrict__ tw4) {
-  constexpr int C = ColCfg<N2>::C;
-  constexpr int T = ColCfg<N2>::T;
-  constexpr int n = N2 / 2;
-  extern __shared__ float2 tile[];
-  const int c = threadIdx.x % C, t = threadIdx.x / C;
-  const int col0 = blockIdx.x * C;
-  const long z = blockIdx.y;
-  const float2* src = fde + z * N2 * N2;
-  for (int idx = threadIdx.x; idx < N2 * C; idx += blockDim.x) {
-    const int ky = idx / C, cc = idx % C;
-    float2 v = (col0 + cc < N2) ? src[(long)ky * N2 + col0 + cc] : make_float2(0.f, 0.f);
-    if ((ky + col0 + cc) & 1) v = make_float2(-v.x, -v.y);  // pre-sign (-1)^(ky+kx)
-    tile[idx] = v;
-  }
-  __syncthreads();
-  fft_line<N2, true>(SmCol<C>{tile + c}, t, tw4);
-  float2* dst = fb + z * n * N2;
-  const float s = 1.0f / (float)N2;
-  for (int idx = threadIdx.x; idx < n * C; idx += blockDim.x) {
-    const int r = idx / C, cc = idx % C;
-    if (col0 + cc >= N2) continue;
-    const int pr = r + n / 2;
-    float2 v = cscale(tile[pr * C + cc], (pr & 1) ? -s : s);  // post row sign
-    dst[(long)r * N2 + col0 + cc] = v;
-  }
-}
-
-// --------------------------------------------- RT pass 4: row IFFT
-// fb [nz, n, 2n] -> out [nz, n, n] = crop(IFFT) * post column sign * phi
-template <int N2>
-__global__ void __launch_bounds__(RowCfg<N2>::THREADS)
-k_tomo_rows_adj(const float2* __restrict__ fb, const float* __restrict__ phi, float2* __restrict__ out,
-                long nrows, const float2* __restrict__ tw4) {
-  constexpr int T = RowCfg<N2>::T;
+__global__ void __launch_bounds__(ZCfg<N2, TZ<N2>::Z>::THREADS)
+k_tcol_adj(const float2* __restrict__ fde, float2* __restrict__ fb, const float2* __restrict__ tw4) {
+  constexpr int Z = TZ<N2>::Z;
+  constexpr int T = ZCfg<N2, Z>::T;
   constexpr int n = N2 / 2;
   extern __shared__ float2 smem[];
-  const int line = threadIdx.x / T, t = threadIdx.x % T;
-  const long row = (long)blockIdx.x * RowCfg<N2>::LINES + line;
-  const bool valid = row < nrows;
-  SmRow sm{smem + line * SmRow::padded(N2)};
-  for (int k = t; k < N2; k += T) sm.st(k, valid ? fb[row * N2 + k] : make_float2(0.f, 0.f));
+  const int l = threadIdx.x / T, t = threadIdx.x % T;
+  const int kx = blockIdx.x, zb = blockIdx.y;
+  const float2* src = fde + (long)zb * N2 * N2 * Z + (long)kx * Z;
+  for (int idx = threadIdx.x; idx < N2 * Z; idx += blockDim.x) {
+    const int ky = idx / Z, ll = idx % Z;
+    float2 v = src[(long)ky * N2 * Z + ll];
+    if ((ky + kx) & 1) v = make_float2(-v.x, -v.y);  // pre-sign (-1)^(ky+kx)
+    zline<N2, Z>(smem, ll).st(ky, v);
+  }
   __syncthreads();
+  fft_line<N2, true>(zline<N2, Z>(smem, l), t, tw4);
+  float2* dst = fb + (long)zb * n * N2 * Z + (long)kx * Z;
+  const float s = 1.0f / (float)N2;
+  for (int idx = threadIdx.x; idx < n * Z; idx += blockDim.x) {
+    const int r = idx / Z, ll = idx % Z;
+    const int pr = r + n / 2;
+    dst[(long)r * N2 * Z + ll] = cscale(zline<N2, Z>(smem, ll).ld(pr), (pr & 1) ? -s : s);  // post row sign
+  }
+}
+
+// ---------------------------------------------- RT 4: row IFFT
+// fb [zb][n][2n][Z] -> out [nz, n, n] = crop(IFFT) * (-1)^q * phi;  grid (n, nzb)
+template <int N2>
+__global__ void __launch_bounds__(ZCfg<N2, TZ<N2>::Z>::THREADS)
+k_trow_adj(const float2* __restrict__ fb, const float* __restrict__ phi, float2* __restrict__ out, int nz,
+           const float2* __restrict__ tw4) {
+  constexpr int Z = TZ<N2>::Z;
+  constexpr int T = ZCfg<N2, Z>::T;
+  constexpr int n = N2 / 2;
+  extern __shared__ float2 smem[];
+  const int l = threadIdx.x / T, t = threadIdx.x % T;
+  const int r = blockIdx.x, zb = blockIdx.y;
+  const float2* src = fb + ((long)zb * n + r) * N2 * Z;
+  for (int idx = threadIdx.x; idx < N2 * Z; idx += blockDim.x) {
+    const int kx = idx / Z, ll = idx % Z;
+    zline<N2, Z>(smem, ll).st(kx, src[idx]);
+  }
+  __syncthreads();
+  SmRow sm = zline<N2, Z>(smem, l);
   fft_line<N2, true>(sm, t, tw4);
-  if (!valid) return;
-  const int r = (int)(row % n);
+  const int z = zb * Z + l;
+  if (z >= nz) return;
   const float s = 1.0f / (float)N2;
   for (int q = t + n / 2; q < 3 * n / 2; q += T) {
-    // note: loop covers q in [n/2, 3n/2) with stride T
     float ph = phi[r * n + (q - n / 2)] * s;
     if (q & 1) ph = -ph;
-    out[row * n + (q - n / 2)] = cscale(sm.ld(q), ph);
+    out[((long)z * n + r) * n + (q - n / 2)] = cscale(sm.ld(q), ph);
   }
 }
 
 // ================================================================ launch
-#define HT_LAUNCH_ROWS(K, N, nrows, st, ...)                                                 \
-  do {                                                                                        \
-    using CF = RowCfg<N>;                                                                     \
-    cudaError_t _e = allow_smem(K<N>, CF::SMEM);                                              \
-    if (_e != cudaSuccess) return _e;                                                         \
-    const long _g = ((nrows) + CF::LINES - 1) / CF::LINES;                                    \
-    K<N><<<(unsigned)_g, CF::THREADS, CF::SMEM, st>>>(__VA_ARGS__); ::ht::count_launch();                           \
-    return cudaGetLastError();                                                                \
-  } while (0)
+template <int N2>
+static cudaError_t tomo_R_sized(const float2* obj, float2* sino, const float* phi, float2* fa, float2* fde,
+                                const GatherGeom& G, int nz, const float2* tw_n, const float2* tw_2n,
+                                cudaStream_t st) {
+  constexpr int n = N2 / 2;
+  constexpr int Z = TZ<N2>::Z;
+  using C2 = ZCfg<N2, Z>;
+  using C1 = ZCfg<n, Z>;
+  const int nzb = (nz + Z - 1) / Z;
+  cudaError_t e;
+  if ((e = allow_smem(k_trow_fwd<N2>, C2::SMEM)) != cudaSuccess) return e;
+  if ((e = allow_smem(k_tcol_fwd<N2>, C2::SMEM)) != cudaSuccess) return e;
+  if ((e = allow_smem(k_tgather<n>, C1::SMEM)) != cudaSuccess) return e;
+  k_trow_fwd<N2><<<dim3(n, nzb), C2::THREADS, C2::SMEM, st>>>(obj, phi, fa, nz, tw_2n);
+  count_launch();
+  k_tcol_fwd<N2><<<dim3(N2, nzb), C2::THREADS, C2::SMEM, st>>>(fa, fde, tw_2n);
+  count_launch();
+  k_tgather<n><<<dim3(G.ntheta, nzb), C1::THREADS, C1::SMEM, st>>>(fde, sino, G, nz, tw_n);
+  count_launch();
+  return cudaGetLastError();
+}
 
-#define HT_LAUNCH_COLS(K, N, ncols, nimg, st, ...)                                           \
-  do {                                                                                        \
-    using CF = ColCfg<N>;                                                                     \
-    cudaError_t _e = allow_smem(K<N>, CF::SMEM);                                              \
-    if (_e != cudaSuccess) return _e;                                                         \
-    dim3 _g(((ncols) + CF::C - 1) / CF::C, (unsigned)(nimg));                                 \
-    K<N><<<_g, CF::THREADS, CF::SMEM, st>>>(__VA_ARGS__); ::ht::count_launch();                                     \
-    return cudaGetLastError();                                                                \
-  } while (0)
-
 template <int N2>
-static cudaError_t l_rows_fwd(const float2* obj, const float* phi, float2* fa, long nrows, const float2* tw,
-                              cudaStream_t st) {
-  HT_LAUNCH_ROWS(k_tomo_rows_fwd, N2, nrows, st, obj, phi, fa, nrows, tw);
-}
-template <int N2>
-static cudaError_t l_cols_fwd(const float2* fa, float2* fde, int nz, const float2* tw, cudaStream_t st) {
-  HT_LAUNCH_COLS(k_tomo_cols_fwd, N2, N2, nz, st, fa, fde, tw);
-}
-template <int N>
-static cudaError_t l_gather(const float2* fde, float2* sino, const GatherGeom& G, int nz, const float2* tw,
-                            cudaStream_t st) {
-  HT_LAUNCH_ROWS(k_gather_ifft, N, (long)nz * G.ntheta, st, fde, sino, G, nz, tw);
-}
-template <int N>
-static cudaError_t l_sino_fft(const float2* sino, float2* out, long nrows, const float2* tw, cudaStream_t st) {
-  HT_LAUNCH_ROWS(k_sino_fft, N, nrows, st, sino, out, nrows, tw);
-}
-template <int N2>
-static cudaError_t l_cols_adj(const float2* fde, float2* fb, int nz, const float2* tw, cudaStream_t st) {
-  HT_LAUNCH_COLS(k_tomo_cols_adj, N2, N2, nz, st, fde, fb, tw);
-}
-template <int N2>
-static cudaError_t l_rows_adj(const float2* fb, const float* phi, float2* out, long nrows, const float2* tw,
-                              cudaStream_t st) {
-  HT_LAUNCH_ROWS(k_tomo_rows_adj, N2, nrows, st, fb, phi, out, nrows, tw);
+static cudaError_t tomo_RT_sized(const float2* sino, float2* obj, const float* phi, float2* fab, float2* fde,
+                                 float2* gs, const GatherGeom& G, int nz, const float2* tw_n, const float2* tw_2n,
+                                 cudaStream_t st) {
+  constexpr int n = N2 / 2;
+  constexpr int Z = TZ<N2>::Z;
+  using C2 = ZCfg<N2, Z>;
+  using C1 = ZCfg<n, Z>;
+  const int nzb = (nz + Z - 1) / Z;
+  cudaError_t e;
+  if ((e = allow_smem(k_tsino_fft<n>, C1::SMEM)) != cudaSuccess) return e;
+  if ((e = allow_smem(k_tcol_adj<N2>, C2::SMEM)) != cudaSuccess) return e;
+  if ((e = allow_smem(k_trow_adj<N2>, C2::SMEM)) != cudaSuccess) return e;
+  k_tsino_fft<n><<<dim3(G.ntheta, nzb), C1::THREADS, C1::SMEM, st>>>(sino, gs, G.ntheta, nz, tw_n);
+  count_launch();
+  k_tcell<Z><<<dim3((N2 + 15) / 16, (N2 + 15) / 16, nzb), dim3(16, 16), 0, st>>>(gs, fde, G);
+  count_launch();
+  k_tcol_adj<N2><<<dim3(N2, nzb), C2::THREADS, C2::SMEM, st>>>(fde, fab, tw_2n);
+  count_launch();
+  k_trow_adj<N2><<<dim3(n, nzb), C2::THREADS, C2::SMEM, st>>>(fab, phi, obj, nz, tw_2n);
+  count_launch();
+  return cudaGetLastError();
 }
 
 #define HT_TOMO_SIZES(X) X(18, 36) X(24, 48) X(32, 64) X(48, 96) X(64, 128) X(96, 192) X(128, 256) \
   X(192, 384) X(256, 512) X(384, 768) X(512, 1024) X(768, 1536) X(1024, 2048) X(1536, 3072) X(2048, 4096)
+
+static int tomo_Z(int n) {
+  const int N2 = 2 * n;
+  return (N2 <= 1024) ? 8 : ((N2 == 2048) ? 4 : 2);
+}
 
 }  // namespace ht
 
@@ -394,9 +475,11 @@ struct ht_tomo_s {
   float mu;
   float* phi;          // [n, n] deapodisation * mask * norm (the reference's phi)
   float2* cs;          // [ntheta] (cos, sin) of the angles
-  float2* fde;         // workspace [nz, 2n, 2n]
-  float2* fab;         // workspace [nz, n, 2n]
-  float2* gs;          // workspace [ntheta, nz, n]
+  float* th_sorted;    // [ntheta] angles mod pi, ascending
+  int* th_index;       // [ntheta]
+  float2* fde;         // workspace [nzb][2n][2n][Z]
+  float2* fab;         // workspace [nzb][n][2n][Z]
+  float2* gs;          // workspace [nzb][ntheta][n][Z]
   const float2* tw_n;
   const float2* tw_2n;
 };
@@ -410,6 +493,16 @@ static bool tomo_size_ok(int n) {
     default:
       return false;
   }
+}
+
+static void tomo_free(ht_tomo_s* t) {
+  cudaFree(t->phi);
+  cudaFree(t->cs);
+  cudaFree(t->th_sorted);
+  cudaFree(t->th_index);
+  cudaFree(t->fde);
+  cudaFree(t->fab);
+  cudaFree(t->gs);
 }
 
 extern "C" int ht_tomo_create(int n, int nz, int ntheta, const float* theta_host, const float* phi_host,
@@ -437,30 +530,42 @@ extern "C" int ht_tomo_create(int n, int nz, int ntheta, const float* theta_host
   t->mu = (float)mu;
   cudaGetDevice(&t->device);
   std::vector<float2> cs(ntheta);
+  std::vector<float> thm(ntheta);
   for (int i = 0; i < ntheta; ++i) {
     const double th = (double)theta_host[i];
     cs[i] = make_float2((float)std::cos(th), (float)std::sin(th));
+    double r = std::fmod(th, M_PI);
+    if (r < 0) r += M_PI;
+    thm[i] = (float)r;
+    if (thm[i] >= (float)M_PI) thm[i] = 0.f;
   }
+  std::vector<int> idx(ntheta);
+  std::iota(idx.begin(), idx.end(), 0);
+  std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) { return thm[a] < thm[b]; });
+  std::vector<float> ths(ntheta);
+  for (int i = 0; i < ntheta; ++i) ths[i] = thm[idx[i]];
   t->tw_n = twiddle_table(n, t->device);
   t->tw_2n = twiddle_table(2 * n, t->device);
+  const int Z = tomo_Z(n);
+  const size_t nzp = (size_t)((nz + Z - 1) / Z) * Z;
   cudaError_t e = cudaSuccess;
   auto alloc = [&](void** p, size_t b) {
     if (e == cudaSuccess) e = cudaMalloc(p, b);
   };
   alloc((void**)&t->phi, sizeof(float) * n * n);
   alloc((void**)&t->cs, sizeof(float2) * ntheta);
-  alloc((void**)&t->fde, sizeof(float2) * (size_t)nz * 4 * n * n);
-  alloc((void**)&t->fab, sizeof(float2) * (size_t)nz * 2 * n * n);
-  alloc((void**)&t->gs, sizeof(float2) * (size_t)ntheta * nz * n);
+  alloc((void**)&t->th_sorted, sizeof(float) * ntheta);
+  alloc((void**)&t->th_index, sizeof(int) * ntheta);
+  alloc((void**)&t->fde, sizeof(float2) * nzp * 4 * n * n);
+  alloc((void**)&t->fab, sizeof(float2) * nzp * 2 * n * n);
+  alloc((void**)&t->gs, sizeof(float2) * nzp * ntheta * n);
   if (e == cudaSuccess) e = cudaMemcpy(t->phi, phi_host, sizeof(float) * n * n, cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemcpy(t->cs, cs.data(), sizeof(float2) * ntheta, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(t->th_sorted, ths.data(), sizeof(float) * ntheta, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(t->th_index, idx.data(), sizeof(int) * ntheta, cudaMemcpyHostToDevice);
   if (e != cudaSuccess || !t->tw_n || !t->tw_2n) {
     if (e != cudaSuccess) set_error(std::string("ht_tomo_create: ") + cudaGetErrorString(e));
-    cudaFree(t->phi);
-    cudaFree(t->cs);
-    cudaFree(t->fde);
-    cudaFree(t->fab);
-    cudaFree(t->gs);
+    tomo_free(t);
     delete t;
     return kCudaError;
   }
@@ -470,11 +575,7 @@ extern "C" int ht_tomo_create(int n, int nz, int ntheta, const float* theta_host
 
 extern "C" int ht_tomo_destroy(ht_tomo_s* t) {
   if (!t) return ht::kOk;
-  cudaFree(t->phi);
-  cudaFree(t->cs);
-  cudaFree(t->fde);
-  cudaFree(t->fab);
-  cudaFree(t->gs);
+  tomo_free(t);
   delete t;
   return ht::kOk;
 }
@@ -489,49 +590,9 @@ static GatherGeom geom(const ht_tomo_s* t) {
   G.coeff0 = PI / t->mu;
   G.coeff1 = -PI * PI / t->mu;
   G.cs = t->cs;
+  G.th_sorted = t->th_sorted;
+  G.th_index = t->th_index;
   return G;
-}
-
-static cudaError_t tomo_R_impl(ht_tomo_s* t, const float2* obj, float2* sino, int nz, cudaStream_t st) {
-  const GatherGeom G = geom(t);
-  cudaError_t e = cudaErrorInvalidValue;
-  switch (t->n) {
-#define X(A, B)                                                                    \
-  case A:                                                                          \
-    e = l_rows_fwd<B>(obj, t->phi, t->fab, (long)nz * A, t->tw_2n, st);             \
-    if (e == cudaSuccess) e = l_cols_fwd<B>(t->fab, t->fde, nz, t->tw_2n, st);      \
-    if (e == cudaSuccess) e = l_gather<A>(t->fde, sino, G, nz, t->tw_n, st);        \
-    break;
-    HT_TOMO_SIZES(X)
-#undef X
-    default:
-      break;
-  }
-  return e;
-}
-
-static cudaError_t tomo_RT_impl(ht_tomo_s* t, const float2* sino, float2* obj, int nz, cudaStream_t st) {
-  const GatherGeom G = geom(t);
-  const int n = t->n;
-  cudaError_t e = cudaErrorInvalidValue;
-  dim3 sgrid((2 * n + kTile - 1) / kTile, (2 * n + kTile - 1) / kTile, nz);
-  switch (n) {
-#define X(A, B)                                                                          \
-  case A:                                                                                \
-    e = l_sino_fft<A>(sino, t->gs, (long)t->ntheta * nz, t->tw_n, st);                    \
-    if (e == cudaSuccess) {                                                              \
-      k_scatter_tiles<<<sgrid, kScatterWarps * 32, 0, st>>>(t->gs, t->fde, G, nz); ::ht::count_launch();        \
-      e = cudaGetLastError();                                                            \
-    }                                                                                    \
-    if (e == cudaSuccess) e = l_cols_adj<B>(t->fde, t->fab, nz, t->tw_2n, st);            \
-    if (e == cudaSuccess) e = l_rows_adj<B>(t->fab, t->phi, obj, (long)nz * A, t->tw_2n, st); \
-    break;
-    HT_TOMO_SIZES(X)
-#undef X
-    default:
-      break;
-  }
-  return e;
 }
 }  // namespace ht
 
@@ -540,8 +601,21 @@ extern "C" int ht_tomo_R(ht_tomo_s* t, const void* obj, void* sino, int nz, void
   HT_REQUIRE(t && obj && sino, "ht_tomo_R: null pointer");
   HT_REQUIRE(nz >= 0 && nz <= t->nz, "ht_tomo_R: nz exceeds the handle's slice capacity");
   if (nz == 0) return kOk;
-  HT_CHECK_CUDA(tomo_R_impl(t, static_cast<const float2*>(obj), static_cast<float2*>(sino), nz,
-                            static_cast<cudaStream_t>(stream)));
+  const GatherGeom G = geom(t);
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  cudaError_t e = cudaErrorInvalidValue;
+  switch (t->n) {
+#define X(A, B)                                                                                             \
+  case A:                                                                                                   \
+    e = tomo_R_sized<B>(static_cast<const float2*>(obj), static_cast<float2*>(sino), t->phi, t->fab, t->fde, G, \
+                        nz, t->tw_n, t->tw_2n, st);                                                         \
+    break;
+    HT_TOMO_SIZES(X)
+#undef X
+    default:
+      break;
+  }
+  HT_CHECK_CUDA(e);
   return kOk;
 }
 
@@ -550,7 +624,20 @@ extern "C" int ht_tomo_RT(ht_tomo_s* t, const void* sino, void* obj, int nz, voi
   HT_REQUIRE(t && obj && sino, "ht_tomo_RT: null pointer");
   HT_REQUIRE(nz >= 0 && nz <= t->nz, "ht_tomo_RT: nz exceeds the handle's slice capacity");
   if (nz == 0) return kOk;
-  HT_CHECK_CUDA(tomo_RT_impl(t, static_cast<const float2*>(sino), static_cast<float2*>(obj), nz,
-                             static_cast<cudaStream_t>(stream)));
+  const GatherGeom G = geom(t);
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  cudaError_t e = cudaErrorInvalidValue;
+  switch (t->n) {
+#define X(A, B)                                                                                                 \
+  case A:                                                                                                       \
+    e = tomo_RT_sized<B>(static_cast<const float2*>(sino), static_cast<float2*>(obj), t->phi, t->fab, t->fde,    \
+                         t->gs, G, nz, t->tw_n, t->tw_2n, st);                                                  \
+    break;
+    HT_TOMO_SIZES(X)
+#undef X
+    default:
+      break;
+  }
+  HT_CHECK_CUDA(e);
   return kOk;
 }

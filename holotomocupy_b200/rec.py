@@ -374,21 +374,29 @@ class Rec:
 
     # ====================== cascade functions, operator by operator
     # (rec_mpi.py:517-813; used for derivative checks, not by BH())
+    # F0 and its derivatives are scalar reductions: evaluated in float64
+    @staticmethod
+    def _d64(*a):
+        return [None if v is None else (v.to(torch.complex128) if v.is_complex() else v.double()) for v in a]
+
     def F0(self, x, d):
+        x, d = self._d64(x, d)
         t = torch.abs(x) - d
-        return float(torch.sum((t * t).double())) / self.data_size
+        return float(torch.sum(t * t)) / self.data_size
 
     def dF0(self, x, y, d, return_x=False):
+        x, y, d = self._d64(x, y, d)
         return 2 / self.data_size * redot(x - d * (x / torch.abs(x)), y)
 
     def d2F_dF0(self, x, y, z, w, d):
+        x, y, z, w, d = self._d64(x, y, z, w, d)
         absval = torch.abs(x)
         l0 = x / absval
         d0 = d / absval
         v = (1 - d0) * reprod(y, z) + d0 * reprod(l0, y) * reprod(l0, z)
         if w is not None:
             v = v + reprod(x - d * l0, w)
-        return 2 / self.data_size * float(torch.sum(v.double()))
+        return 2 / self.data_size * float(torch.sum(v))
 
     def gF0(self, x, y):
         for i in range(1, 4)[::-1]:
