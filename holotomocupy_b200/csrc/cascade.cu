@@ -832,3 +832,4 @@ extern "C" int ht_rec_hessian(ht_rec_s* r, const void* c, const float* pos, cons
   HT_CHECK_CUDA(cudaGetLastError());
   return kOk;
 }
+

@@ -135,14 +135,15 @@ int ht_rec_destroy(ht_rec_s* r);
 
 /* Forward model.  With amp != NULL: amp[ntheta, ndist, nz, n] = |x0|
  * (gen_sqrt_data, rec_mpi.py:882-897).  Otherwise *fval (device double) =
- * 1/N sum (|x0| - data)^2 (F0 of min, rec_mpi.py:517-527, 815-835). */
+ * sum (|x0| - data)^2; divided by N = ntheta*ndist*nz*n it is F0 of min
+ * (rec_mpi.py:517-527, 815-835). */
 int ht_rec_forward(ht_rec_s* r, const void* c, const float* pos, const float* mag, const void* prb, const float* data,
                    float* amp, double* fval, void* stream);
 
 /* Gradient of the data term (gF0..gF3, rec_mpi.py:327-353, 562-813), unscaled:
  * gc [ntheta, nzobj, nobj] = sum_k S_k^T(Y22) (apply coeff() for the proj
  * gradient), gpos [ntheta, ndist, 2] float32, gprb [ndist, nz, n] complex64,
- * *fval (device double) = the objective at the same point. */
+ * *fval (device double) = sum (|x0| - data)^2 at the same point. */
 int ht_rec_gradient(ht_rec_s* r, const void* c, const float* pos, const float* mag, const void* prb,
                     const float* data, void* gc, float* gpos, void* gprb, double* fval, void* stream);
 

@@ -164,8 +164,9 @@ def test_taylor_orders():
                          lambda l: rec.d2F_dF1(x1, sc(l), sc(l), [None, None]), L)
     assert 3.0 < e2[0] / e2[1] < 5.0 and e3[0] < 1e-5 * e1[0]
     # F0
-    data = torch.abs(rf((ntheta, ndist, n, n))) + 0.1
-    x0, dx0 = rc((ntheta, ndist, n, n)), rc((ntheta, ndist, n, n), 0.1)
+    # F0 is a reduction evaluated in float64: build the perturbed points in float64 too
+    data = (torch.abs(rf((ntheta, ndist, n, n))) + 0.1).double()
+    x0, dx0 = rc((ntheta, ndist, n, n)).to(torch.complex128), rc((ntheta, ndist, n, n), 0.1).to(torch.complex128)
     e1, e2, e3 = _taylor(rec.F0(x0, data), lambda l: rec.F0(x0 + l * dx0, data),
                          lambda l: rec.dF0(x0, l * dx0, data), lambda l: rec.d2F_dF0(x0, l * dx0, l * dx0, None, data), L)
     assert 3.0 < e2[0] / e2[1] < 5.0 and 6.0 < e3[0] / e3[1] < 10.0
