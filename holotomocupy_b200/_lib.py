@@ -42,6 +42,7 @@ SIGNATURES = {
     "ht_rec_destroy": [_vp],
     "ht_rec_forward": [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
     "ht_rec_gradient": [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
+    "ht_rec_objective_noalloc": [_vp, _c_int, _c_int, _c_int, _c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
     "ht_rec_hessian": [_vp, _vp, _vp, _vp, _vp, _vp, _c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
 }
 _RESTYPE = {"ht_last_error": ctypes.c_char_p, "ht_launch_count": ctypes.c_long}

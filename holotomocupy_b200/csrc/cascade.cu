@@ -30,6 +30,9 @@
 #include "dct.cuh"
 #include "holotomo_b200_internal.h"
 
+#include <algorithm>
+#include <mutex>
+#include <string>
 #include <vector>
 
 namespace ht {
@@ -833,3 +836,121 @@ extern "C" int ht_rec_hessian(ht_rec_s* r, const void* c, const float* pos, cons
   return kOk;
 }
 
+// ====================================== objective without allocation
+// For callers that cannot allocate device memory: their memory belongs to
+// another allocator (a framework's caching pool, a serving loop with a fixed
+// budget), or they must not call cudaMalloc/cudaFree because those calls can
+// synchronise the whole device and stall other streams.  The scratch of this
+// entry point is one file-scope device array of kNoAllocBytes, which every
+// GPU that loads the library keeps until the process exits.
+namespace ht {
+constexpr size_t kNoAllocBytes = (size_t)32 << 20;  // 32 MiB
+constexpr size_t kNoAllocAccBytes = 256;             // accumulators at the start
+}  // namespace ht
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[ht::kNoAllocBytes];
+
+namespace ht {
+namespace {
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mutex;
+unsigned char* g_noalloc_ptr[kMaxDevices] = {};
+
+// Device address of the scratch array on the current device (looked up once
+// per device; host code cannot use the array's name as a device address).
+unsigned char* noalloc_scratch(int device) {
+  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+  if (device < 0 || device >= kMaxDevices) return nullptr;
+  if (!g_noalloc_ptr[device]) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) {
+      set_error(std::string("ht_rec_objective_noalloc: cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+      return nullptr;
+    }
+    g_noalloc_ptr[device] = static_cast<unsigned char*>(p);
+  }
+  return g_noalloc_ptr[device];
+}
+}  // namespace
+
+template <int N, class T>
+static cudaError_t noalloc_chunks(const ht_prop_s* prop, int nz, int nobj, int nzobj, int ndist, int ntheta,
+                                  int per_chunk, const T* c, const float* pos, const float* mag, const float2* prb,
+                                  const float* data, double* acc, float2* tmp, cudaStream_t st) {
+  const float2 *hw, *twn, *twz;
+  prop_tables(prop, &hw, &twn, &twz);
+  using CF = RowCfg<N>;
+  cudaError_t e = allow_smem(k_casc_fwd<N, T>, CF::SMEM);
+  const int smr = CF::SMEM + CF::THREADS * (int)sizeof(double);
+  if (e == cudaSuccess) e = allow_smem(k_casc_resid<N, 1>, smr);
+  for (int th0 = 0; th0 < ntheta && e == cudaSuccess; th0 += per_chunk) {
+    const int nt = std::min(per_chunk, ntheta - th0);
+    const CascDims D{N, nz, nobj, nzobj, ndist, (long)nt * ndist};
+    const long nrows = D.nimg * nz;
+    k_casc_fwd<N, T><<<HT_ROWS_GRID(N, nrows), CF::THREADS, CF::SMEM, st>>>(
+        c + (long)th0 * nzobj * nobj, pos + (long)th0 * ndist * 2, mag + (long)th0 * ndist, prb, tmp, D, twn);
+    count_launch();
+    if ((e = cudaGetLastError()) != cudaSuccess) break;
+    if ((e = dct_cols(nz, false, tmp, D.nimg, N, hw, ndist, twz, st)) != cudaSuccess) break;
+    k_casc_resid<N, 1><<<HT_ROWS_GRID(N, nrows), CF::THREADS, smr, st>>>(
+        tmp, nullptr, data + (long)th0 * ndist * nz * N, nullptr, acc, 0.f, D, twn);
+    count_launch();
+    e = cudaGetLastError();
+  }
+  return e;
+}
+}  // namespace ht
+
+extern "C" int ht_rec_objective_noalloc(ht_prop_s* prop, int nobj, int nzobj, int ntheta, int is_complex,
+                                        const void* c, const float* pos, const float* mag, const void* prb,
+                                        const float* data, double* fval, void* stream) {
+  using namespace ht;
+  HT_REQUIRE(prop && c && pos && mag && prb && data && fval, "ht_rec_objective_noalloc: null pointer");
+  HT_REQUIRE(nobj > 0 && nzobj > 0 && ntheta > 0, "ht_rec_objective_noalloc: sizes must be positive");
+  int n, nz, ndist;
+  prop_dims(prop, &n, &nz, &ndist);
+  bool n_ok = false;
+#define X(S) n_ok = n_ok || (n == S);
+  HT_REC_SIZES(X)
+#undef X
+  if (!n_ok) {
+    set_error("ht_rec_objective_noalloc: n must be one of 32, 64, 128, 256, 384, 512, 768, 1024, 2048");
+    return kUnsupported;
+  }
+  const size_t per_angle = sizeof(float2) * (size_t)ndist * nz * n;
+  const size_t room = kNoAllocBytes - kNoAllocAccBytes;
+  if (per_angle > room) {
+    set_error("ht_rec_objective_noalloc: one angle needs " + std::to_string(per_angle) +
+              " bytes of scratch (ndist*nz*n*8); the fixed scratch holds " + std::to_string(room) +
+              " bytes (32 MiB minus 256)");
+    return kBadArgument;
+  }
+  int device = 0;
+  HT_CHECK_CUDA(cudaGetDevice(&device));
+  unsigned char* base = noalloc_scratch(device);
+  if (!base) return kCudaError;
+  double* acc = reinterpret_cast<double*>(base);
+  float2* tmp = reinterpret_cast<float2*>(base + kNoAllocAccBytes);
+  const int per_chunk = (int)std::min<size_t>(room / per_angle, (size_t)ntheta);
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  // the array keeps the previous call's contents: clear the accumulators
+  HT_CHECK_CUDA(cudaMemsetAsync(acc, 0, kNoAllocAccBytes, st));
+  cudaError_t e = cudaErrorInvalidValue;
+  switch (n) {
+#define X(S)                                                                                                      \
+  case S:                                                                                                         \
+    e = is_complex ? noalloc_chunks<S, float2>(prop, nz, nobj, nzobj, ndist, ntheta, per_chunk, (const float2*)c, \
+                                               pos, mag, (const float2*)prb, data, acc, tmp, st)                  \
+                   : noalloc_chunks<S, float>(prop, nz, nobj, nzobj, ndist, ntheta, per_chunk, (const float*)c,   \
+                                              pos, mag, (const float2*)prb, data, acc, tmp, st);                  \
+    break;
+    HT_REC_SIZES(X)
+#undef X
+    default:
+      break;
+  }
+  HT_CHECK_CUDA(e);
+  HT_CHECK_CUDA(cudaMemcpyAsync(fval, acc + kF, sizeof(double), cudaMemcpyDeviceToDevice, st));
+  return kOk;
+}

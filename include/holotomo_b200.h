@@ -168,6 +168,21 @@ int ht_axpby(void* x, const void* y, float a, float b, long n, double* dot, void
 /* *dot += sum(x * y) (device double). */
 int ht_dot(const void* x, const void* y, long n, double* dot, void* stream);
 
+/* The objective sum (|x0| - data)^2 of ht_rec_forward, without allocating.
+ * No counterpart in the reference.  For callers that cannot allocate device
+ * memory (their memory belongs to another allocator, or they must not call
+ * cudaMalloc/cudaFree because those can synchronise the device): needs only
+ * the propagator handle (created once at set-up) and the inputs, and works
+ * in one fixed 32 MiB device array that every GPU loading the library holds
+ * until exit.  Angles are processed in chunks that fit it; one angle needs
+ * ndist*nz*n*8 bytes, and larger sizes are rejected (status 1).  The first
+ * call on a device looks up the array's device address: make it before any
+ * stream capture.  All calls share the array, so calls that overlap on the
+ * GPU race; run them in one stream. */
+int ht_rec_objective_noalloc(ht_prop_s* prop, int nobj, int nzobj, int ntheta, int is_complex, const void* c,
+                             const float* pos, const float* mag, const void* prb, const float* data, double* fval,
+                             void* stream);
+
 /* Row filter: out[r] = IFFT(sym * FFT(in[r])) for each of nrows rows of
  * length N (complex64); sym: device float32 [N] in FFT order, carrying the
  * 1/N of the inverse transform.  Serves Tomo._filter_sino
