@@ -10,6 +10,15 @@ One JSON line on stdout (rank 0).  Under torchrun (N > 1) every rank runs an
 independent reconstruction (the solver does not shard across GPUs: replicas
 only) and `value` is the sum over ranks; time is the max over ranks.
 
+`value` is the served form of one reconstruction: device-side step sizes
+and the iteration replayed from a CUDA graph.  `plain` is the same
+reconstruction iterated the reference's way (step sizes on the host, one
+round trip per iteration).  `served` runs a mixed stream of requests
+(grid n in {128, 256, 384, 512} with probabilities 0.4/0.3/0.2/0.1,
+1.75 n angles, 4 distances, Poisson arrivals at 2/s, 16 iterations each)
+through the continuous-batching server and, on the same requests, one at a
+time through the plain path, with p50/p99 per-iteration latencies.
+
 `--impl reference` times the reference algorithm's CPU implementation (the
 NumPy port in oracle/, FP32, all host cores) on a bounded sample of the same
 workload: the per-angle BH cascades (one gradient and three Hessian cascades,
@@ -192,6 +201,8 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--e2e-iters", type=int, default=4)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--serve-requests", type=int, default=12, help="requests in the mixed served stream (0: skip)")
+    ap.add_argument("--serve-iters", type=int, default=16)
     ap.add_argument("--profile", action="store_true",
                     help="time the device iterations only (no roofline, e2e or CPU legs): for ncu launch lists")
     a = ap.parse_args()
@@ -224,41 +235,69 @@ def main():
         if world > 1:
             dist.barrier()
 
-    # ---- device-resident iterations
+    # ---- the plain path: host step sizes, one round trip per iteration
     reset_state(rec, prb0, pos0)
     rec.bh_setup()
     it = 0
     for _ in range(a.warmup):
         rec.bh_iteration(it)
         it += 1
+    torch.cuda.synchronize()
+    st = torch.cuda.current_stream()
+    lat_plain = []
+    l0 = _lib.lib().ht_launch_count()
+    p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    p0.record(st)
+    for _ in range(a.steps):
+        s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s0.record(st)
+        rec.bh_iteration(it)
+        s1.record(st)
+        lat_plain.append((s0, s1))
+        it += 1
+    p1.record(st)
+    torch.cuda.synchronize()
+    launches = (_lib.lib().ht_launch_count() - l0) / a.steps
+    ms_plain = p0.elapsed_time(p1) / a.steps
+    lat_plain = sorted(s.elapsed_time(e) for s, e in lat_plain)
+    rec.bh_finish()
+
+    # ---- the served form: device step sizes, graph-replayed iterations
+    sst = torch.cuda.Stream(device=device)
+    with torch.cuda.stream(sst):
+        reset_state(rec, prb0, pos0)
+        rec.bh_setup()
+        rec.bh_iteration(0, sync=False)
+        rec.capture_iteration()
+        for _ in range(a.warmup - 1):
+            rec.replay_iteration()
+    torch.cuda.synchronize()
     barrier()
     torch.cuda.synchronize()
     clocks = ClockSampler(local)
     clocks.start()
-    st = torch.cuda.current_stream()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     lat = []
-    l0 = _lib.lib().ht_launch_count()
-    e0.record(st)
-    for _ in range(a.steps):
-        s0 = torch.cuda.Event(enable_timing=True)
-        s1 = torch.cuda.Event(enable_timing=True)
-        s0.record(st)
-        rec.bh_iteration(it)
-        s1.record(st)
-        lat.append((s0, s1))
-        it += 1
-    e1.record(st)
+    with torch.cuda.stream(sst):
+        e0.record(sst)
+        for _ in range(a.steps):
+            s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s0.record(sst)
+            rec.replay_iteration()
+            s1.record(sst)
+            lat.append((s0, s1))
+        e1.record(sst)
     torch.cuda.synchronize()
-    launches = (_lib.lib().ht_launch_count() - l0) / a.steps
     barrier()
     clk = clocks.stop()
     ms = e0.elapsed_time(e1) / a.steps
     per_lat = sorted(s.elapsed_time(e) for s, e in lat)
     if world > 1:
-        t = torch.tensor([ms], device=device)
+        t = torch.tensor([ms, ms_plain], device=device)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t)
+        ms, ms_plain = float(t[0]), float(t[1])
+    with torch.cuda.stream(sst):
+        rec.release_graph()
     rec.bh_finish()
     value = world * 1e3 / ms
 
@@ -268,14 +307,28 @@ def main():
     # ---- end to end through the public API with pinned host buffers
     e2e = None if a.profile else end_to_end(a, rec, obj_true, prb0, pos0, data, device, barrier, world)
 
+    # ---- mixed served stream vs the same requests one at a time
+    served = None
+    if a.serve_requests > 0 and not a.profile:
+        del rec, data, obj_true, prb_true, pos_true
+        torch.cuda.synchronize()
+        torch.cuda.empty_cache()
+        served = served_vs_plain(a.serve_requests, a.serve_iters, 4321 + rank)
+
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
         "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c64",
         "data": "synthetic (seeded ellipsoid phantom, random probe and positions, Poisson noise at 1e4 photons)",
         "config": {"workload": f"one BH iteration, {n}^3 object, {ntheta} angles, {ndist} distances, {n}^2 detector",
                    "n": n, "ntheta": ntheta, "ndist": ndist, "parallelism": f"replicas x{world}",
-                   "l2": "inputs larger than L2 (state ~50 GB)", "latency_ms_p50": float(np.percentile(per_lat, 50)),
+                   "form": "served: device step sizes, iteration replayed from a CUDA graph",
+                   "l2": "inputs larger than L2 (state ~60 GB)", "latency_ms_p50": float(np.percentile(per_lat, 50)),
                    "latency_ms_p99": float(np.percentile(per_lat, 99))},
+        "plain": {"value": world * 1e3 / ms_plain, "unit": UNIT, "ms_per_step": ms_plain,
+                  "latency_ms_p50": float(np.percentile(lat_plain, 50)),
+                  "latency_ms_p99": float(np.percentile(lat_plain, 99)),
+                  "form": "host step sizes (H and dots copied to the host each iteration), eager launches"},
+        "served": served,
         "gpu_launches": launches,
         "roofline": roof,
         "e2e": e2e,
@@ -289,6 +342,41 @@ def main():
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()
+
+
+def served_vs_plain(nreq, niter, seed):
+    """The mixed request stream through the server and one at a time."""
+    import torch
+    from holotomocupy_b200.serving import Request, Server, run_plain
+    from holotomocupy_b200.synthetic import make_problem
+    rng = np.random.default_rng(seed)
+    sizes = rng.choice([128, 256, 384, 512], size=nreq, p=[0.4, 0.3, 0.2, 0.1])
+    arrivals = np.cumsum(rng.exponential(0.5, nreq))
+    arrivals -= arrivals[0]
+    reqs = []
+    for rid, (n, t) in enumerate(zip(sizes, arrivals)):
+        args, data, prb0, pos0, _ = make_problem(int(n), int(round(1.75 * n)), 4, seed + 10 * rid, host=True)
+        reqs.append(Request(rid=rid, args=args, data=data, prb0=prb0, pos0=pos0, niter=niter, arrival=float(t)))
+        torch.cuda.synchronize()
+        torch.cuda.empty_cache()
+    total = nreq * niter
+    wall_p, lat_p, _ = run_plain(reqs, realtime=True)
+    torch.cuda.empty_cache()
+    for r in reqs:
+        r.latencies_ms = []
+    srv = Server(max_active=8)
+    for r in reqs:
+        srv.submit(r)
+    srv.run(realtime=True)
+    st = Server.latency_stats(reqs)
+    return {"workload": f"{nreq} requests, n from {{128,256,384,512}} (p 0.4/0.3/0.2/0.1), 1.75 n angles, "
+                        f"4 distances, Poisson arrivals at 2/s, {niter} BH iterations each",
+            "sizes": [int(x) for x in sizes], "iterations": total,
+            "served_iters_per_s": total / srv.wall, "plain_iters_per_s": total / wall_p,
+            "served_wall_s": srv.wall, "plain_wall_s": wall_p,
+            "served_p50_ms": st["p50_ms"], "served_p99_ms": st["p99_ms"],
+            "plain_p50_ms": float(np.percentile(lat_p, 50)), "plain_p99_ms": float(np.percentile(lat_p, 99)),
+            "max_concurrent": srv.max_concurrent, "peak_bytes_admitted": srv.peak_bytes}
 
 
 def roofline(rec, device):
@@ -353,7 +441,7 @@ def end_to_end(a, rec, obj_true, prb0, pos0, data, device, barrier, world):
         rec.vars["obj"].copy_(h_obj, non_blocking=True)
         rec.vars["prb"].copy_(h_prb, non_blocking=True)
         rec.vars["pos"].copy_(h_pos, non_blocking=True)
-        rec.BH(niter=a.e2e_iters)
+        rec.BH(niter=a.e2e_iters, mode="graph")
         out_obj.copy_(rec.vars["obj"], non_blocking=True)
         out_prb.copy_(rec.vars["prb"], non_blocking=True)
         out_pos.copy_(rec.vars["pos"], non_blocking=True)
@@ -364,8 +452,8 @@ def end_to_end(a, rec, obj_true, prb0, pos0, data, device, barrier, world):
     ms = float(np.mean(times))
     return {"value": world * a.e2e_iters * 1e3 / ms, "unit": UNIT, "h2d_bytes_per_step": h2d,
             "d2h_bytes_per_step": d2h, "iterations_per_step": a.e2e_iters, "ms_per_step": ms,
-            "step": "upload data + initial obj/prb/pos from pinned host memory, Rec.BH with the iterations, "
-                    "download obj/prb/pos"}
+            "step": "upload data + initial obj/prb/pos from pinned host memory, Rec.BH(mode='graph') with the "
+                    "iterations, download obj/prb/pos"}
 
 
 if __name__ == "__main__":

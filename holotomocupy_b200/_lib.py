@@ -38,6 +38,12 @@ SIGNATURES = {
     "ht_filter_rows": [_c_int, _vp, _vp, _c_long, _vp, _vp],
     "ht_axpby": [_vp, _vp, _c_float, _c_float, _c_long, _vp, _vp],
     "ht_dot": [_vp, _vp, _c_long, _vp, _vp],
+    "ht_axpby_dev": [_vp, _vp, _vp, _c_float, _vp, _c_float, _c_long, _vp, _vp],
+    "ht_bh_scalars": [_vp, _vp, _c_int, _c_int, _c_double, _c_double, _c_double, _vp, _vp, _c_int, _vp, _vp],
+    "ht_graph_begin": [_vp],
+    "ht_graph_end": [_vp, ctypes.POINTER(_vp)],
+    "ht_graph_launch": [_vp, _vp],
+    "ht_graph_destroy": [_vp],
     "ht_rec_create": [_c_int, _c_int, _c_int, _c_int, _c_int, _c_int, _c_int, _vp, ctypes.POINTER(_vp)],
     "ht_rec_destroy": [_vp],
     "ht_rec_forward": [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],

@@ -1,4 +1,5 @@
-// Library-wide entry points: version and last-error message.
+// Library-wide entry points: version, last-error message, launch counter and
+// CUDA-graph capture of a stream's work.
 #include "common.cuh"
 #include "holotomo_b200_internal.h"
 
@@ -7,3 +8,35 @@ extern "C" int ht_version(void) { return 100; }
 extern "C" const char* ht_last_error(void) { return ht::last_error(); }
 
 extern "C" long ht_launch_count(void) { return ht::launch_count(); }
+
+// ------------------------------------------------------------ graphs
+// Record the work issued to `stream` (by this thread) until ht_graph_end into
+// a graph, instead of running it.
+extern "C" int ht_graph_begin(void* stream) {
+  HT_REQUIRE(stream, "ht_graph_begin: capture needs a non-default stream");
+  HT_CHECK_CUDA(cudaStreamBeginCapture(static_cast<cudaStream_t>(stream), cudaStreamCaptureModeThreadLocal));
+  return ht::kOk;
+}
+
+extern "C" int ht_graph_end(void* stream, void** exec) {
+  HT_REQUIRE(stream && exec, "ht_graph_end: null pointer");
+  cudaGraph_t g = nullptr;
+  HT_CHECK_CUDA(cudaStreamEndCapture(static_cast<cudaStream_t>(stream), &g));
+  cudaGraphExec_t ex = nullptr;
+  const cudaError_t e = cudaGraphInstantiate(&ex, g, 0);
+  cudaGraphDestroy(g);
+  HT_CHECK_CUDA(e);
+  *exec = ex;
+  return ht::kOk;
+}
+
+extern "C" int ht_graph_launch(void* exec, void* stream) {
+  HT_REQUIRE(exec, "ht_graph_launch: null graph");
+  HT_CHECK_CUDA(cudaGraphLaunch(static_cast<cudaGraphExec_t>(exec), static_cast<cudaStream_t>(stream)));
+  return ht::kOk;
+}
+
+extern "C" int ht_graph_destroy(void* exec) {
+  if (exec) HT_CHECK_CUDA(cudaGraphExecDestroy(static_cast<cudaGraphExec_t>(exec)));
+  return ht::kOk;
+}

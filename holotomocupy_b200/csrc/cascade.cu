@@ -38,23 +38,40 @@
 namespace ht {
 
 // -------------------------------------------------------------- basics
-__device__ __forceinline__ float bsp0(float t) {
-  if (-2.0f < t && t <= -1.0f) return (t + 2.0f) * (t + 2.0f) * (t + 2.0f);
-  if (-1.0f < t && t <= 1.0f) return 4.0f - 6.0f * t * t + 3.0f * fabsf(t) * t * t;
-  if (1.0f < t && t <= 2.0f) return (2.0f - t) * (2.0f - t) * (2.0f - t);
-  return 0.0f;
+// Cubic B-spline weights of the four taps j = 0..3 of a sample whose
+// fractional offset is d in [0, 1): the reference's piecewise kernels
+// (cuda_kernels.py:8-60) evaluated at t = d + 1, d, d - 1, d - 2, with the
+// branch of each tap fixed (e = 1 - d).
+__device__ __forceinline__ void bw0(float d, float (&w)[4]) {
+  const float e = 1.0f - d, d2 = d * d, e2 = e * e;
+  w[0] = e2 * e;
+  w[1] = 4.0f - 6.0f * d2 + 3.0f * d2 * d;
+  w[2] = 4.0f - 6.0f * e2 + 3.0f * e2 * e;
+  w[3] = d2 * d;
 }
-__device__ __forceinline__ float bsp1(float t) {
-  if (-2.0f < t && t <= -1.0f) return 3.0f * (t + 2.0f) * (t + 2.0f);
-  if (-1.0f < t && t <= 1.0f) return -12.0f * t + 9.0f * fabsf(t) * t;
-  if (1.0f < t && t <= 2.0f) return -3.0f * (2.0f - t) * (2.0f - t);
-  return 0.0f;
+__device__ __forceinline__ void bw1(float d, float (&w)[4]) {
+  const float e = 1.0f - d;
+  w[0] = -3.0f * e * e;
+  w[1] = -12.0f * d + 9.0f * d * d;
+  w[2] = 12.0f * e - 9.0f * e * e;
+  w[3] = 3.0f * d * d;
 }
-__device__ __forceinline__ float bsp2(float t) {
-  if (-2.0f < t && t <= -1.0f) return 6.0f * (t + 2.0f);
-  if (-1.0f < t && t <= 1.0f) return -12.0f + 18.0f * fabsf(t);
-  if (1.0f < t && t <= 2.0f) return 6.0f * (2.0f - t);
-  return 0.0f;
+__device__ __forceinline__ void bw2(float d, float (&w)[4]) {
+  const float e = 1.0f - d;
+  w[0] = 6.0f * e;
+  w[1] = -12.0f + 18.0f * d;
+  w[2] = -12.0f + 18.0f * e;
+  w[3] = 6.0f * d;
+}
+// weight of tap j alone
+__device__ __forceinline__ float bw0_tap(float d, int j) {
+  const float e = 1.0f - d;
+  switch (j) {
+    case 0: return e * e * e;
+    case 1: return 4.0f - 6.0f * d * d + 3.0f * d * d * d;
+    case 2: return 4.0f - 6.0f * e * e + 3.0f * e * e * e;
+    default: return d * d * d;
+  }
 }
 
 // Object-side element: complex (complex64 objects) or real (float32 objects)
@@ -70,6 +87,7 @@ struct El<float2> {
   static __device__ __forceinline__ float2 cplx(float2 v) { return v; }
   // projection of a complex gradient onto the element space
   static __device__ __forceinline__ float2 proj(float2 g) { return g; }
+  static __device__ __forceinline__ float2 from_sm(float2 g) { return g; }
   static __device__ __forceinline__ float redot(float2 a, float2 b) { return a.x * b.x + a.y * b.y; }
 };
 template <>
@@ -78,6 +96,7 @@ struct El<float> {
   static __device__ __forceinline__ void fma(float& a, float w, float v) { a += w * v; }
   static __device__ __forceinline__ float2 cplx(float v) { return make_float2(v, 0.f); }
   static __device__ __forceinline__ float proj(float2 g) { return g.x; }
+  static __device__ __forceinline__ float from_sm(float2 g) { return g.x; }
   static __device__ __forceinline__ float redot(float a, float b) { return a * b; }
 };
 
@@ -94,51 +113,92 @@ struct CascDims {
   long nimg;  // ntheta * ndist
 };
 
-// Stencil weights at one detector pixel (cuda_kernels.py:177-190).
-struct Taps {
-  int ix, iy;
-  float px[4], py[4], dpx[4], dpy[4], d2px[4], d2py[4];
-};
-
-template <int ORDER>
-__device__ __forceinline__ void taps(const CascDims& D, float mag, float2 r /* (y, x) */, int tx, int ty, Taps& w) {
-  const float half = (mag - 1.0f) / 2.0f;
-  const float x = (mag * (float)(tx - D.n / 2) - r.y + half) + (float)(D.nobj / 2);
-  const float y = (mag * (float)(ty - D.nz / 2) - r.x + half) + (float)(D.nzobj / 2);
-  w.ix = (int)floorf(x);
-  w.iy = (int)floorf(y);
-  const float dx = x - (float)w.ix, dy = y - (float)w.iy;
-#pragma unroll
-  for (int j = 0; j < 4; ++j) {
-    const float ux = dx - (float)(j - 1), uy = dy - (float)(j - 1);
-    w.px[j] = bsp0(ux);
-    w.py[j] = bsp0(uy);
-    if (ORDER >= 1) {
-      w.dpx[j] = bsp1(ux);
-      w.dpy[j] = bsp1(uy);
-    }
-    if (ORDER >= 2) {
-      w.d2px[j] = bsp2(ux);
-      w.d2py[j] = bsp2(uy);
-    }
-  }
+// Object coordinate of detector column tx / row ty (cuda_kernels.py:177-190):
+// mag * (t - n/2) - shift + (mag - 1)/2 + nobj/2.  Forward and adjoint use
+// these same expressions, so the stencil footprints agree exactly.
+__device__ __forceinline__ float sample_x(const CascDims& D, float mag, float rx, int tx) {
+  return (mag * (float)(tx - D.n / 2) - rx + (mag - 1.0f) / 2.0f) + (float)(D.nobj / 2);
+}
+__device__ __forceinline__ float sample_y(const CascDims& D, float mag, float ry, int ty) {
+  return (mag * (float)(ty - D.nz / 2) - ry + (mag - 1.0f) / 2.0f) + (float)(D.nzobj / 2);
 }
 
-// sum over the 4x4 taps of weight(jy, jx) * c[...], zero outside
-#define HT_TAP_LOOP(D, w, cbase, BODY)                                  \
-  _Pragma("unroll") for (int jy = 0; jy < 4; ++jy) {                    \
-    const int yy = w.iy + jy - 1;                                       \
-    if (yy < 0 || yy >= D.nzobj) continue;                              \
-    _Pragma("unroll") for (int jx = 0; jx < 4; ++jx) {                  \
-      const int xx = w.ix + jx - 1;                                     \
-      if (xx < 0 || xx >= D.nobj) continue;                             \
-      const long ci = (long)yy * D.nobj + xx;                           \
-      BODY                                                              \
-    }                                                                   \
+// Vertical stencil of one detector row: the four object rows it reads
+// (clamped into range; taps outside the object get weight 0) and their
+// weights.  The whole detector row shares it.
+template <int ORDER>
+struct RowGeo {
+  int yy[4];
+  float py[4], dpy[4], d2py[4];
+  __device__ __forceinline__ RowGeo(const CascDims& D, float mag, float ry, int ty) {
+    const float y = sample_y(D, mag, ry, ty);
+    const int iy = (int)floorf(y);
+    const float dy = y - (float)iy;
+    bw0(dy, py);
+    if (ORDER >= 1) bw1(dy, dpy);
+    if (ORDER >= 2) bw2(dy, d2py);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int r = iy + j - 1;
+      const bool in = r >= 0 && r < D.nzobj;
+      yy[j] = in ? r : 0;
+      if (!in) {
+        py[j] = 0.f;
+        if (ORDER >= 1) dpy[j] = 0.f;
+        if (ORDER >= 2) d2py[j] = 0.f;
+      }
+    }
   }
+};
+
+// Horizontal stencil of one detector pixel (same conventions).
+template <int ORDER>
+struct ColGeo {
+  int xx[4];
+  float px[4], dpx[4], d2px[4];
+  __device__ __forceinline__ ColGeo(const CascDims& D, float mag, float rx, int tx) {
+    const float x = sample_x(D, mag, rx, tx);
+    const int ix = (int)floorf(x);
+    const float dx = x - (float)ix;
+    bw0(dx, px);
+    if (ORDER >= 1) bw1(dx, dpx);
+    if (ORDER >= 2) bw2(dx, d2px);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int c = ix + j - 1;
+      const bool in = c >= 0 && c < D.nobj;
+      xx[j] = in ? c : 0;
+      if (!in) {
+        px[j] = 0.f;
+        if (ORDER >= 1) dpx[j] = 0.f;
+        if (ORDER >= 2) d2px[j] = 0.f;
+      }
+    }
+  }
+};
+
+// the four samples of one object row under a pixel's horizontal stencil
+template <class T>
+__device__ __forceinline__ void row4(const T* __restrict__ rowp, const int (&xx)[4], T (&v)[4]) {
+#pragma unroll
+  for (int j = 0; j < 4; ++j) v[j] = __ldg(&rowp[xx[j]]);
+}
+template <class T>
+__device__ __forceinline__ T dot4(const float (&w)[4], const T (&v)[4]) {
+  T a = El<T>::zero();
+#pragma unroll
+  for (int j = 0; j < 4; ++j) El<T>::fma(a, w[j], v[j]);
+  return a;
+}
 
 __device__ __forceinline__ float2 ld_pos(const float* pos, long img) {
   return make_float2(pos[2 * img + 0], pos[2 * img + 1]);
+}
+
+// Doubles of shared scratch line_sums<T, K> needs for a block of THREADS.
+template <int T>
+__host__ __device__ constexpr int red_doubles(int K, int threads) {
+  return (T % 32 == 0) ? K * (threads / 32) : K * threads;
 }
 
 // Per-image accumulator slots
@@ -165,13 +225,18 @@ k_casc_fwd(const T* __restrict__ c, const float* __restrict__ pos, const float* 
   const T* cb = c + th * (long)D.nzobj * D.nobj;
   const float m0 = valid ? mag[img] : 1.f;
   const float2 r = valid ? ld_pos(pos, img) : make_float2(0.f, 0.f);
+  const RowGeo<0> rg(D, m0, r.x, ty);
   for (int tx = t; tx < N; tx += TT) {
     float2 u = make_float2(0.f, 0.f);
     if (valid) {
-      Taps w;
-      taps<0>(D, m0, r, tx, ty, w);
+      const ColGeo<0> cg(D, m0, r.y, tx);
       T x22 = El<T>::zero();
-      HT_TAP_LOOP(D, w, cb, El<T>::fma(x22, w.px[jx] * w.py[jy], __ldg(&cb[ci]));)
+#pragma unroll
+      for (int jy = 0; jy < 4; ++jy) {
+        T v[4];
+        row4(cb + (long)rg.yy[jy] * D.nobj, cg.xx, v);
+        El<T>::fma(x22, rg.py[jy], dot4(cg.px, v));
+      }
       u = cmul(prb[((long)k * D.nz + ty) * N + tx], cexp_i(El<T>::cplx(x22)));
     }
     dct2_put<N>(sm, tx, u);
@@ -235,16 +300,36 @@ k_casc_resid(float2* __restrict__ tmp, float2* __restrict__ x0c, const float* __
   dct2_finish<N, TT>(sm, t, tw4, tmp + row * N, valid);
 }
 
+// Detector columns [lo, hi] whose stencil can reach object index i (a
+// superset; callers test the exact footprint).  C0 is the coordinate offset
+// and nhalf the detector half size of the axis.
+__device__ __forceinline__ void cand_range(float m0, float C0, int i, int nhalf, int nmax, int& lo, int& hi) {
+  if (!(fabsf(m0) > 1e-3f)) {
+    lo = 0;
+    hi = nmax - 1;
+    return;
+  }
+  const float a = ((float)(i - 2) - C0) / m0 + (float)nhalf;
+  const float b = ((float)(i + 2) - C0) / m0 + (float)nhalf;
+  const float l = fminf(fmaxf(fminf(a, b), -1e7f), 1e7f);
+  const float h = fminf(fmaxf(fmaxf(a, b), -1e7f), 1e7f);
+  lo = max(0, (int)floorf(l) - 1);
+  hi = min(nmax - 1, (int)ceilf(h) + 1);
+}
+
 // ============================================== adjoint row pass
 // tmp holds the column-processed spectrum of g0.  G = DCT-III; recompute
 // x12; P = G conj(x12) -> cache; Y22 = -i conj(prb) P; per-image sums
-// Ax, Ay, Hxx, Hxy, Hyy.
+// Ax, Ay, Hxx, Hxy, Hyy; and the horizontal half of S^T: for every object
+// column ix, hrow[ix] = sum_tx px(tx -> ix) Y22[tx]  (the vertical half is
+// k_casc_vsum; S is separable, so S^T is too).
 template <int N, class T>
 __global__ void __launch_bounds__(RowCfg<N>::THREADS)
-k_casc_adj(const float2* __restrict__ tmp, float2* __restrict__ Pc, const T* __restrict__ c,
+k_casc_adj(const float2* __restrict__ tmp, float2* __restrict__ Pc, T* __restrict__ hbuf, const T* __restrict__ c,
            const float* __restrict__ pos, const float* __restrict__ mag, const float2* __restrict__ prb,
            double* __restrict__ acc_img, CascDims D, const float2* __restrict__ tw4) {
   constexpr int TT = RowCfg<N>::T;
+  constexpr int E = Plan<N>::E;
   extern __shared__ float2 smem[];
   double* red = reinterpret_cast<double*>(smem + RowCfg<N>::LINES * SmRow::padded(N));
   const int line = threadIdx.x / TT, t = threadIdx.x % TT;
@@ -259,29 +344,37 @@ k_casc_adj(const float2* __restrict__ tmp, float2* __restrict__ Pc, const T* __r
   const T* cb = c + th * (long)D.nzobj * D.nobj;
   const float m0 = valid ? mag[img] : 1.f;
   const float2 r = valid ? ld_pos(pos, img) : make_float2(0.f, 0.f);
+  const RowGeo<2> rg(D, m0, r.x, ty);
   float s[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
-  for (int tx = t; tx < N; tx += TT) {
-    if (!valid) break;
+  float2 Yr[E];
+#pragma unroll
+  for (int i = 0; i < E; ++i) {
+    const int tx = t + i * TT;
+    Yr[i] = make_float2(0.f, 0.f);
+    if (!valid) continue;
     const float2 G = sm.ld(dct_perm(tx, N));
-    Taps w;
-    taps<2>(D, m0, r, tx, ty, w);
+    const ColGeo<2> cg(D, m0, r.y, tx);
     T x22 = El<T>::zero(), ax = El<T>::zero(), ay = El<T>::zero(), hxx = El<T>::zero(), hxy = El<T>::zero(),
       hyy = El<T>::zero();
-    HT_TAP_LOOP(D, w, cb, {
-      const T cv = __ldg(&cb[ci]);
-      El<T>::fma(x22, w.px[jx] * w.py[jy], cv);
-      El<T>::fma(ax, w.dpx[jx] * w.py[jy], cv);
-      El<T>::fma(ay, w.px[jx] * w.dpy[jy], cv);
-      El<T>::fma(hxx, w.d2px[jx] * w.py[jy], cv);
-      El<T>::fma(hxy, w.dpx[jx] * w.dpy[jy], cv);
-      El<T>::fma(hyy, w.px[jx] * w.d2py[jy], cv);
-    })
+#pragma unroll
+    for (int jy = 0; jy < 4; ++jy) {
+      T v[4];
+      row4(cb + (long)rg.yy[jy] * D.nobj, cg.xx, v);
+      const T h0 = dot4(cg.px, v), h1 = dot4(cg.dpx, v), h2 = dot4(cg.d2px, v);
+      El<T>::fma(x22, rg.py[jy], h0);
+      El<T>::fma(ax, rg.py[jy], h1);
+      El<T>::fma(ay, rg.dpy[jy], h0);
+      El<T>::fma(hxx, rg.py[jy], h2);
+      El<T>::fma(hxy, rg.dpy[jy], h1);
+      El<T>::fma(hyy, rg.d2py[jy], h0);
+    }
     const float2 x12 = cexp_i(El<T>::cplx(x22));
     const float2 P = cmulc(G, x12);
     Pc[row * N + tx] = P;
     const float2 pr = prb[((long)k * D.nz + ty) * N + tx];
     // Y22 = -i conj(pr) P  (rec_mpi.py:706-707, .real for float32 objects)
     const T Y = El<T>::proj(rot<false>(cmulc(P, pr)));
+    Yr[i] = El<T>::cplx(Y);
     s[0] += El<T>::redot(Y, ax);
     s[1] += El<T>::redot(Y, ay);
     s[2] += El<T>::redot(Y, hxx);
@@ -291,10 +384,30 @@ k_casc_adj(const float2* __restrict__ tmp, float2* __restrict__ Pc, const T* __r
   double v[5];
 #pragma unroll
   for (int i = 0; i < 5; ++i) v[i] = s[i];
-  line_sums<TT, 5>(v, red, line, t);
+  line_sums<TT, 5>(v, red, line, t);  // contains barriers: G is no longer read
   if (t == 0 && valid) {
 #pragma unroll
     for (int i = 0; i < 5; ++i) atomicAdd(&acc_img[img * kNAcc + kAx + i], v[i]);
+  }
+  __syncthreads();
+#pragma unroll
+  for (int i = 0; i < E; ++i) sm.st(t + i * TT, Yr[i]);
+  __syncthreads();
+  if (!valid) return;
+  const float C0 = -r.y + (m0 - 1.0f) / 2.0f + (float)(D.nobj / 2);
+  T* hrow = hbuf + row * (long)D.nobj;
+  for (int ix = t; ix < D.nobj; ix += TT) {
+    int lo, hi;
+    cand_range(m0, C0, ix, D.n / 2, D.n, lo, hi);
+    T acc = El<T>::zero();
+    for (int tx = lo; tx <= hi; ++tx) {
+      const float x = sample_x(D, m0, r.y, tx);
+      const int ixw = (int)floorf(x);
+      const int j = ix - ixw + 1;
+      if (j < 0 || j > 3) continue;
+      El<T>::fma(acc, bw0_tap(x - (float)ixw, j), El<T>::from_sm(sm.ld(tx)));
+    }
+    hrow[ix] = acc;
   }
 }
 
@@ -316,26 +429,12 @@ __global__ void k_sum_theta(const float2* __restrict__ Pc, float2* __restrict__ 
 }
 
 // ================================================= object gradient
-// gc[theta, iy, ix] = sum_k S_k^T(Y22[theta, k]) (gF3, rec_mpi.py:802-808),
-// gathered from the detector pixels whose 4x4 footprint holds (iy, ix).
-__device__ __forceinline__ void cand(float m0, float C0, int i, int nhalf, int nmax, int& lo, int& hi) {
-  if (!(fabsf(m0) > 1e-3f)) {
-    lo = 0;
-    hi = nmax - 1;
-    return;
-  }
-  const float a = ((float)(i - 2) - C0) / m0 + (float)nhalf;
-  const float b = ((float)(i + 2) - C0) / m0 + (float)nhalf;
-  const float l = fminf(fmaxf(fminf(a, b), -1e7f), 1e7f);
-  const float h = fminf(fmaxf(fmaxf(a, b), -1e7f), 1e7f);
-  lo = max(0, (int)floorf(l) - 1);
-  hi = min(nmax - 1, (int)ceilf(h) + 1);
-}
-
+// gc[theta, iy, ix] = sum_k sum_ty py(ty -> iy) hbuf[theta, k, ty, ix]
+// (the vertical half of sum_k S_k^T Y22, gF3, rec_mpi.py:802-808).
 template <class T>
 __global__ void __launch_bounds__(256)
-k_casc_sadj(T* __restrict__ gc, const float2* __restrict__ Pc, const float2* __restrict__ prb,
-            const float* __restrict__ pos, const float* __restrict__ mag, CascDims D) {
+k_casc_vsum(T* __restrict__ gc, const T* __restrict__ hbuf, const float* __restrict__ pos,
+            const float* __restrict__ mag, CascDims D) {
   const int ix = blockIdx.x * blockDim.x + threadIdx.x;
   const int iy = blockIdx.y * blockDim.y + threadIdx.y;
   const long th = blockIdx.z;
@@ -344,28 +443,16 @@ k_casc_sadj(T* __restrict__ gc, const float2* __restrict__ Pc, const float2* __r
   for (int k = 0; k < D.ndist; ++k) {
     const long img = th * D.ndist + k;
     const float m0 = mag[img];
-    const float ry = pos[2 * img + 0], rx = pos[2 * img + 1];
-    const float half = (m0 - 1.0f) / 2.0f;
-    int tx0, tx1, ty0, ty1;
-    cand(m0, -rx + half + (float)(D.nobj / 2), ix, D.n / 2, D.n, tx0, tx1);
-    cand(m0, -ry + half + (float)(D.nzobj / 2), iy, D.nz / 2, D.nz, ty0, ty1);
-    const float2* Pi = Pc + img * (long)D.nz * D.n;
-    const float2* pk = prb + (long)k * D.nz * D.n;
+    const float ry = pos[2 * img + 0];
+    int ty0, ty1;
+    cand_range(m0, -ry + (m0 - 1.0f) / 2.0f + (float)(D.nzobj / 2), iy, D.nz / 2, D.nz, ty0, ty1);
+    const T* hb = hbuf + img * (long)D.nz * D.nobj + ix;
     for (int ty = ty0; ty <= ty1; ++ty) {
-      const float y = (m0 * (float)(ty - D.nz / 2) - ry + half) + (float)(D.nzobj / 2);
-      const int jy = iy - (int)floorf(y);
-      if (jy < -1 || jy > 2) continue;
-      const float wy = bsp0(y - floorf(y) - (float)jy);
-      T racc = El<T>::zero();
-      for (int tx = tx0; tx <= tx1; ++tx) {
-        const float x = (m0 * (float)(tx - D.n / 2) - rx + half) + (float)(D.nobj / 2);
-        const int jx = ix - (int)floorf(x);
-        if (jx < -1 || jx > 2) continue;
-        const long p = (long)ty * D.n + tx;
-        const T Y = El<T>::proj(rot<false>(cmulc(__ldg(&Pi[p]), __ldg(&pk[p]))));
-        El<T>::fma(racc, bsp0(x - floorf(x) - (float)jx), Y);
-      }
-      El<T>::fma(acc, wy, racc);
+      const float y = sample_y(D, m0, ry, ty);
+      const int iyw = (int)floorf(y);
+      const int j = iy - iyw + 1;
+      if (j < 0 || j > 3) continue;
+      El<T>::fma(acc, bw0_tap(y - (float)iyw, j), __ldg(&hb[(long)ty * D.nobj]));
     }
   }
   gc[(th * D.nzobj + iy) * D.nobj + ix] = acc;
@@ -406,41 +493,46 @@ k_casc_hess_fwd(const T* __restrict__ c, const float* __restrict__ pos, const fl
   SmRow sm1{smem + (LINES + line) * SmRow::padded(N)};
   const long coff = th * (long)D.nzobj * D.nobj;
   const T* cb = c + coff;
+  const T* cb0 = c0 + coff;
+  const T* cb1 = (NDIR == 2) ? c1 + coff : c0 + coff;
   const float m0 = valid ? mag[img] : 1.f;
   const float2 r = valid ? ld_pos(pos, img) : make_float2(0.f, 0.f);
   const float2 rd0 = valid ? ld_pos(pos0, img) : make_float2(0.f, 0.f);
   const float2 rd1 = (valid && NDIR == 2) ? ld_pos(pos1, img) : make_float2(0.f, 0.f);
+  const RowGeo<1> rg(D, m0, r.x, ty);
   // sums: L1 00,01,11 ; L2 00,01,11 ; A: ax0, ay0, ax1, ay1
   float s[10] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
   for (int tx = t; tx < N; tx += TT) {
     float2 v0 = make_float2(0.f, 0.f), v1 = make_float2(0.f, 0.f);
     if (valid) {
-      Taps w;
-      taps<1>(D, m0, r, tx, ty, w);
+      const ColGeo<1> cg(D, m0, r.y, tx);
       T x22 = El<T>::zero(), dxc = El<T>::zero(), dyc = El<T>::zero();
       T s0 = El<T>::zero(), ax0 = El<T>::zero(), ay0 = El<T>::zero();
       T s1 = El<T>::zero(), ax1 = El<T>::zero(), ay1 = El<T>::zero();
-      const T* cb0 = c0 + coff;
-      const T* cb1 = (NDIR == 2) ? c1 + coff : c0 + coff;
-      HT_TAP_LOOP(D, w, cb, {
-        const float pp = w.px[jx] * w.py[jy];
-        const float dxw = w.dpx[jx] * w.py[jy];
-        const float dyw = w.px[jx] * w.dpy[jy];
-        const T cv = __ldg(&cb[ci]);
-        El<T>::fma(x22, pp, cv);
-        El<T>::fma(dxc, dxw, cv);
-        El<T>::fma(dyc, dyw, cv);
-        const T a0 = __ldg(&cb0[ci]);
-        El<T>::fma(s0, pp, a0);
-        El<T>::fma(ax0, dxw, a0);
-        El<T>::fma(ay0, dyw, a0);
+#pragma unroll
+      for (int jy = 0; jy < 4; ++jy) {
+        const long ro = (long)rg.yy[jy] * D.nobj;
+        T v[4];
+        row4(cb + ro, cg.xx, v);
+        T h0 = dot4(cg.px, v), h1 = dot4(cg.dpx, v);
+        El<T>::fma(x22, rg.py[jy], h0);
+        El<T>::fma(dxc, rg.py[jy], h1);
+        El<T>::fma(dyc, rg.dpy[jy], h0);
+        row4(cb0 + ro, cg.xx, v);
+        h0 = dot4(cg.px, v);
+        h1 = dot4(cg.dpx, v);
+        El<T>::fma(s0, rg.py[jy], h0);
+        El<T>::fma(ax0, rg.py[jy], h1);
+        El<T>::fma(ay0, rg.dpy[jy], h0);
         if (NDIR == 2) {
-          const T a1 = __ldg(&cb1[ci]);
-          El<T>::fma(s1, pp, a1);
-          El<T>::fma(ax1, dxw, a1);
-          El<T>::fma(ay1, dyw, a1);
+          row4(cb1 + ro, cg.xx, v);
+          h0 = dot4(cg.px, v);
+          h1 = dot4(cg.dpx, v);
+          El<T>::fma(s1, rg.py[jy], h0);
+          El<T>::fma(ax1, rg.py[jy], h1);
+          El<T>::fma(ay1, rg.dpy[jy], h0);
         }
-      })
+      }
       // dS (rec_mpi.py:757; cuda_kernels.py:600-609): sum phi phi c_d - (dphi_x phi_y r_dx + phi_x dphi_y r_dy) c
       T y0 = s0, y1 = s1;
       El<T>::fma(y0, -rd0.y, dxc);
@@ -478,22 +570,35 @@ k_casc_hess_fwd(const T* __restrict__ c, const float* __restrict__ pos, const fl
     dct2_put<N>(sm0, tx, v0);
     if (NDIR == 2) dct2_put<N>(sm1, tx, v1);
   }
-  double v[10];
+  constexpr int K = (NDIR == 2) ? 10 : 4;
+  double v[K];
+  if (NDIR == 2) {
 #pragma unroll
-  for (int i = 0; i < 10; ++i) v[i] = s[i];
-  line_sums<TT, 10>(v, red, line, t);
+    for (int i = 0; i < K; ++i) v[i] = s[i];
+  } else {
+    v[0] = s[0];
+    v[1] = s[3];
+    v[2] = s[6];
+    v[3] = s[7];
+  }
+  line_sums<TT, K>(v, red, line, t);
   if (t == 0 && valid) {
-    atomicAdd(&glob[kL10], v[0]);
-    atomicAdd(&glob[kL20], v[3]);
-    atomicAdd(&acc_img[img * kNAcc + kAyx], v[6]);
-    atomicAdd(&acc_img[img * kNAcc + kAyy], v[7]);
     if (NDIR == 2) {
+      atomicAdd(&glob[kL10], v[0]);
+      atomicAdd(&glob[kL20], v[3]);
+      atomicAdd(&acc_img[img * kNAcc + kAyx], v[6]);
+      atomicAdd(&acc_img[img * kNAcc + kAyy], v[7]);
       atomicAdd(&glob[kL11], v[1]);
       atomicAdd(&glob[kL12], v[2]);
       atomicAdd(&glob[kL21], v[4]);
       atomicAdd(&glob[kL22], v[5]);
       atomicAdd(&acc_img[img * kNAcc + kAzx], v[8]);
       atomicAdd(&acc_img[img * kNAcc + kAzy], v[9]);
+    } else {
+      atomicAdd(&glob[kL10], v[0]);
+      atomicAdd(&glob[kL20], v[1]);
+      atomicAdd(&acc_img[img * kNAcc + kAyx], v[2]);
+      atomicAdd(&acc_img[img * kNAcc + kAyy], v[3]);
     }
   }
   __syncthreads();
@@ -639,7 +744,10 @@ extern "C" int ht_rec_create(int n, int nz, int nobj, int nzobj, int ntheta, int
   const size_t img = (size_t)ntheta * ndist * nz * n;
   cudaError_t e = cudaMalloc(&r->x0, sizeof(float2) * img);
   if (e == cudaSuccess) e = cudaMalloc(&r->P, sizeof(float2) * img);
-  if (e == cudaSuccess) e = cudaMalloc(&r->tmp, sizeof(float2) * 2 * img);
+  // tmp: two spectra for the Hessian pass; during the gradient pass its
+  // second part holds the horizontal S^T rows [nimg, nz, nobj] of T
+  const size_t hrow = ((size_t)ntheta * ndist * nz * nobj * (is_complex ? 8 : 4) + 7) / 8;
+  if (e == cudaSuccess) e = cudaMalloc(&r->tmp, sizeof(float2) * (img + std::max(img, hrow)));
   if (e == cudaSuccess) e = cudaMalloc(&r->acc_img, sizeof(double) * (size_t)ntheta * ndist * kNAcc);
   if (e == cudaSuccess) e = cudaMalloc(&r->glob, sizeof(double) * kNGlob);
   if (e != cudaSuccess) {
@@ -687,7 +795,7 @@ template <int N, int MODE>
 static cudaError_t resid_pass(ht_rec_s* r, const float* data, float* amp, float scale, const float2* twn,
                               cudaStream_t st) {
   using CF = RowCfg<N>;
-  const int smem = CF::SMEM + CF::THREADS * (int)sizeof(double);
+  const int smem = CF::SMEM + red_doubles<CF::T>(1, CF::THREADS) * (int)sizeof(double);
   cudaError_t e = allow_smem(k_casc_resid<N, MODE>, smem);
   if (e != cudaSuccess) return e;
   const long nrows = r->D.nimg * r->D.nz;
@@ -707,15 +815,16 @@ static cudaError_t grad_impl(ht_rec_s* r, const void* c, const float* pos, const
   if ((e = dct_cols(r->D.nz, true, r->tmp, r->D.nimg, N, hw, r->D.ndist, twz, st)) != cudaSuccess) return e;
   using CF = RowCfg<N>;
   const long nrows = r->D.nimg * r->D.nz;
-  const int smem = CF::SMEM + 5 * CF::THREADS * (int)sizeof(double);
+  const int smem = CF::SMEM + red_doubles<CF::T>(5, CF::THREADS) * (int)sizeof(double);
   if ((e = allow_smem(k_casc_adj<N, T>, smem)) != cudaSuccess) return e;
-  k_casc_adj<N, T><<<HT_ROWS_GRID(N, nrows), CF::THREADS, smem, st>>>(r->tmp, r->P, (const T*)c, pos, mag, prb,
-                                                                      r->acc_img, r->D, twn); ::ht::count_launch();
+  T* hbuf = reinterpret_cast<T*>(r->tmp + nrows * N);
+  k_casc_adj<N, T><<<HT_ROWS_GRID(N, nrows), CF::THREADS, smem, st>>>(r->tmp, r->P, hbuf, (const T*)c, pos, mag,
+                                                                      prb, r->acc_img, r->D, twn); ::ht::count_launch();
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   const long npix = (long)r->D.nz * N;
   k_sum_theta<<<(unsigned)((r->D.ndist * npix + 255) / 256), 256, 0, st>>>(r->P, gprb, r->ntheta, r->D.ndist, npix); ::ht::count_launch();
   dim3 g2((r->D.nobj + 31) / 32, (r->D.nzobj + 7) / 8, r->ntheta);
-  k_casc_sadj<T><<<g2, dim3(32, 8), 0, st>>>((T*)gc, r->P, prb, pos, mag, r->D); ::ht::count_launch();
+  k_casc_vsum<T><<<g2, dim3(32, 8), 0, st>>>((T*)gc, hbuf, pos, mag, r->D); ::ht::count_launch();
   k_casc_gpos<<<(unsigned)((r->D.nimg + 255) / 256), 256, 0, st>>>(r->acc_img, gpos, r->D.nimg); ::ht::count_launch();
   return cudaGetLastError();
 }
@@ -728,7 +837,7 @@ static cudaError_t hess_impl(ht_rec_s* r, const void* c, const float* pos, const
   prop_tables(r->prop, &hw, &twn, &twz);
   using CF = RowCfg<N>;
   const long nrows = r->D.nimg * r->D.nz;
-  const int smem = NDIR * CF::SMEM + 10 * CF::THREADS * (int)sizeof(double);
+  const int smem = NDIR * CF::SMEM + red_doubles<CF::T>(NDIR == 2 ? 10 : 4, CF::THREADS) * (int)sizeof(double);
   cudaError_t e = allow_smem(k_casc_hess_fwd<N, T, NDIR>, smem);
   if (e != cudaSuccess) return e;
   k_casc_hess_fwd<N, T, NDIR><<<HT_ROWS_GRID(N, nrows), CF::THREADS, smem, st>>>(
@@ -736,7 +845,7 @@ static cudaError_t hess_impl(ht_rec_s* r, const void* c, const float* pos, const
       r->D, twn); ::ht::count_launch();
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   if ((e = dct_cols(r->D.nz, false, r->tmp, NDIR * r->D.nimg, N, hw, r->D.ndist, twz, st)) != cudaSuccess) return e;
-  const int smq = NDIR * CF::SMEM + 3 * CF::THREADS * (int)sizeof(double);
+  const int smq = NDIR * CF::SMEM + red_doubles<CF::T>(3, CF::THREADS) * (int)sizeof(double);
   if ((e = allow_smem(k_casc_hess_q<N, NDIR>, smq)) != cudaSuccess) return e;
   k_casc_hess_q<N, NDIR><<<HT_ROWS_GRID(N, nrows), CF::THREADS, smq, st>>>(r->tmp, r->x0, data, r->glob, r->D, twn); ::ht::count_launch();
   return cudaGetLastError();

@@ -21,6 +21,27 @@ std::atomic<long> g_launches{0};
 void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 long launch_count() { return g_launches.load(std::memory_order_relaxed); }
 
+namespace {
+std::mutex g_attr_mutex;
+std::map<std::pair<int, const void*>, int> g_attr;  // (device, kernel) -> bytes allowed
+}  // namespace
+
+bool smem_attr_done(const void* kernel, int bytes) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lock(g_attr_mutex);
+  auto it = g_attr.find(std::make_pair(dev, kernel));
+  return it != g_attr.end() && it->second >= bytes;
+}
+
+void smem_attr_mark(const void* kernel, int bytes) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lock(g_attr_mutex);
+  int& b = g_attr[std::make_pair(dev, kernel)];
+  if (bytes > b) b = bytes;
+}
+
 void set_error(const std::string& msg) { g_last_error = msg; }
 const char* last_error() { return g_last_error.c_str(); }
 

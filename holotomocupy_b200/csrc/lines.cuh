@@ -23,11 +23,20 @@ struct ColCfg {
   static constexpr int SMEM = N * C * (int)sizeof(float2);
 };
 
-// Set the dynamic shared-memory limit of a kernel once (no-op below 48 KB).
+// Raise the dynamic shared-memory limit of a kernel (no-op below 48 KB).  The
+// attribute is set once per (device, kernel, size), so the launches that
+// follow (including ones recorded into CUDA graphs) make no further runtime
+// calls.
+bool smem_attr_done(const void* kernel, int bytes);
+void smem_attr_mark(const void* kernel, int bytes);
 template <class K>
 inline cudaError_t allow_smem(K kernel, int bytes) {
   if (bytes <= 48 * 1024) return cudaSuccess;
-  return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  const void* key = reinterpret_cast<const void*>(kernel);
+  if (smem_attr_done(key, bytes)) return cudaSuccess;
+  const cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e == cudaSuccess) smem_attr_mark(key, bytes);
+  return e;
 }
 
 // Position of input sample g after the even/odd-reversed reordering used by

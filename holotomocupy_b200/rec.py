@@ -103,6 +103,10 @@ class Rec:
         self._scal = torch.zeros(8, dtype=torch.float64, device=dev)
 
     def __del__(self):
+        try:
+            self.release_graph()
+        except Exception:
+            pass
         h = getattr(self, "_h", None)
         if h is not None and h.value:
             try:
@@ -133,6 +137,18 @@ class Rec:
         # B-spline coefficients of vars/grads/etas proj
         self._c = {"vars": z(self.ntheta, self.nzobj, self.nobj), "grads": z(self.ntheta, self.nzobj, self.nobj),
                    "etas": z(self.ntheta, self.nzobj, self.nobj)}
+        # persistent outputs of the fused passes and the device-side BH state:
+        # nothing in an iteration allocates, so it can be recorded in a graph
+        self._gc = z(self.ntheta, self.nzobj, self.nobj)
+        self._gpos = z(self.ntheta, self.ndist, 2, dt=torch.float32)
+        self._gprb = z(*prb_shape, dt=torch.complex64)
+        self._H = z(4, dt=torch.float64)
+        self._dots = z(4, dt=torch.float64)
+        self._bh = z(2, dt=torch.float64)            # beta, alpha
+        self._hist_cap = 4096
+        self._hist = z(self._hist_cap, 2, dt=torch.float64)
+        self._count = z(1, dt=torch.int32)
+        self._graph = None
 
     def _coeff_into(self, src, dst):
         """dst = coeff(src) (shift.py:74-82) for a [ntheta, nzobj, nobj] array."""
@@ -149,20 +165,25 @@ class Rec:
                   _lib.ptr(dot) if dot is not None else None, _lib.stream_ptr())
 
     # -------------------------------------------------- fused cascade
-    def _gradient_pass(self, c, pos, prb):
-        """Fused gF0..gF3 (rec_mpi.py:327-353): returns (sum_k S^T Y22, gpos, gprb), F in _scal[0]."""
-        gc = torch.empty_like(c)
-        gpos = torch.empty(self.ntheta, self.ndist, 2, dtype=torch.float32, device=self.device)
-        gprb = torch.empty(self.ndist, self.nz, self.n, dtype=torch.complex64, device=self.device)
+    def _gradient_pass(self, c, pos, prb, persistent=False):
+        """Fused gF0..gF3 (rec_mpi.py:327-353): returns (sum_k S^T Y22, gpos, gprb), F in _scal[0].
+        persistent=True writes into the Rec's own output arrays (no allocation)."""
+        if persistent:
+            gc, gpos, gprb = self._gc, self._gpos, self._gprb
+        else:
+            gc = torch.empty_like(c)
+            gpos = torch.empty(self.ntheta, self.ndist, 2, dtype=torch.float32, device=self.device)
+            gprb = torch.empty(self.ndist, self.nz, self.n, dtype=torch.complex64, device=self.device)
         _lib.call("ht_rec_gradient", self._h, _lib.ptr(c), _lib.ptr(pos), _lib.ptr(self.eff_demagnifications),
                   _lib.ptr(prb), _lib.ptr(self.data), _lib.ptr(gc), _lib.ptr(gpos), _lib.ptr(gprb),
                   _lib.ptr(self._scal), _lib.stream_ptr())
         return gc, gpos, gprb
 
-    def _hessian_pass(self, c, pos, prb, y, z=None):
+    def _hessian_pass(self, c, pos, prb, y, z=None, out=None):
         """Fused Hessian forms; y, z = (coefficients, pos, prb) of the directions.
         Returns float64 tensor [H(y,y), H_ref(y,z), H(z,z), H_sym(y,z)]."""
-        out = torch.zeros(4, dtype=torch.float64, device=self.device)
+        if out is None:
+            out = torch.zeros(4, dtype=torch.float64, device=self.device)
         zz = z if z is not None else (None, None, None)
         _lib.call("ht_rec_hessian", self._h, _lib.ptr(c), _lib.ptr(pos), _lib.ptr(self.eff_demagnifications),
                   _lib.ptr(prb), _lib.ptr(self.data), 2 if z is not None else 1, _lib.ptr(y[0]), _lib.ptr(y[1]),
@@ -275,10 +296,31 @@ class Rec:
             out[j] = torch.abs(self.cl_prop.D(prb[j: j + 1].contiguous(), j)[0])
 
     # ------------------------------------------------------------ BH
-    def BH(self, writer=None, niter=None, record=None):
-        """rec_mpi.py:138-232.  ``record`` (a list) receives (iteration, alpha, beta)."""
+    def BH(self, writer=None, niter=None, record=None, mode="host"):
+        """rec_mpi.py:138-232.  ``record`` (a list) receives (iteration, alpha, beta).
+
+        mode="host" iterates as the reference does (step sizes on the host).
+        mode="graph" keeps the step sizes on the device and replays the
+        steady-state iteration from a CUDA graph (same arithmetic; needs
+        lam_prbfit == 0 and no error table)."""
         self.bh_setup()
         niter = self.niter if niter is None else niter
+        if mode == "graph" and self.lam_prbfit == 0 and self.err_step == -1 and niter > self.start_iter:
+            cur = torch.cuda.current_stream(self.device)
+            side = torch.cuda.Stream(device=self.device)
+            side.wait_stream(cur)
+            with torch.cuda.stream(side):
+                self.bh_iteration(self.start_iter, sync=False)
+                if niter - self.start_iter > 1:
+                    self.capture_iteration()
+                    for _ in range(self.start_iter + 1, niter):
+                        self.replay_iteration()
+                    self.release_graph()
+            cur.wait_stream(side)
+            if record is not None:
+                for k, (a, b) in enumerate(self.bh_history()):
+                    record.append((self.start_iter + k, float(a), float(b)))
+            return self.bh_finish()
         for i in range(self.start_iter, niter):
             a, b = self.bh_iteration(i)
             if record is not None:
@@ -299,21 +341,26 @@ class Rec:
         self._coeff_into(vars["proj"], C["vars"])
         self.error_debug(vars, -1)
         self.time_start = time.time()
-        if not hasattr(self, "_dots"):
-            self._dots = torch.zeros(4, dtype=torch.float64, device=self.device)
+        self._count.zero_()
 
     def bh_finish(self):
         """End of BH (rec_mpi.py:229-232)."""
         self.vars["obj"] *= self.norm_const
         return self.vars
 
-    def bh_iteration(self, i):
-        """One BH iteration (rec_mpi.py:163-227); returns (alpha, beta)."""
+    def bh_iteration(self, i, sync=True):
+        """One BH iteration (rec_mpi.py:163-227); returns (alpha, beta).
+
+        sync=False keeps alpha and beta on the device (ht_bh_scalars,
+        ht_axpby_dev): the iteration then makes no host round trip and can be
+        recorded into a CUDA graph; it returns None and appends the step sizes
+        to the device history (bh_history())."""
         vars, grads, etas, C = self.vars, self.grads, self.etas, self._c
         rho = self.rho_sq
         dots = self._dots
+        first = i == self.start_iter
         # ---- gradients (rec_mpi.py:305-325)
-        gc, gpos, gprb = self._gradient_pass(C["vars"], vars["pos"], vars["prb"])
+        gc, gpos, gprb = self._gradient_pass(C["vars"], vars["pos"], vars["prb"], persistent=True)
         torch.mul(gprb, rho["prb"], out=grads["prb"])
         torch.mul(gpos, rho["pos"], out=grads["pos"])
         self._coeff_into(gc, grads["proj"])
@@ -324,14 +371,44 @@ class Rec:
         self._coeff_into(grads["proj"], C["grads"])
         # ---- Hessian forms (rec_mpi.py:180-213)
         y = (C["grads"], grads["pos"], grads["prb"])
-        if i == self.start_iter:
+        z = None if first else (C["etas"], etas["pos"], etas["prb"])
+        H = self._hessian_pass(C["vars"], vars["pos"], vars["prb"], y, z, out=self._H)
+        if sync or self.lam_prbfit != 0:
+            return self._bh_update_host(H.cpu().numpy(), first)
+        # ---- the same with the step sizes on the device
+        st = _lib.stream_ptr()
+        bh = self._bh
+        rr = (float(rho["obj"]), float(rho["pos"]), float(rho["prb"]))
+        _lib.call("ht_bh_scalars", _lib.ptr(H), None, int(first), 0, *rr, _lib.ptr(bh), None, 0, None, st)
+        beta = _lib.ptr(bh)
+        dots.zero_()
+        for k, v in enumerate(("obj", "pos", "prb")):
+            self._axpby_dev(etas[v], grads[v], beta, 1.0, None, -1.0, dots[k:k + 1])
+        self._axpby_dev(etas["proj"], grads["proj"], beta, 1.0, None, -1.0)
+        self._axpby_dev(C["etas"], C["grads"], beta, 1.0, None, -1.0)
+        _lib.call("ht_bh_scalars", _lib.ptr(H), _lib.ptr(dots), int(first), 1, *rr, _lib.ptr(bh),
+                  _lib.ptr(self._hist), self._hist_cap, _lib.ptr(self._count), st)
+        alpha = ctypes.c_void_p(bh.data_ptr() + 8)
+        for v in ("obj", "prb", "pos", "proj"):
+            self._axpby_dev(vars[v], etas[v], None, 1.0, alpha, 1.0)
+        self._axpby_dev(C["vars"], C["etas"], None, 1.0, alpha, 1.0)
+        return None
+
+    def _axpby_dev(self, x, y, A, sa, B, sb, dot=None):
+        n = x.numel() * (2 if x.is_complex() else 1)
+        _lib.call("ht_axpby_dev", _lib.ptr(x), _lib.ptr(y), A, float(sa), B, float(sb), n,
+                  _lib.ptr(dot) if dot is not None else None, _lib.stream_ptr())
+
+    def _bh_update_host(self, H, first):
+        """Direction and variable updates with host step sizes (rec_mpi.py:180-218)."""
+        vars, grads, etas, C = self.vars, self.grads, self.etas, self._c
+        rho = self.rho_sq
+        dots = self._dots
+        if first:
             beta = 0.0
-            H = self._hessian_pass(C["vars"], vars["pos"], vars["prb"], y).cpu().numpy()
             pf = self._prbfit_forms(vars["prb"], grads["prb"], None)
             Hgg = H[0] + pf[0]
         else:
-            z = (C["etas"], etas["pos"], etas["prb"])
-            H = self._hessian_pass(C["vars"], vars["pos"], vars["prb"], y, z).cpu().numpy()
             pf = self._prbfit_forms(vars["prb"], grads["prb"], etas["prb"])
             Hgg, Hge, Hee, Hge_sym = H[0] + pf[0], H[1] + pf[1], H[2] + pf[2], H[3] + pf[1]
             beta = Hge / Hee
@@ -344,12 +421,44 @@ class Rec:
         self._axpby(C["etas"], C["grads"], beta, -1)
         d = dots.cpu().numpy()
         top = -(d[0] / rho["obj"] + d[1] / rho["pos"] + d[2] / rho["prb"])
-        bottom = Hgg if i == self.start_iter else beta * beta * Hee - 2 * beta * Hge_sym + Hgg
+        bottom = Hgg if first else beta * beta * Hee - 2 * beta * Hge_sym + Hgg
         alpha = top / bottom
         for v in ("obj", "prb", "pos", "proj"):
             self._axpby(vars[v], etas[v], 1, alpha)
         self._axpby(C["vars"], C["etas"], 1, alpha)
         return float(alpha), float(beta)
+
+    def bh_history(self):
+        """(alpha, beta) of the device-scalar iterations since bh_setup()."""
+        n = min(int(self._count.item()), self._hist_cap)
+        return [tuple(r) for r in self._hist[:n].cpu().numpy()]
+
+    def capture_iteration(self):
+        """Record one steady-state device-scalar iteration (not the first) on
+        the current stream into a CUDA graph; replay_iteration() then runs it
+        with one launch.  Call after one iteration has run on this device (so
+        every kernel's launch attributes are set).  Recording runs nothing."""
+        if self.lam_prbfit != 0:
+            raise ValueError("graph capture needs lam_prbfit == 0 (the probe-fit forms are host-side)")
+        self.release_graph()
+        st = _lib.stream_ptr()
+        _lib.call("ht_graph_begin", st)
+        try:
+            self.bh_iteration(self.start_iter + 1, sync=False)
+        finally:
+            ex = ctypes.c_void_p()
+            _lib.call("ht_graph_end", st, ctypes.byref(ex))
+        self._graph = ex
+        return ex
+
+    def replay_iteration(self):
+        """Run the recorded iteration on the current stream."""
+        _lib.call("ht_graph_launch", self._graph, _lib.stream_ptr())
+
+    def release_graph(self):
+        if getattr(self, "_graph", None) is not None:
+            _lib.lib().ht_graph_destroy(self._graph)
+            self._graph = None
 
     def error_debug(self, vars, i):
         """rec_mpi.py:862-880 (the convergence table is kept in self.table)."""

@@ -83,3 +83,37 @@ def noisy_amplitudes(amp, photons, seed):
         inten = torch.poisson(photons * amp[i] ** 2, generator=gen)
         amp[i] = torch.sqrt(inten / photons)
     return amp
+
+
+def workload_args(n, ntheta, ndist=4, niter=16, distances=(3e-3, 4e-3, 5e-3, 6e-3), wavelength=7.3e-11,
+                  voxelsize=20e-9, mask=0.9):
+    """Rec arguments of the synthetic workloads: n^3 object, n^2 detector,
+    ntheta angles on [0, pi), unit magnification, distances given directly."""
+    import types
+    return types.SimpleNamespace(
+        theta=np.linspace(0, np.pi, ntheta, endpoint=False).astype("float32"), ndist=ndist, ntheta=ntheta,
+        nz=n, n=n, nzobj=n, nobj=n, obj_dtype="complex64", mask=mask, lam_prbfit=0.0, rho=[1, 0.05, 0.02],
+        niter=niter, nchunk=n, vis_step=-1, err_step=-1, start_iter=0, distance=np.array(distances[:ndist]),
+        wavelength=wavelength, voxelsize=voxelsize, norm_magnifications=np.ones(ndist))
+
+
+def make_problem(n, ntheta, ndist, seed, photons=1e4, device="cuda", pos_amp=2.0, pos_err=0.5, host=False):
+    """(args, data, prb0, pos0, truth): a seeded synthetic reconstruction
+    problem with noisy amplitudes; the initial state is a zero object, a
+    flat probe and perturbed positions.  host=True returns data, prb0 and
+    pos0 in pinned host memory (truth stays on the device)."""
+    from .rec import Rec
+    args = workload_args(n, ntheta, ndist)
+    rec = Rec(args)
+    obj = ellipsoid_phantom(n, 80 if n >= 512 else 20, seed, device=device)
+    prb = random_probe(ndist, n, n, seed + 1, device=device)
+    pos = random_positions(ntheta, ndist, pos_amp, seed + 2, device=device)
+    data = rec.forward_amplitudes(obj, prb, pos)
+    noisy_amplitudes(data, photons, seed + 3)
+    gen = torch.Generator(device=device).manual_seed(seed + 4)
+    pos0 = pos + pos_err * (2 * torch.rand(pos.shape, generator=gen, device=device) - 1)
+    prb0 = torch.ones_like(prb)
+    del rec
+    if host:
+        data, prb0, pos0 = (t.cpu().pin_memory() for t in (data, prb0, pos0))
+    return args, data, prb0, pos0, {"obj": obj, "prb": prb, "pos": pos}

@@ -167,6 +167,21 @@ int ht_rec_hessian(ht_rec_s* r, const void* c, const float* pos, const float* ma
 int ht_axpby(void* x, const void* y, float a, float b, long n, double* dot, void* stream);
 /* *dot += sum(x * y) (device double). */
 int ht_dot(const void* x, const void* y, long n, double* dot, void* stream);
+/* x = a*x + b*y with a = (float)(*A) * sa and b = (float)(*B) * sb read on
+ * the device when the stream reaches the call (A or B NULL: the factor
+ * alone); dot as in ht_axpby.  The BH direction and variable updates
+ * (rec_mpi.py:196-218) with step sizes that never visit the host. */
+int ht_axpby_dev(void* x, const void* y, const double* A, float sa, const double* B, float sb, long n, double* dot,
+                 void* stream);
+/* BH step sizes on the device (rec_mpi.py:180-218, with the forms of
+ * ht_rec_hessian in H[4] and dots[3] = <eta,grad> of obj, pos, prb).
+ * phase 0: scal[0] = beta = first ? 0 : H[1]/H[2].
+ * phase 1: scal[1] = alpha = -(dots[0]/rho_obj + dots[1]/rho_pos + dots[2]/rho_prb)
+ *          / (first ? H[0] : beta^2 H[2] - 2 beta H[3] + H[0]);
+ *          if hist: (alpha, beta) goes to hist[2*(*count)] while *count < cap,
+ *          and *count is incremented (device int). */
+int ht_bh_scalars(const double* H, const double* dots, int first, int phase, double rho_obj, double rho_pos,
+                  double rho_prb, double* scal, double* hist, int cap, int* count, void* stream);
 
 /* The objective sum (|x0| - data)^2 of ht_rec_forward, without allocating.
  * No counterpart in the reference.  For callers that cannot allocate device
@@ -188,6 +203,20 @@ int ht_rec_objective_noalloc(ht_prop_s* prop, int nobj, int nzobj, int ntheta, i
  * 1/N of the inverse transform.  Serves Tomo._filter_sino
  * (src/holotomocupy/tomo.py:118-161). */
 int ht_filter_rows(int N, const void* in, void* out, long nrows, const float* sym, void* stream);
+
+/* ------------------------------------------------------------------------
+ * CUDA graphs of a stream's work (the reference launches every kernel from
+ * Python each iteration; no counterpart).  ht_graph_begin starts recording
+ * the work this thread issues to `stream` (a non-default stream); nothing
+ * runs until the graph is launched.  ht_graph_end ends the recording and
+ * returns an executable graph in *exec; ht_graph_launch runs it on a stream;
+ * ht_graph_destroy frees it.  Everything recorded must already have run
+ * once on this device (so launch attributes and tables exist).
+ * --------------------------------------------------------------------- */
+int ht_graph_begin(void* stream);
+int ht_graph_end(void* stream, void** exec);
+int ht_graph_launch(void* exec, void* stream);
+int ht_graph_destroy(void* exec);
 
 #ifdef __cplusplus
 }

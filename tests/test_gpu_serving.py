@@ -1,0 +1,95 @@
+"""Serving: reconstructions admitted into the persistent loop (own streams,
+device-side step sizes, graph-replayed iterations, overlapping on the GPU)
+give the same result as each run alone through the plain host-synchronised
+Rec.BH iteration.  Bound: rel L2 <= 1e-5 (the same kernels on the same data;
+only the order in which independent requests reach the GPU differs)."""
+import numpy as np
+import pytest
+import torch
+
+from conftest import rel_l2
+
+pytestmark = pytest.mark.gpu
+
+
+def _requests(host=False):
+    from holotomocupy_b200.serving import Request
+    from holotomocupy_b200.synthetic import make_problem
+    reqs = []
+    for rid, (n, ntheta, seed) in enumerate([(64, 112, 11), (128, 224, 12), (64, 112, 13)]):
+        args, data, prb0, pos0, _ = make_problem(n, ntheta, 4, seed, host=host)
+        reqs.append(Request(rid=rid, args=args, data=data, prb0=prb0, pos0=pos0, niter=5, arrival=0.0))
+    return reqs
+
+
+@pytest.mark.parametrize("host", [False, True])
+def test_served_results_equal_alone(host):
+    from holotomocupy_b200.serving import Server, run_plain
+    reqs = _requests(host)
+    _, _, alone = run_plain(reqs)
+    srv = Server(max_active=8)
+    for r in reqs:
+        srv.submit(r)
+    done = {r.rid: r for r in srv.run(realtime=False)}
+    assert srv.max_concurrent == 3
+    for r, ref in zip(reqs, alone):
+        got = done[r.rid].result
+        for k in ("obj", "prb", "pos"):
+            assert rel_l2(got[k].numpy(), ref[k].numpy()) < 1e-5, (r.rid, k)
+        assert len(got["history"]) == r.niter
+        assert len(done[r.rid].latencies_ms) == r.niter
+
+
+def test_admission_respects_the_hbm_budget():
+    """With a budget that holds one 128^3 request at a time, requests run one
+    after another and still give the same results."""
+    from holotomocupy_b200.serving import Server, estimate_bytes, run_plain
+    reqs = _requests()
+    _, _, alone = run_plain(reqs)
+    big = max(estimate_bytes(r.args) for r in reqs)
+    srv = Server(budget_bytes=big + 1, max_active=8)
+    for r in reqs:
+        srv.submit(r)
+    done = {r.rid: r for r in srv.run(realtime=False)}
+    assert srv.peak_bytes <= big + 1
+    for r, ref in zip(reqs, alone):
+        assert rel_l2(done[r.rid].result["obj"].numpy(), ref["obj"].numpy()) < 1e-5
+    with pytest.raises(ValueError):
+        Server(budget_bytes=1).submit(reqs[0])
+
+
+def test_device_scalar_iteration_matches_host_iteration():
+    """Rec.bh_iteration(sync=False) (alpha, beta on the device) and its graph
+    replay equal the host-scalar iteration step for step."""
+    from holotomocupy_b200.rec import Rec
+    from holotomocupy_b200.synthetic import make_problem
+    args, data, prb0, pos0, _ = make_problem(64, 112, 4, 21)
+    out = []
+    st = torch.cuda.Stream()
+    for mode in ("host", "device", "graph"):
+        with torch.cuda.stream(st):
+            rec = Rec(args)
+            rec.data.copy_(data)
+            rec.vars["prb"].copy_(prb0)
+            rec.vars["pos"].copy_(pos0)
+            rec.bh_setup()
+            hist = []
+            for i in range(4):
+                if mode == "host":
+                    hist.append(rec.bh_iteration(i))
+                elif mode == "device" or i == 0:
+                    rec.bh_iteration(i, sync=False)
+                else:
+                    if rec._graph is None:
+                        rec.capture_iteration()
+                    rec.replay_iteration()
+            if mode != "host":
+                hist = [(a, b) for a, b in rec.bh_history()]
+            rec.bh_finish()
+            out.append((hist, {k: rec.vars[k].cpu().numpy() for k in ("obj", "prb", "pos")}))
+            rec.release_graph()
+    h0, v0 = out[0]
+    for h, v in out[1:]:
+        np.testing.assert_allclose(np.array(h), np.array(h0), rtol=1e-9)
+        for k in v0:
+            assert rel_l2(v[k], v0[k]) < 1e-6
