@@ -162,6 +162,24 @@ def run_reference(a, rank):
 
 
 # ------------------------------------------------------------------ GPU
+def max_over_ranks(values, device):
+    """Element-wise max over the ranks of the process group (the times of
+    independent replicas); identity without one."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return [float(v) for v in values]
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(v) for v in t.tolist()]
+
+
+def replica_value(ms_max, world):
+    """Whole-job BH iterations/s of `world` replicas whose slowest rank took
+    ms_max per iteration."""
+    return world * 1e3 / ms_max
+
+
 def build_problem(n, ntheta, ndist, seed, device):
     import torch
     from holotomocupy_b200 import synthetic
@@ -245,7 +263,8 @@ def main():
     torch.cuda.synchronize()
     st = torch.cuda.current_stream()
     lat_plain = []
-    l0 = _lib.lib().ht_launch_count()
+    for k in KERNEL_BYTES:
+        _lib.call("ht_ktimer_arm", k.encode(), 1)
     p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     p0.record(st)
     for _ in range(a.steps):
@@ -257,7 +276,7 @@ def main():
         it += 1
     p1.record(st)
     torch.cuda.synchronize()
-    launches = (_lib.lib().ht_launch_count() - l0) / a.steps
+    ktimes = kernel_times(rec)
     ms_plain = p0.elapsed_time(p1) / a.steps
     lat_plain = sorted(s.elapsed_time(e) for s, e in lat_plain)
     rec.bh_finish()
@@ -268,7 +287,9 @@ def main():
         reset_state(rec, prb0, pos0)
         rec.bh_setup()
         rec.bh_iteration(0, sync=False)
+        l0 = _lib.lib().ht_launch_count()
         rec.capture_iteration()
+        launches = _lib.lib().ht_launch_count() - l0     # kernels recorded in one replayed iteration
         for _ in range(a.warmup - 1):
             rec.replay_iteration()
     torch.cuda.synchronize()
@@ -292,17 +313,14 @@ def main():
     clk = clocks.stop()
     ms = e0.elapsed_time(e1) / a.steps
     per_lat = sorted(s.elapsed_time(e) for s, e in lat)
-    if world > 1:
-        t = torch.tensor([ms, ms_plain], device=device)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms, ms_plain = float(t[0]), float(t[1])
+    ms, ms_plain = max_over_ranks([ms, ms_plain], device)
     with torch.cuda.stream(sst):
         rec.release_graph()
     rec.bh_finish()
-    value = world * 1e3 / ms
+    value = replica_value(ms, world)
 
     # ---- roofline of the dominant kernel family (the propagator passes)
-    roof = None if a.profile else roofline(rec, device)
+    roof = None if a.profile else roofline(ktimes)
 
     # ---- end to end through the public API with pinned host buffers
     e2e = None if a.profile else end_to_end(a, rec, obj_true, prb0, pos0, data, device, barrier, world)
@@ -324,7 +342,7 @@ def main():
                    "form": "served: device step sizes, iteration replayed from a CUDA graph",
                    "l2": "inputs larger than L2 (state ~60 GB)", "latency_ms_p50": float(np.percentile(per_lat, 50)),
                    "latency_ms_p99": float(np.percentile(per_lat, 99))},
-        "plain": {"value": world * 1e3 / ms_plain, "unit": UNIT, "ms_per_step": ms_plain,
+        "plain": {"value": replica_value(ms_plain, world), "unit": UNIT, "ms_per_step": ms_plain,
                   "latency_ms_p50": float(np.percentile(lat_plain, 50)),
                   "latency_ms_p99": float(np.percentile(lat_plain, 99)),
                   "form": "host step sizes (H and dots copied to the host each iteration), eager launches"},
@@ -379,40 +397,81 @@ def served_vs_plain(nreq, niter, seed):
             "max_concurrent": srv.max_concurrent, "peak_bytes_admitted": srv.peak_bytes}
 
 
-def roofline(rec, device):
-    """Time the propagator D over every (angle, distance) image of the
-    workload with CUDA events and report algorithmic bytes / time against the
-    measured HBM copy bandwidth."""
-    import torch
+# Algorithmic HBM bytes per work unit of each timed kernel (inputs read once,
+# outputs written once, at their stored types; a unit is one detector image
+# for the cascade and column kernels -- one image and one direction for the
+# two Hessian kernels -- and one object slice for the Radon kernels), and the
+# DRAM bytes per unit one ncu capture measured (256^3 object, 448 angles, 4
+# distances: 1792 images, 256 slices).
+KERNEL_BYTES = {
+    # c read (its share per image), u's DCT-II rows written
+    "k_casc_fwd": lambda r: 8 * r.nz * r.n + 8 * r.nzobj * r.nobj / r.ndist,
+    # spectrum and data read; x0 and the g0 spectrum written
+    "k_casc_resid": lambda r: 28 * r.nz * r.n,
+    # spectrum and c read; P and the horizontal S^T rows written
+    "k_casc_adj": lambda r: 16 * r.nz * r.n + 8 * r.nz * r.nobj + 8 * r.nzobj * r.nobj / r.ndist,
+    # two directions: c, c_y, c_z and P read, two spectra written
+    "k_casc_hess_fwd": lambda r: 12 * r.nz * r.n + 12 * r.nzobj * r.nobj / r.ndist,
+    # two directions: two spectra, x0 and data read
+    "k_casc_hess_q": lambda r: 14 * r.nz * r.n,
+    # one column pass of one image, in place
+    "k_dct_cols": lambda r: 16 * r.nz * r.n,
+    # the Fourier-grid disc the polar samples reach (radius n + m) read; sinogram rows written
+    "k_tgather": lambda r: 8 * np.pi * (r.nobj + 4) ** 2 + 8 * r.ntheta * r.nobj,
+    # sinogram spectra read; the 2n x 2n Fourier grid written
+    "k_tcell": lambda r: 8 * r.ntheta * r.nobj + 32 * r.nobj ** 2,
+}
+NCU_BYTES_PER_UNIT = {   # (dram__bytes_read.sum + dram__bytes_write.sum) / units of the captured launch
+    "k_casc_fwd": 1.122054e9 / 1792,
+    "k_casc_adj": 3.008112e9 / 1792,
+    "k_casc_hess_fwd": 3.496856e9 / (2 * 1792),
+    "k_dct_cols": 1.827770e9 / 1792,
+    "k_tgather": 0.651947e9 / 256,
+    "k_tcell": 0.739341e9 / 256,
+}
+
+
+def kernel_times(rec):
+    """Per-kernel launches, mean CUDA-event duration and work units recorded
+    by the library's timers during the plain timed iterations."""
+    import ctypes
     from holotomocupy_b200 import _lib
+    out = {}
+    for k in KERNEL_BYTES:
+        ms, n, u = ctypes.c_double(), ctypes.c_long(), ctypes.c_double()
+        _lib.call("ht_ktimer_read", k.encode(), ctypes.byref(ms), ctypes.byref(n), ctypes.byref(u))
+        _lib.call("ht_ktimer_arm", k.encode(), 0)
+        if n.value:
+            per_unit = float(KERNEL_BYTES[k](rec))
+            out[k] = {"launches": n.value, "ms": ms.value / n.value, "units": u.value / n.value,
+                      "alg_bytes": per_unit * u.value / n.value}
+    return out
+
+
+def roofline(kt):
+    """The dominant kernel (largest summed time) against the measured HBM
+    copy bandwidth, and the same figures for the other timed kernels."""
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
     except Exception:
         pass
     peak = float(peaks.get("hbm_gbs", 6650.0))
-    nimg = rec.ntheta * rec.ndist
-    x = torch.empty(nimg, rec.nz, rec.n, dtype=torch.complex64, device=device)
-    x.normal_()
-    y = torch.empty_like(x)
-    st = _lib.stream_ptr()
-    for _ in range(2):
-        _lib.call("ht_prop_D", rec.cl_prop._h, _lib.ptr(x), _lib.ptr(y), nimg, 0, st)
-    torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    reps = 5
-    e0.record()
-    for _ in range(reps):
-        _lib.call("ht_prop_D", rec.cl_prop._h, _lib.ptr(x), _lib.ptr(y), nimg, 0, st)
-    e1.record()
-    torch.cuda.synchronize()
-    t = e0.elapsed_time(e1) / reps * 1e-3
-    alg = 16.0 * nimg * rec.nz * rec.n + 32.0 * rec.nz * rec.n
-    achieved = alg / t / 1e9
-    del x, y
-    return {"bound": "hbm", "kernel": "propagator D (row DCT-II, column DCT/table/DCT, row DCT-III) over all images",
-            "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": None,
-            "peak_source": "measured" if peaks else "fallback", "launch_ms": t * 1e3}
+    if not kt:
+        return None
+    rows = {}
+    for k, v in kt.items():
+        gbs = v["alg_bytes"] / (v["ms"] * 1e-3) / 1e9
+        traffic = NCU_BYTES_PER_UNIT[k] * v["units"] if k in NCU_BYTES_PER_UNIT else None   # per launch
+        rows[k] = {"launch_ms": v["ms"], "launches": v["launches"], "alg_bytes": v["alg_bytes"], "achieved": gbs,
+                   "frac": gbs / peak, "traffic": traffic, "total_ms": v["ms"] * v["launches"]}
+    dom = max(rows, key=lambda k: rows[k]["total_ms"])
+    d = rows[dom]
+    return {"bound": "hbm", "kernel": dom, "achieved": d["achieved"], "peak": peak, "unit": "GB/s",
+            "frac": d["frac"], "traffic": d["traffic"], "peak_source": "measured" if peaks else "fallback",
+            "launch_ms": d["launch_ms"],
+            "traffic_source": "ncu dram bytes per unit at 256^3/448 angles, scaled by units processed",
+            "kernels": rows}
 
 
 def end_to_end(a, rec, obj_true, prb0, pos0, data, device, barrier, world):

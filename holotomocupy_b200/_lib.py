@@ -44,6 +44,8 @@ SIGNATURES = {
     "ht_graph_end": [_vp, ctypes.POINTER(_vp)],
     "ht_graph_launch": [_vp, _vp],
     "ht_graph_destroy": [_vp],
+    "ht_ktimer_arm": [ctypes.c_char_p, _c_int],
+    "ht_ktimer_read": [ctypes.c_char_p, ctypes.POINTER(_c_double), ctypes.POINTER(_c_long), ctypes.POINTER(_c_double)],
     "ht_rec_create": [_c_int, _c_int, _c_int, _c_int, _c_int, _c_int, _c_int, _vp, ctypes.POINTER(_vp)],
     "ht_rec_destroy": [_vp],
     "ht_rec_forward": [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],

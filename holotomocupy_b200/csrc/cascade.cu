@@ -785,8 +785,12 @@ static cudaError_t fwd_pass(ht_rec_s* r, const void* c, const float* pos, const 
   const long nrows = r->D.nimg * r->D.nz;
   cudaError_t e = allow_smem(k_casc_fwd<N, T>, CF::SMEM);
   if (e != cudaSuccess) return e;
-  k_casc_fwd<N, T><<<HT_ROWS_GRID(N, nrows), CF::THREADS, CF::SMEM, st>>>((const T*)c, pos, mag, prb, r->tmp, r->D,
-                                                                           twn); ::ht::count_launch();
+  {
+    KTimer kt("k_casc_fwd", st, (double)r->D.nimg);
+    k_casc_fwd<N, T><<<HT_ROWS_GRID(N, nrows), CF::THREADS, CF::SMEM, st>>>((const T*)c, pos, mag, prb, r->tmp,
+                                                                             r->D, twn);
+  }
+  ::ht::count_launch();
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   return dct_cols(r->D.nz, false, r->tmp, r->D.nimg, N, hw, r->D.ndist, twz, st);
 }
@@ -799,8 +803,12 @@ static cudaError_t resid_pass(ht_rec_s* r, const float* data, float* amp, float 
   cudaError_t e = allow_smem(k_casc_resid<N, MODE>, smem);
   if (e != cudaSuccess) return e;
   const long nrows = r->D.nimg * r->D.nz;
-  k_casc_resid<N, MODE><<<HT_ROWS_GRID(N, nrows), CF::THREADS, smem, st>>>(r->tmp, r->x0, data, amp, r->glob, scale,
-                                                                           r->D, twn); ::ht::count_launch();
+  {
+    KTimer kt(MODE == 0 ? "k_casc_resid" : "k_casc_resid_f", st, (double)r->D.nimg);
+    k_casc_resid<N, MODE><<<HT_ROWS_GRID(N, nrows), CF::THREADS, smem, st>>>(r->tmp, r->x0, data, amp, r->glob,
+                                                                             scale, r->D, twn);
+  }
+  ::ht::count_launch();
   return cudaGetLastError();
 }
 
@@ -818,8 +826,12 @@ static cudaError_t grad_impl(ht_rec_s* r, const void* c, const float* pos, const
   const int smem = CF::SMEM + red_doubles<CF::T>(5, CF::THREADS) * (int)sizeof(double);
   if ((e = allow_smem(k_casc_adj<N, T>, smem)) != cudaSuccess) return e;
   T* hbuf = reinterpret_cast<T*>(r->tmp + nrows * N);
-  k_casc_adj<N, T><<<HT_ROWS_GRID(N, nrows), CF::THREADS, smem, st>>>(r->tmp, r->P, hbuf, (const T*)c, pos, mag,
-                                                                      prb, r->acc_img, r->D, twn); ::ht::count_launch();
+  {
+    KTimer kt("k_casc_adj", st, (double)r->D.nimg);
+    k_casc_adj<N, T><<<HT_ROWS_GRID(N, nrows), CF::THREADS, smem, st>>>(r->tmp, r->P, hbuf, (const T*)c, pos, mag,
+                                                                        prb, r->acc_img, r->D, twn);
+  }
+  ::ht::count_launch();
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   const long npix = (long)r->D.nz * N;
   k_sum_theta<<<(unsigned)((r->D.ndist * npix + 255) / 256), 256, 0, st>>>(r->P, gprb, r->ntheta, r->D.ndist, npix); ::ht::count_launch();
@@ -840,14 +852,23 @@ static cudaError_t hess_impl(ht_rec_s* r, const void* c, const float* pos, const
   const int smem = NDIR * CF::SMEM + red_doubles<CF::T>(NDIR == 2 ? 10 : 4, CF::THREADS) * (int)sizeof(double);
   cudaError_t e = allow_smem(k_casc_hess_fwd<N, T, NDIR>, smem);
   if (e != cudaSuccess) return e;
-  k_casc_hess_fwd<N, T, NDIR><<<HT_ROWS_GRID(N, nrows), CF::THREADS, smem, st>>>(
-      (const T*)c, pos, mag, prb, r->P, (const T*)c0, p0, q0, (const T*)c1, p1, q1, r->tmp, r->acc_img, r->glob,
-      r->D, twn); ::ht::count_launch();
+  {
+    KTimer kt("k_casc_hess_fwd", st, (double)NDIR * r->D.nimg);
+    k_casc_hess_fwd<N, T, NDIR><<<HT_ROWS_GRID(N, nrows), CF::THREADS, smem, st>>>(
+        (const T*)c, pos, mag, prb, r->P, (const T*)c0, p0, q0, (const T*)c1, p1, q1, r->tmp, r->acc_img, r->glob,
+        r->D, twn);
+  }
+  ::ht::count_launch();
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   if ((e = dct_cols(r->D.nz, false, r->tmp, NDIR * r->D.nimg, N, hw, r->D.ndist, twz, st)) != cudaSuccess) return e;
   const int smq = NDIR * CF::SMEM + red_doubles<CF::T>(3, CF::THREADS) * (int)sizeof(double);
   if ((e = allow_smem(k_casc_hess_q<N, NDIR>, smq)) != cudaSuccess) return e;
-  k_casc_hess_q<N, NDIR><<<HT_ROWS_GRID(N, nrows), CF::THREADS, smq, st>>>(r->tmp, r->x0, data, r->glob, r->D, twn); ::ht::count_launch();
+  {
+    KTimer kt("k_casc_hess_q", st, (double)NDIR * r->D.nimg);
+    k_casc_hess_q<N, NDIR><<<HT_ROWS_GRID(N, nrows), CF::THREADS, smq, st>>>(r->tmp, r->x0, data, r->glob, r->D,
+                                                                             twn);
+  }
+  ::ht::count_launch();
   return cudaGetLastError();
 }
 

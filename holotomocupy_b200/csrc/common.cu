@@ -42,6 +42,44 @@ void smem_attr_mark(const void* kernel, int bytes) {
   if (bytes > b) b = bytes;
 }
 
+// ------------------------------------------------------------- timers
+namespace {
+struct TimerState {
+  bool armed = false;
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev;
+  double units = 0.0;
+};
+std::mutex g_timer_mutex;
+std::map<std::string, TimerState> g_timers;
+std::vector<std::pair<std::string, size_t>> g_timer_slots;  // slot -> (name, pair index)
+}  // namespace
+
+KTimer::KTimer(const char* name, cudaStream_t stream, double units) : st(stream) {
+  std::lock_guard<std::mutex> lock(g_timer_mutex);
+  auto it = g_timers.find(name);
+  if (it == g_timers.end() || !it->second.armed) return;
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(stream, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) return;
+  cudaEvent_t a = nullptr, b = nullptr;
+  if (cudaEventCreate(&a) != cudaSuccess) return;
+  if (cudaEventCreate(&b) != cudaSuccess) {
+    cudaEventDestroy(a);
+    return;
+  }
+  cudaEventRecord(a, stream);
+  it->second.ev.emplace_back(a, b);
+  it->second.units += units;
+  g_timer_slots.emplace_back(name, it->second.ev.size() - 1);
+  slot = (int)g_timer_slots.size() - 1;
+}
+
+KTimer::~KTimer() {
+  if (slot < 0) return;
+  std::lock_guard<std::mutex> lock(g_timer_mutex);
+  const auto& s = g_timer_slots[slot];
+  cudaEventRecord(g_timers[s.first].ev[s.second].second, st);
+}
+
 void set_error(const std::string& msg) { g_last_error = msg; }
 const char* last_error() { return g_last_error.c_str(); }
 
@@ -80,3 +118,40 @@ const float2* twiddle_table(int N, int device) {
 }
 
 }  // namespace ht
+
+extern "C" int ht_ktimer_arm(const char* name, int on) {
+  using namespace ht;
+  HT_REQUIRE(name, "ht_ktimer_arm: null name");
+  std::lock_guard<std::mutex> lock(g_timer_mutex);
+  TimerState& t = g_timers[name];
+  for (auto& p : t.ev) {
+    cudaEventDestroy(p.first);
+    cudaEventDestroy(p.second);
+  }
+  t.ev.clear();
+  t.units = 0.0;
+  g_timer_slots.clear();
+  t.armed = on != 0;
+  return kOk;
+}
+
+extern "C" int ht_ktimer_read(const char* name, double* total_ms, long* launches, double* units) {
+  using namespace ht;
+  HT_REQUIRE(name && total_ms && launches && units, "ht_ktimer_read: null pointer");
+  std::lock_guard<std::mutex> lock(g_timer_mutex);
+  double tot = 0.0;
+  long n = 0;
+  auto it = g_timers.find(name);
+  *units = it != g_timers.end() ? it->second.units : 0.0;
+  if (it != g_timers.end())
+    for (auto& p : it->second.ev) {
+      HT_CHECK_CUDA(cudaEventSynchronize(p.second));
+      float ms = 0.f;
+      HT_CHECK_CUDA(cudaEventElapsedTime(&ms, p.first, p.second));
+      tot += ms;
+      ++n;
+    }
+  *total_ms = tot;
+  *launches = n;
+  return kOk;
+}

@@ -63,6 +63,17 @@ const float2* twiddle_table(int N, int device);  // nullptr + error on failure
 void count_launch();
 long launch_count();
 
+// Per-kernel CUDA-event timers (read through ht_ktimer_*).  A KTimer around a
+// launch records an event pair on the launch stream when the kernel's timer
+// is armed and the stream is not being captured into a graph; `units` is the
+// work of the launch (images, or slices for the Radon kernels).
+struct KTimer {
+  int slot = -1;
+  cudaStream_t st = nullptr;
+  KTimer(const char* name, cudaStream_t stream, double units);
+  ~KTimer();
+};
+
 // Sizes accepted by the line transforms: N = 2^a 3^b from the list below.
 bool fft_size_supported(int N);
 

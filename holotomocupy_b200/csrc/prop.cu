@@ -162,11 +162,19 @@ static cudaError_t launch_dct_cols(bool conj, float2* data, long nimg, int n, co
   if (conj) {
     cudaError_t e = allow_smem(k_dct_cols<NZ, true>, CF::SMEM);
     if (e != cudaSuccess) return e;
-    k_dct_cols<NZ, true><<<grid, CF::THREADS, CF::SMEM, st>>>(data, n, H, ntab, tw4); ::ht::count_launch();
+    {
+      KTimer kt("k_dct_cols", st, (double)nimg);
+      k_dct_cols<NZ, true><<<grid, CF::THREADS, CF::SMEM, st>>>(data, n, H, ntab, tw4);
+    }
+    ::ht::count_launch();
   } else {
     cudaError_t e = allow_smem(k_dct_cols<NZ, false>, CF::SMEM);
     if (e != cudaSuccess) return e;
-    k_dct_cols<NZ, false><<<grid, CF::THREADS, CF::SMEM, st>>>(data, n, H, ntab, tw4); ::ht::count_launch();
+    {
+      KTimer kt("k_dct_cols", st, (double)nimg);
+      k_dct_cols<NZ, false><<<grid, CF::THREADS, CF::SMEM, st>>>(data, n, H, ntab, tw4);
+    }
+    ::ht::count_launch();
   }
   return cudaGetLastError();
 }

@@ -430,7 +430,10 @@ static cudaError_t tomo_R_sized(const float2* obj, float2* sino, const float* ph
   count_launch();
   k_tcol_fwd<N2><<<dim3(N2, nzb), C2::THREADS, C2::SMEM, st>>>(fa, fde, tw_2n);
   count_launch();
-  k_tgather<n><<<dim3(G.ntheta, nzb), C1::THREADS, C1::SMEM, st>>>(fde, sino, G, nz, tw_n);
+  {
+    KTimer kt("k_tgather", st, (double)nz);
+    k_tgather<n><<<dim3(G.ntheta, nzb), C1::THREADS, C1::SMEM, st>>>(fde, sino, G, nz, tw_n);
+  }
   count_launch();
   return cudaGetLastError();
 }
@@ -450,7 +453,10 @@ static cudaError_t tomo_RT_sized(const float2* sino, float2* obj, const float* p
   if ((e = allow_smem(k_trow_adj<N2>, C2::SMEM)) != cudaSuccess) return e;
   k_tsino_fft<n><<<dim3(G.ntheta, nzb), C1::THREADS, C1::SMEM, st>>>(sino, gs, G.ntheta, nz, tw_n);
   count_launch();
-  k_tcell<Z><<<dim3((N2 + 15) / 16, (N2 + 15) / 16, nzb), dim3(16, 16), 0, st>>>(gs, fde, G);
+  {
+    KTimer kt("k_tcell", st, (double)nz);
+    k_tcell<Z><<<dim3((N2 + 15) / 16, (N2 + 15) / 16, nzb), dim3(16, 16), 0, st>>>(gs, fde, G);
+  }
   count_launch();
   k_tcol_adj<N2><<<dim3(N2, nzb), C2::THREADS, C2::SMEM, st>>>(fde, fab, tw_2n);
   count_launch();

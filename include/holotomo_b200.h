@@ -218,6 +218,17 @@ int ht_graph_end(void* stream, void** exec);
 int ht_graph_launch(void* exec, void* stream);
 int ht_graph_destroy(void* exec);
 
+/* Per-kernel CUDA-event timers (instrumentation; no counterpart).  Arming a
+ * kernel's timer (names: k_casc_fwd, k_casc_resid, k_casc_resid_f,
+ * k_casc_adj, k_casc_hess_fwd, k_casc_hess_q, k_dct_cols, k_tgather,
+ * k_tcell) clears its record; while armed, every launch of it outside graph
+ * capture is bracketed by an event pair on its stream.  ht_ktimer_read
+ * waits for the recorded launches and returns their summed time, their
+ * count and their summed work units (images for the cascade and column
+ * kernels, slices for k_tgather and k_tcell). */
+int ht_ktimer_arm(const char* name, int on);
+int ht_ktimer_read(const char* name, double* total_ms, long* launches, double* units);
+
 #ifdef __cplusplus
 }
 #endif
