@@ -32,6 +32,7 @@ import subprocess
 import sys
 import tempfile
 import time
+import types
 
 import numpy as np
 
@@ -421,14 +422,25 @@ KERNEL_BYTES = {
     # sinogram spectra read; the 2n x 2n Fourier grid written
     "k_tcell": lambda r: 8 * r.ntheta * r.nobj + 32 * r.nobj ** 2,
 }
-NCU_BYTES_PER_UNIT = {   # (dram__bytes_read.sum + dram__bytes_write.sum) / units of the captured launch
-    "k_casc_fwd": 1.122054e9 / 1792,
-    "k_casc_adj": 3.008112e9 / 1792,
-    "k_casc_hess_fwd": 3.496856e9 / (2 * 1792),
-    "k_dct_cols": 1.827770e9 / 1792,
-    "k_tgather": 0.651947e9 / 256,
-    "k_tcell": 0.739341e9 / 256,
+# (dram__bytes_read.sum + dram__bytes_write.sum) of one captured launch and its
+# work units, at the 256^3 / 448-angle capture; traffic at other sizes is this
+# ratio to the algorithmic bytes times the algorithmic bytes there.
+_NCU_CASE = types.SimpleNamespace(n=256, nz=256, nobj=256, nzobj=256, ntheta=448, ndist=4)
+NCU_CAPTURE = {
+    "k_casc_fwd": (1.122054e9, 1792),
+    "k_casc_adj": (3.008112e9, 1792),
+    "k_casc_hess_fwd": (3.496856e9, 2 * 1792),
+    "k_dct_cols": (1.827770e9, 1792),
+    "k_tgather": (0.651947e9, 256),
+    "k_tcell": (0.739341e9, 256),
 }
+
+
+def ncu_traffic_ratio(k):
+    if k not in NCU_CAPTURE:
+        return None
+    b, units = NCU_CAPTURE[k]
+    return b / (KERNEL_BYTES[k](_NCU_CASE) * units)
 
 
 def kernel_times(rec):
@@ -462,7 +474,8 @@ def roofline(kt):
     rows = {}
     for k, v in kt.items():
         gbs = v["alg_bytes"] / (v["ms"] * 1e-3) / 1e9
-        traffic = NCU_BYTES_PER_UNIT[k] * v["units"] if k in NCU_BYTES_PER_UNIT else None   # per launch
+        ratio = ncu_traffic_ratio(k)
+        traffic = ratio * v["alg_bytes"] if ratio is not None else None   # per launch
         rows[k] = {"launch_ms": v["ms"], "launches": v["launches"], "alg_bytes": v["alg_bytes"], "achieved": gbs,
                    "frac": gbs / peak, "traffic": traffic, "total_ms": v["ms"] * v["launches"]}
     dom = max(rows, key=lambda k: rows[k]["total_ms"])
@@ -470,7 +483,8 @@ def roofline(kt):
     return {"bound": "hbm", "kernel": dom, "achieved": d["achieved"], "peak": peak, "unit": "GB/s",
             "frac": d["frac"], "traffic": d["traffic"], "peak_source": "measured" if peaks else "fallback",
             "launch_ms": d["launch_ms"],
-            "traffic_source": "ncu dram bytes per unit at 256^3/448 angles, scaled by units processed",
+            "traffic_source": "ncu dram bytes / algorithmic bytes of one launch at 256^3, 448 angles, times the "
+                              "algorithmic bytes of this launch",
             "kernels": rows}
 
 

@@ -201,6 +201,54 @@ __host__ __device__ constexpr int red_doubles(int K, int threads) {
   return (T % 32 == 0) ? K * (threads / 32) : K * threads;
 }
 
+// Launch shape of a stencil row kernel: NFFT row lines of the DCT plus NSET
+// vertically reduced object rows (nobj <= N values each) per detector row,
+// with as many detector rows per CTA as keep the shared memory near 100 KB.
+template <int N, int NSET, int NFFT>
+struct StCfg {
+  static constexpr int T = Plan<N>::T;
+  static constexpr int PER_LINE = NFFT * SmRow::padded(N) * 8 + NSET * N * 8;
+  static constexpr int fit(int l) { return (l > 1 && l * PER_LINE > 100 * 1024) ? fit(l / 2) : l; }
+  static constexpr int LINES = fit(RowCfg<N>::LINES);
+  static constexpr int THREADS = LINES * T;
+  // dynamic shared memory: FFT lines, then reduction scratch, then the rows
+  static constexpr int FFT_BYTES = LINES * NFFT * SmRow::padded(N) * 8;
+  static int bytes(int K, int nobj, int elem) {
+    return FFT_BYTES + red_doubles<T>(K, THREADS) * 8 + LINES * NSET * nobj * elem;
+  }
+};
+
+// Vertical pass of a detector row: V[s][ix] = sum_jy w_s[jy] c[yy[jy], ix]
+// for the weight sets w_s of the row (every object column ix, by the T threads
+// of the line).  The horizontal taps then read V from shared memory.
+template <class T, int NS>
+__device__ __forceinline__ void vrows(T* __restrict__ V, int nobj, const T* __restrict__ cb, const int (&yy)[4],
+                                      const float* const (&w)[NS], int t, int TT) {
+  const T* r0 = cb + (long)yy[0] * nobj;
+  const T* r1 = cb + (long)yy[1] * nobj;
+  const T* r2 = cb + (long)yy[2] * nobj;
+  const T* r3 = cb + (long)yy[3] * nobj;
+  for (int ix = t; ix < nobj; ix += TT) {
+    const T v0 = __ldg(&r0[ix]), v1 = __ldg(&r1[ix]), v2 = __ldg(&r2[ix]), v3 = __ldg(&r3[ix]);
+#pragma unroll
+    for (int k = 0; k < NS; ++k) {
+      T a = El<T>::zero();
+      El<T>::fma(a, w[k][0], v0);
+      El<T>::fma(a, w[k][1], v1);
+      El<T>::fma(a, w[k][2], v2);
+      El<T>::fma(a, w[k][3], v3);
+      V[k * nobj + ix] = a;
+    }
+  }
+}
+
+// the four samples of a vertically reduced row under a pixel's stencil
+template <class T>
+__device__ __forceinline__ void vrow4(const T* __restrict__ V, const int (&xx)[4], T (&v)[4]) {
+#pragma unroll
+  for (int j = 0; j < 4; ++j) v[j] = V[xx[j]];
+}
+
 // Per-image accumulator slots
 enum Acc : int { kAx = 0, kAy, kHxx, kHxy, kHyy, kAyx, kAyy, kAzx, kAzy, kNAcc };
 // Global accumulator slots
@@ -209,34 +257,36 @@ enum Glob : int { kF = 0, kQ0, kQ1, kQ2, kL10, kL11, kL12, kL20, kL21, kL22, kNG
 // ================================================= forward row pass
 // u = prb[k] exp(i S(c)) -> row DCT-II -> tmp
 template <int N, class T>
-__global__ void __launch_bounds__(RowCfg<N>::THREADS)
+__global__ void __launch_bounds__(StCfg<N, 1, 1>::THREADS)
 k_casc_fwd(const T* __restrict__ c, const float* __restrict__ pos, const float* __restrict__ mag,
            const float2* __restrict__ prb, float2* __restrict__ tmp, CascDims D, const float2* __restrict__ tw4) {
-  constexpr int TT = RowCfg<N>::T;
+  using CF = StCfg<N, 1, 1>;
+  constexpr int TT = CF::T;
   extern __shared__ float2 smem[];
   const int line = threadIdx.x / TT, t = threadIdx.x % TT;
-  const long row = (long)blockIdx.x * RowCfg<N>::LINES + line;  // img * nz + ty
+  const long row = (long)blockIdx.x * CF::LINES + line;  // img * nz + ty
   const bool valid = row < D.nimg * D.nz;
   const long img = valid ? row / D.nz : 0;
   const int ty = valid ? (int)(row % D.nz) : 0;
   const int k = (int)(img % D.ndist);
   const long th = img / D.ndist;
   SmRow sm{smem + line * SmRow::padded(N)};
-  const T* cb = c + th * (long)D.nzobj * D.nobj;
+  T* V = reinterpret_cast<T*>(reinterpret_cast<char*>(smem) + CF::FFT_BYTES) + (long)line * D.nobj;
   const float m0 = valid ? mag[img] : 1.f;
   const float2 r = valid ? ld_pos(pos, img) : make_float2(0.f, 0.f);
   const RowGeo<0> rg(D, m0, r.x, ty);
+  if (valid) {
+    const float* const w[1] = {rg.py};
+    vrows<T, 1>(V, D.nobj, c + th * (long)D.nzobj * D.nobj, rg.yy, w, t, TT);
+  }
+  __syncthreads();
   for (int tx = t; tx < N; tx += TT) {
     float2 u = make_float2(0.f, 0.f);
     if (valid) {
       const ColGeo<0> cg(D, m0, r.y, tx);
-      T x22 = El<T>::zero();
-#pragma unroll
-      for (int jy = 0; jy < 4; ++jy) {
-        T v[4];
-        row4(cb + (long)rg.yy[jy] * D.nobj, cg.xx, v);
-        El<T>::fma(x22, rg.py[jy], dot4(cg.px, v));
-      }
+      T v[4];
+      vrow4(V, cg.xx, v);
+      const T x22 = dot4(cg.px, v);
       u = cmul(prb[((long)k * D.nz + ty) * N + tx], cexp_i(El<T>::cplx(x22)));
     }
     dct2_put<N>(sm, tx, u);
@@ -324,27 +374,35 @@ __device__ __forceinline__ void cand_range(float m0, float C0, int i, int nhalf,
 // column ix, hrow[ix] = sum_tx px(tx -> ix) Y22[tx]  (the vertical half is
 // k_casc_vsum; S is separable, so S^T is too).
 template <int N, class T>
-__global__ void __launch_bounds__(RowCfg<N>::THREADS)
+__global__ void __launch_bounds__(StCfg<N, 3, 1>::THREADS)
 k_casc_adj(const float2* __restrict__ tmp, float2* __restrict__ Pc, T* __restrict__ hbuf, const T* __restrict__ c,
            const float* __restrict__ pos, const float* __restrict__ mag, const float2* __restrict__ prb,
            double* __restrict__ acc_img, CascDims D, const float2* __restrict__ tw4) {
-  constexpr int TT = RowCfg<N>::T;
+  using CF = StCfg<N, 3, 1>;
+  constexpr int TT = CF::T;
   constexpr int E = Plan<N>::E;
   extern __shared__ float2 smem[];
-  double* red = reinterpret_cast<double*>(smem + RowCfg<N>::LINES * SmRow::padded(N));
+  double* red = reinterpret_cast<double*>(reinterpret_cast<char*>(smem) + CF::FFT_BYTES);
   const int line = threadIdx.x / TT, t = threadIdx.x % TT;
-  const long row = (long)blockIdx.x * RowCfg<N>::LINES + line;
+  T* V = reinterpret_cast<T*>(red + red_doubles<TT>(5, CF::THREADS)) + (long)line * 3 * D.nobj;
+  const long row = (long)blockIdx.x * CF::LINES + line;
   const bool valid = row < D.nimg * D.nz;
   const long img = valid ? row / D.nz : 0;
   const int ty = valid ? (int)(row % D.nz) : 0;
   const int k = (int)(img % D.ndist);
   const long th = img / D.ndist;
   SmRow sm{smem + line * SmRow::padded(N)};
-  dct3_start<N, TT>(sm, t, tw4, tmp + row * N, valid);
-  const T* cb = c + th * (long)D.nzobj * D.nobj;
   const float m0 = valid ? mag[img] : 1.f;
   const float2 r = valid ? ld_pos(pos, img) : make_float2(0.f, 0.f);
   const RowGeo<2> rg(D, m0, r.x, ty);
+  if (valid) {
+    const float* const w[3] = {rg.py, rg.dpy, rg.d2py};
+    vrows<T, 3>(V, D.nobj, c + th * (long)D.nzobj * D.nobj, rg.yy, w, t, TT);
+  }
+  dct3_start<N, TT>(sm, t, tw4, tmp + row * N, valid);  // ends with a barrier: V is complete
+  const T* V0 = V;
+  const T* V1 = V + D.nobj;
+  const T* V2 = V + 2 * D.nobj;
   float s[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
   float2 Yr[E];
 #pragma unroll
@@ -354,20 +412,13 @@ k_casc_adj(const float2* __restrict__ tmp, float2* __restrict__ Pc, T* __restric
     if (!valid) continue;
     const float2 G = sm.ld(dct_perm(tx, N));
     const ColGeo<2> cg(D, m0, r.y, tx);
-    T x22 = El<T>::zero(), ax = El<T>::zero(), ay = El<T>::zero(), hxx = El<T>::zero(), hxy = El<T>::zero(),
-      hyy = El<T>::zero();
-#pragma unroll
-    for (int jy = 0; jy < 4; ++jy) {
-      T v[4];
-      row4(cb + (long)rg.yy[jy] * D.nobj, cg.xx, v);
-      const T h0 = dot4(cg.px, v), h1 = dot4(cg.dpx, v), h2 = dot4(cg.d2px, v);
-      El<T>::fma(x22, rg.py[jy], h0);
-      El<T>::fma(ax, rg.py[jy], h1);
-      El<T>::fma(ay, rg.dpy[jy], h0);
-      El<T>::fma(hxx, rg.py[jy], h2);
-      El<T>::fma(hxy, rg.dpy[jy], h1);
-      El<T>::fma(hyy, rg.d2py[jy], h0);
-    }
+    T v[4];
+    vrow4(V0, cg.xx, v);
+    const T x22 = dot4(cg.px, v), ax = dot4(cg.dpx, v), hxx = dot4(cg.d2px, v);
+    vrow4(V1, cg.xx, v);
+    const T ay = dot4(cg.px, v), hxy = dot4(cg.dpx, v);
+    vrow4(V2, cg.xx, v);
+    const T hyy = dot4(cg.px, v);
     const float2 x12 = cexp_i(El<T>::cplx(x22));
     const float2 P = cmulc(G, x12);
     Pc[row * N + tx] = P;
@@ -471,18 +522,22 @@ __global__ void k_casc_gpos(const double* __restrict__ acc_img, float* __restric
 // -> row DCT-II -> tmp[d];  plus the pointwise second-order sums L1, L2
 // (pairs 00, 01, 11) and the per-image Ax(c_d), Ay(c_d).
 template <int N, class T, int NDIR>
-__global__ void __launch_bounds__(RowCfg<N>::THREADS)
+__global__ void __launch_bounds__(StCfg<N, 2 * (1 + NDIR), NDIR>::THREADS)
 k_casc_hess_fwd(const T* __restrict__ c, const float* __restrict__ pos, const float* __restrict__ mag,
                 const float2* __restrict__ prb, const float2* __restrict__ Pc, const T* __restrict__ c0,
                 const float* __restrict__ pos0, const float2* __restrict__ prb0, const T* __restrict__ c1,
                 const float* __restrict__ pos1, const float2* __restrict__ prb1, float2* __restrict__ tmp,
                 double* __restrict__ acc_img, double* __restrict__ glob, CascDims D,
                 const float2* __restrict__ tw4) {
-  constexpr int TT = RowCfg<N>::T;
-  constexpr int LINES = RowCfg<N>::LINES;
+  constexpr int NS = 2 * (1 + NDIR);
+  using CF = StCfg<N, NS, NDIR>;
+  constexpr int TT = CF::T;
+  constexpr int LINES = CF::LINES;
+  constexpr int K = (NDIR == 2) ? 10 : 4;
   extern __shared__ float2 smem[];
-  double* red = reinterpret_cast<double*>(smem + NDIR * LINES * SmRow::padded(N));
+  double* red = reinterpret_cast<double*>(reinterpret_cast<char*>(smem) + CF::FFT_BYTES);
   const int line = threadIdx.x / TT, t = threadIdx.x % TT;
+  T* V = reinterpret_cast<T*>(red + red_doubles<TT>(K, CF::THREADS)) + (long)line * NS * D.nobj;
   const long row = (long)blockIdx.x * LINES + line;
   const bool valid = row < D.nimg * D.nz;
   const long img = valid ? row / D.nz : 0;
@@ -492,46 +547,43 @@ k_casc_hess_fwd(const T* __restrict__ c, const float* __restrict__ pos, const fl
   SmRow sm0{smem + line * SmRow::padded(N)};
   SmRow sm1{smem + (LINES + line) * SmRow::padded(N)};
   const long coff = th * (long)D.nzobj * D.nobj;
-  const T* cb = c + coff;
-  const T* cb0 = c0 + coff;
-  const T* cb1 = (NDIR == 2) ? c1 + coff : c0 + coff;
   const float m0 = valid ? mag[img] : 1.f;
   const float2 r = valid ? ld_pos(pos, img) : make_float2(0.f, 0.f);
   const float2 rd0 = valid ? ld_pos(pos0, img) : make_float2(0.f, 0.f);
   const float2 rd1 = (valid && NDIR == 2) ? ld_pos(pos1, img) : make_float2(0.f, 0.f);
-  const RowGeo<1> rg(D, m0, r.x, ty);
+  {
+    const RowGeo<1> rg(D, m0, r.x, ty);
+    if (valid) {
+      const float* const w[2] = {rg.py, rg.dpy};
+      // sets: (c, py) (c, dpy) (c_y, py) (c_y, dpy) [(c_z, py) (c_z, dpy)]
+      vrows<T, 2>(V, D.nobj, c + coff, rg.yy, w, t, TT);
+      vrows<T, 2>(V + 2 * D.nobj, D.nobj, c0 + coff, rg.yy, w, t, TT);
+      if (NDIR == 2) vrows<T, 2>(V + 4 * D.nobj, D.nobj, c1 + coff, rg.yy, w, t, TT);
+    }
+  }
+  __syncthreads();
   // sums: L1 00,01,11 ; L2 00,01,11 ; A: ax0, ay0, ax1, ay1
   float s[10] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
   for (int tx = t; tx < N; tx += TT) {
     float2 v0 = make_float2(0.f, 0.f), v1 = make_float2(0.f, 0.f);
     if (valid) {
       const ColGeo<1> cg(D, m0, r.y, tx);
-      T x22 = El<T>::zero(), dxc = El<T>::zero(), dyc = El<T>::zero();
-      T s0 = El<T>::zero(), ax0 = El<T>::zero(), ay0 = El<T>::zero();
+      T v[4];
+      vrow4(V, cg.xx, v);
+      const T x22 = dot4(cg.px, v), dxc = dot4(cg.dpx, v);
+      vrow4(V + D.nobj, cg.xx, v);
+      const T dyc = dot4(cg.px, v);
+      vrow4(V + 2 * D.nobj, cg.xx, v);
+      const T s0 = dot4(cg.px, v), ax0 = dot4(cg.dpx, v);
+      vrow4(V + 3 * D.nobj, cg.xx, v);
+      const T ay0 = dot4(cg.px, v);
       T s1 = El<T>::zero(), ax1 = El<T>::zero(), ay1 = El<T>::zero();
-#pragma unroll
-      for (int jy = 0; jy < 4; ++jy) {
-        const long ro = (long)rg.yy[jy] * D.nobj;
-        T v[4];
-        row4(cb + ro, cg.xx, v);
-        T h0 = dot4(cg.px, v), h1 = dot4(cg.dpx, v);
-        El<T>::fma(x22, rg.py[jy], h0);
-        El<T>::fma(dxc, rg.py[jy], h1);
-        El<T>::fma(dyc, rg.dpy[jy], h0);
-        row4(cb0 + ro, cg.xx, v);
-        h0 = dot4(cg.px, v);
-        h1 = dot4(cg.dpx, v);
-        El<T>::fma(s0, rg.py[jy], h0);
-        El<T>::fma(ax0, rg.py[jy], h1);
-        El<T>::fma(ay0, rg.dpy[jy], h0);
-        if (NDIR == 2) {
-          row4(cb1 + ro, cg.xx, v);
-          h0 = dot4(cg.px, v);
-          h1 = dot4(cg.dpx, v);
-          El<T>::fma(s1, rg.py[jy], h0);
-          El<T>::fma(ax1, rg.py[jy], h1);
-          El<T>::fma(ay1, rg.dpy[jy], h0);
-        }
+      if (NDIR == 2) {
+        vrow4(V + 4 * D.nobj, cg.xx, v);
+        s1 = dot4(cg.px, v);
+        ax1 = dot4(cg.dpx, v);
+        vrow4(V + 5 * D.nobj, cg.xx, v);
+        ay1 = dot4(cg.px, v);
       }
       // dS (rec_mpi.py:757; cuda_kernels.py:600-609): sum phi phi c_d - (dphi_x phi_y r_dx + phi_x dphi_y r_dy) c
       T y0 = s0, y1 = s1;
@@ -570,7 +622,6 @@ k_casc_hess_fwd(const T* __restrict__ c, const float* __restrict__ pos, const fl
     dct2_put<N>(sm0, tx, v0);
     if (NDIR == 2) dct2_put<N>(sm1, tx, v1);
   }
-  constexpr int K = (NDIR == 2) ? 10 : 4;
   double v[K];
   if (NDIR == 2) {
 #pragma unroll
@@ -778,20 +829,42 @@ extern "C" int ht_rec_destroy(ht_rec_s* r) {
 namespace ht {
 #define HT_ROWS_GRID(N, nrows) (unsigned)(((nrows) + RowCfg<N>::LINES - 1) / RowCfg<N>::LINES)
 
+// Dynamic shared memory of the stencil row kernels, checked against the device
+// limit (the vertically reduced rows grow with nobj).
+template <class CF>
+static cudaError_t stencil_smem(const void* kernel, int K, int nobj, int elem, int* bytes) {
+  *bytes = CF::bytes(K, nobj, elem);
+  if (*bytes > 227 * 1024) {
+    set_error("fused cascade: nobj = " + std::to_string(nobj) + " needs " + std::to_string(*bytes) +
+              " bytes of shared memory per block (limit 227 KB)");
+    return cudaErrorInvalidValue;
+  }
+  return cudaSuccess;
+}
+
+template <int N, class T>
+static cudaError_t launch_fwd(const CascDims& D, const T* c, const float* pos, const float* mag, const float2* prb,
+                              float2* tmp, const float2* twn, cudaStream_t st) {
+  using CF = StCfg<N, 1, 1>;
+  int smem = 0;
+  cudaError_t e = stencil_smem<CF>(nullptr, 0, D.nobj, (int)sizeof(T), &smem);
+  if (e == cudaSuccess) e = allow_smem(k_casc_fwd<N, T>, smem);
+  if (e != cudaSuccess) return e;
+  const long nrows = D.nimg * D.nz;
+  {
+    KTimer kt("k_casc_fwd", st, (double)D.nimg);
+    k_casc_fwd<N, T><<<(unsigned)((nrows + CF::LINES - 1) / CF::LINES), CF::THREADS, smem, st>>>(c, pos, mag, prb,
+                                                                                               tmp, D, twn);
+  }
+  ::ht::count_launch();
+  return cudaGetLastError();
+}
+
 template <int N, class T>
 static cudaError_t fwd_pass(ht_rec_s* r, const void* c, const float* pos, const float* mag, const float2* prb,
                             const float2* hw, const float2* twn, const float2* twz, cudaStream_t st) {
-  using CF = RowCfg<N>;
-  const long nrows = r->D.nimg * r->D.nz;
-  cudaError_t e = allow_smem(k_casc_fwd<N, T>, CF::SMEM);
+  cudaError_t e = launch_fwd<N, T>(r->D, (const T*)c, pos, mag, prb, r->tmp, twn, st);
   if (e != cudaSuccess) return e;
-  {
-    KTimer kt("k_casc_fwd", st, (double)r->D.nimg);
-    k_casc_fwd<N, T><<<HT_ROWS_GRID(N, nrows), CF::THREADS, CF::SMEM, st>>>((const T*)c, pos, mag, prb, r->tmp,
-                                                                             r->D, twn);
-  }
-  ::ht::count_launch();
-  if ((e = cudaGetLastError()) != cudaSuccess) return e;
   return dct_cols(r->D.nz, false, r->tmp, r->D.nimg, N, hw, r->D.ndist, twz, st);
 }
 
@@ -821,15 +894,16 @@ static cudaError_t grad_impl(ht_rec_s* r, const void* c, const float* pos, const
   if (e != cudaSuccess) return e;
   if ((e = resid_pass<N, 0>(r, data, nullptr, scale, twn, st)) != cudaSuccess) return e;
   if ((e = dct_cols(r->D.nz, true, r->tmp, r->D.nimg, N, hw, r->D.ndist, twz, st)) != cudaSuccess) return e;
-  using CF = RowCfg<N>;
+  using CA = StCfg<N, 3, 1>;
   const long nrows = r->D.nimg * r->D.nz;
-  const int smem = CF::SMEM + red_doubles<CF::T>(5, CF::THREADS) * (int)sizeof(double);
+  int smem = 0;
+  if ((e = stencil_smem<CA>(nullptr, 5, r->D.nobj, (int)sizeof(T), &smem)) != cudaSuccess) return e;
   if ((e = allow_smem(k_casc_adj<N, T>, smem)) != cudaSuccess) return e;
   T* hbuf = reinterpret_cast<T*>(r->tmp + nrows * N);
   {
     KTimer kt("k_casc_adj", st, (double)r->D.nimg);
-    k_casc_adj<N, T><<<HT_ROWS_GRID(N, nrows), CF::THREADS, smem, st>>>(r->tmp, r->P, hbuf, (const T*)c, pos, mag,
-                                                                        prb, r->acc_img, r->D, twn);
+    k_casc_adj<N, T><<<(unsigned)((nrows + CA::LINES - 1) / CA::LINES), CA::THREADS, smem, st>>>(
+        r->tmp, r->P, hbuf, (const T*)c, pos, mag, prb, r->acc_img, r->D, twn);
   }
   ::ht::count_launch();
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
@@ -848,13 +922,15 @@ static cudaError_t hess_impl(ht_rec_s* r, const void* c, const float* pos, const
   const float2 *hw, *twn, *twz;
   prop_tables(r->prop, &hw, &twn, &twz);
   using CF = RowCfg<N>;
+  using CH = StCfg<N, 2 * (1 + NDIR), NDIR>;
   const long nrows = r->D.nimg * r->D.nz;
-  const int smem = NDIR * CF::SMEM + red_doubles<CF::T>(NDIR == 2 ? 10 : 4, CF::THREADS) * (int)sizeof(double);
-  cudaError_t e = allow_smem(k_casc_hess_fwd<N, T, NDIR>, smem);
+  int smem = 0;
+  cudaError_t e = stencil_smem<CH>(nullptr, NDIR == 2 ? 10 : 4, r->D.nobj, (int)sizeof(T), &smem);
+  if (e == cudaSuccess) e = allow_smem(k_casc_hess_fwd<N, T, NDIR>, smem);
   if (e != cudaSuccess) return e;
   {
     KTimer kt("k_casc_hess_fwd", st, (double)NDIR * r->D.nimg);
-    k_casc_hess_fwd<N, T, NDIR><<<HT_ROWS_GRID(N, nrows), CF::THREADS, smem, st>>>(
+    k_casc_hess_fwd<N, T, NDIR><<<(unsigned)((nrows + CH::LINES - 1) / CH::LINES), CH::THREADS, smem, st>>>(
         (const T*)c, pos, mag, prb, r->P, (const T*)c0, p0, q0, (const T*)c1, p1, q1, r->tmp, r->acc_img, r->glob,
         r->D, twn);
   }
@@ -1011,17 +1087,15 @@ static cudaError_t noalloc_chunks(const ht_prop_s* prop, int nz, int nobj, int n
   const float2 *hw, *twn, *twz;
   prop_tables(prop, &hw, &twn, &twz);
   using CF = RowCfg<N>;
-  cudaError_t e = allow_smem(k_casc_fwd<N, T>, CF::SMEM);
   const int smr = CF::SMEM + CF::THREADS * (int)sizeof(double);
-  if (e == cudaSuccess) e = allow_smem(k_casc_resid<N, 1>, smr);
+  cudaError_t e = allow_smem(k_casc_resid<N, 1>, smr);
   for (int th0 = 0; th0 < ntheta && e == cudaSuccess; th0 += per_chunk) {
     const int nt = std::min(per_chunk, ntheta - th0);
     const CascDims D{N, nz, nobj, nzobj, ndist, (long)nt * ndist};
     const long nrows = D.nimg * nz;
-    k_casc_fwd<N, T><<<HT_ROWS_GRID(N, nrows), CF::THREADS, CF::SMEM, st>>>(
-        c + (long)th0 * nzobj * nobj, pos + (long)th0 * ndist * 2, mag + (long)th0 * ndist, prb, tmp, D, twn);
-    count_launch();
-    if ((e = cudaGetLastError()) != cudaSuccess) break;
+    e = launch_fwd<N, T>(D, c + (long)th0 * nzobj * nobj, pos + (long)th0 * ndist * 2, mag + (long)th0 * ndist, prb,
+                         tmp, twn, st);
+    if (e != cudaSuccess) break;
     if ((e = dct_cols(nz, false, tmp, D.nimg, N, hw, ndist, twz, st)) != cudaSuccess) break;
     k_casc_resid<N, 1><<<HT_ROWS_GRID(N, nrows), CF::THREADS, smr, st>>>(
         tmp, nullptr, data + (long)th0 * ndist * nz * N, nullptr, acc, 0.f, D, twn);

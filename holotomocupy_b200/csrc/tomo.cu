@@ -172,18 +172,29 @@ k_tcol_fwd(const float2* __restrict__ fa, float2* __restrict__ fde, const float2
 
 // ------------------------------------- 3: gather + detector IFFT (R)
 // fde [zb][2n][2n][Z] -> sino [ntheta, nz, n];  grid (ntheta, nzb)
-template <int N>
-__global__ void __launch_bounds__(ZCfg<N, TZ<2 * N>::Z>::THREADS)
+// Z/2 consecutive lanes share one polar sample, each lane reading one float4
+// (two slices) of every tap's Z-vector, so the lanes of a warp read whole
+// 64-byte cell vectors instead of 16 bytes from 32 different cells.
+// Register cap of the gather: 64 at 512 threads (two blocks per SM), else 96.
+template <int THREADS>
+constexpr int gather_max_regs() {
+  return THREADS >= 512 ? 64 : 96;
+}
+
+template <int N, int THREADS = ZCfg<N, TZ<2 * N>::Z>::THREADS>
+__global__ void __maxnreg__(gather_max_regs<THREADS>())
 k_tgather(const float2* __restrict__ fde, float2* __restrict__ sino, GatherGeom G, int nz,
           const float2* __restrict__ tw4) {
   constexpr int Z = TZ<2 * N>::Z;
+  constexpr int Q = Z / 2;                       // lanes per sample
   constexpr int T = ZCfg<N, Z>::T;
   constexpr int twon = 2 * N;
   extern __shared__ float2 smem[];
   const int th = blockIdx.x, zb = blockIdx.y;
   const float2 cs = G.cs[th];
-  const float2* f = fde + (long)zb * twon * twon * Z;
-  for (int tx = threadIdx.x; tx < N; tx += blockDim.x) {
+  const int q = threadIdx.x % Q;
+  const float4* f = reinterpret_cast<const float4*>(fde + (long)zb * twon * twon * Z) + q;
+  for (int tx = threadIdx.x / Q; tx < N; tx += blockDim.x / Q) {
     Window w;
     window_base(G, tx, cs, w);
     float ex[9];
@@ -193,29 +204,30 @@ k_tgather(const float2* __restrict__ fde, float2* __restrict__ sino, GatherGeom 
       ex[i] = wx_tap(G, w, i);
       cols[i] = (N + w.bx + i + twon) % twon;
     }
-    float2 acc[Z];
-#pragma unroll
-    for (int l = 0; l < Z; ++l) acc[l] = make_float2(0.f, 0.f);
+    float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
     for (int i1 = 0; i1 < 9; ++i1) {
       const int row = (N + w.by + i1 + twon) % twon;
       const float ey = wy_tap(G, w, i1);
-      const float2* frow = f + (long)row * twon * Z;
-      float2 ra[Z];
+      const float4* frow = f + (long)row * twon * Q;
+      float4 ra = make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
-      for (int l = 0; l < Z; ++l) ra[l] = make_float2(0.f, 0.f);
-#pragma unroll
-      for (int i0 = 0; i0 < 9; ++i0) zload_fma<Z>(ra, ex[i0], frow + (long)cols[i0] * Z);
-#pragma unroll
-      for (int l = 0; l < Z; ++l) {
-        acc[l].x += ey * ra[l].x;
-        acc[l].y += ey * ra[l].y;
+      for (int i0 = 0; i0 < 9; ++i0) {
+        const float4 v = __ldg(&frow[(long)cols[i0] * Q]);
+        ra.x += ex[i0] * v.x;
+        ra.y += ex[i0] * v.y;
+        ra.z += ex[i0] * v.z;
+        ra.w += ex[i0] * v.w;
       }
+      acc.x += ey * ra.x;
+      acc.y += ey * ra.y;
+      acc.z += ey * ra.z;
+      acc.w += ey * ra.w;
     }
     // /n of the gather, (-1)^tx before the IFFT
     const float s = ((tx & 1) ? -1.f : 1.f) / (float)N;
-#pragma unroll
-    for (int l = 0; l < Z; ++l) zline<N, Z>(smem, l).st(tx, cscale(acc[l], s));
+    zline<N, Z>(smem, 2 * q).st(tx, make_float2(s * acc.x, s * acc.y));
+    zline<N, Z>(smem, 2 * q + 1).st(tx, make_float2(s * acc.z, s * acc.w));
   }
   __syncthreads();
   const int l = threadIdx.x / T, t = threadIdx.x % T;
@@ -286,11 +298,15 @@ __device__ __forceinline__ void cell_angle(const GatherGeom& G, int j, float px,
   for (int tx = t0; tx <= t1; ++tx) {
     Window w;
     window_base(G, tx, cs, w);
-    int i0 = (X - n - w.bx) % twon;
-    if (i0 < 0) i0 += twon;
+    // (X - n - bx) mod 2n: bx lies in [-n - m, n - m] and X - n in [-n, n), so
+    // one correction either way reduces it
+    int i0 = X - n - w.bx;
+    i0 += (i0 < 0) ? twon : 0;
+    i0 -= (i0 >= twon) ? twon : 0;
     if (i0 > 8) continue;
-    int i1 = (Y - n - w.by) % twon;
-    if (i1 < 0) i1 += twon;
+    int i1 = Y - n - w.by;
+    i1 += (i1 < 0) ? twon : 0;
+    i1 -= (i1 >= twon) ? twon : 0;
     if (i1 > 8) continue;
     const float wt = wx_tap(G, w, i0) * wy_tap(G, w, i1);
     zload_fma<Z>(acc, wt, g + ((long)j * n + tx) * Z);
