@@ -90,12 +90,19 @@ struct SmRow {
   __device__ __forceinline__ void st(int k, float2 v) const { p[k + (k >> 4)] = v; }
 };
 
-// Column line inside a [N][C] tile (row-major, C columns side by side).
+// Column line inside a [N][C] tile (row-major, C columns side by side).  For
+// C = 4 (32-byte rows) row k is stored at k ^ ((k >> 3) & 3): the rows 8
+// apart that the first radix-8 stage writes together then fall on different
+// banks, and consecutive rows stay on different banks.
+template <int C>
+__host__ __device__ __forceinline__ int col_row(int k) {
+  return (C == 4) ? (k ^ ((k >> 3) & 3)) : k;
+}
 template <int C>
 struct SmCol {
   float2* p;  // points at column c of row 0
-  __device__ __forceinline__ float2 ld(int k) const { return p[k * C]; }
-  __device__ __forceinline__ void st(int k, float2 v) const { p[k * C] = v; }
+  __device__ __forceinline__ float2 ld(int k) const { return p[col_row<C>(k) * C]; }
+  __device__ __forceinline__ void st(int k, float2 v) const { p[col_row<C>(k) * C] = v; }
 };
 
 // --------------------------------------------------------------- the plan

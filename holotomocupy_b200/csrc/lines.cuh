@@ -14,7 +14,8 @@ struct RowCfg {
   static constexpr int SMEM = LINES * SmRow::padded(N) * (int)sizeof(float2);
 };
 
-// Columns per CTA for a column pass of length N (tile N x C in shared memory).
+// Columns per CTA for a column pass of length N (tile N x C in shared memory;
+// at N >= 2048 the 4-column tile's rows are swizzled, see SmCol).
 template <int N>
 struct ColCfg {
   static constexpr int T = Plan<N>::T;

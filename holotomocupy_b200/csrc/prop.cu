@@ -102,7 +102,7 @@ k_dct_cols(float2* data, int n, const float2* __restrict__ Hall, int ntab, const
   for (int idx = threadIdx.x; idx < NZ * C; idx += blockDim.x) {
     const int r = idx / C, cc = idx % C;
     const int col = col0 + cc;
-    tile[dct_perm_inv(r, NZ) * C + cc] = (col < n) ? img[(long)r * n + col] : make_float2(0.f, 0.f);
+    tile[col_row<C>(dct_perm_inv(r, NZ)) * C + cc] = (col < n) ? img[(long)r * n + col] : make_float2(0.f, 0.f);
   }
   __syncthreads();
   SmCol<C> sm{tile + c};
@@ -132,7 +132,7 @@ k_dct_cols(float2* data, int n, const float2* __restrict__ Hall, int ntab, const
   for (int idx = threadIdx.x; idx < NZ * C; idx += blockDim.x) {
     const int r = idx / C, cc = idx % C;
     const int cl = col0 + cc;
-    if (cl < n) img[(long)r * n + cl] = tile[dct_perm(r, NZ) * C + cc];
+    if (cl < n) img[(long)r * n + cl] = tile[col_row<C>(dct_perm(r, NZ)) * C + cc];
   }
 }
 

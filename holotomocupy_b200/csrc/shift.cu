@@ -310,7 +310,7 @@ k_symbol_cols(float2* data, int ncols, const float* __restrict__ sym, const floa
   float2* img = data + (long)blockIdx.y * N * ncols;
   for (int idx = threadIdx.x; idx < N * C; idx += blockDim.x) {
     const int rr = idx / C, cc = idx % C;
-    tile[idx] = (col0 + cc < ncols) ? img[(long)rr * ncols + col0 + cc] : make_float2(0.f, 0.f);
+    tile[col_row<C>(rr) * C + cc] = (col0 + cc < ncols) ? img[(long)rr * ncols + col0 + cc] : make_float2(0.f, 0.f);
   }
   __syncthreads();
   SmCol<C> sm{tile + c};
@@ -320,7 +320,7 @@ k_symbol_cols(float2* data, int ncols, const float* __restrict__ sym, const floa
   fft_line<N, true>(sm, t, tw4);
   for (int idx = threadIdx.x; idx < N * C; idx += blockDim.x) {
     const int rr = idx / C, cc = idx % C;
-    if (col0 + cc < ncols) img[(long)rr * ncols + col0 + cc] = tile[idx];
+    if (col0 + cc < ncols) img[(long)rr * ncols + col0 + cc] = tile[col_row<C>(rr) * C + cc];
   }
 }
 
