@@ -51,7 +51,11 @@ def deapodisation(n, ntheta, mask):
 class Tomo:
     """Functionality for Radon transforms (tomo.py:9)."""
 
-    def __init__(self, n, nz, theta, mask_r, device=None):
+    def __init__(self, n, nz, theta, mask_r, device=None, norm_ntheta=None):
+        """``norm_ntheta`` (default: the number of angles) is the angle count
+        in the 1/(n sqrt(n ntheta)) scaling of R; a Tomo over a chunk of a
+        larger angle set passes the full count so that its R is a slice of
+        the full R."""
         self.n = n
         self._nz = nz
         theta = np.asarray(theta.cpu() if isinstance(theta, torch.Tensor) else theta).astype("float32")
@@ -60,7 +64,7 @@ class Tomo:
         self.theta = torch.from_numpy(theta).to(self.device)
         mask = support_mask(n, mask_r)
         self.mask = 1.0 if mask is None else torch.from_numpy(mask).to(self.device)
-        phi = deapodisation(n, self.ntheta, mask)
+        phi = deapodisation(n, self.ntheta if norm_ntheta is None else norm_ntheta, mask)
         _, mu, m = usfft_params(n)
         self._phi = phi
         self.pars = (m, torch.tensor([mu], dtype=torch.float32, device=self.device),
