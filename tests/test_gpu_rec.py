@@ -212,3 +212,30 @@ def test_cascade_at_large_magnifications_matches_oracle():
     orc.gradients_cascade(o(v), ref)
     for k in ("prb", "proj", "pos"):
         assert rel_l2(out[k].cpu().numpy(), ref[k]) < 1e-4, k
+
+
+@pytest.mark.parametrize("mode", ["host", "graph"])
+def test_bh_32_iterations_against_fp64_oracle(golden, mode):
+    """32 BH iterations (FP32 bulk, FP64 reductions and step sizes) stay
+    within rel L2 1e-4 of the FP64 oracle's BH on the golden problem
+    (measured: obj 1.6e-5, prb 9e-8, pos 1.5e-7); the graph-replayed,
+    device-scalar form gives the same state as the host-scalar one."""
+    from oracle import holo_oracle as O
+    from holotomocupy_b200.rec import Rec
+    g = golden("rec")
+    n, ntheta, ndist, nobj, _ = [int(v) for v in g["bh_dims"]]
+    args = rec_args(n, ntheta, ndist, nobj, 32)
+    rec = Rec(args)
+    orc = O.Rec(args, "complex128")
+    for r, put in ((rec, cuda), (orc, lambda a: a)):
+        r.vars["obj"][:] = put(g["bh_obj_true"])
+        r.vars["prb"][:] = put(g["bh_prb_true"])
+        r.vars["pos"][:] = put(g["bh_pos_true"])
+        r.gen_sqrt_data(r.vars, r.data)
+        r.vars["obj"][:] = 0
+        r.vars["prb"][:] = 1
+        r.vars["pos"][:] = put(g["bh_pos_true"] + g["bh_pos_err"])
+    rec.BH(mode=mode)
+    orc.BH()
+    for k in ("obj", "prb", "pos"):
+        assert rel_l2(rec.vars[k].cpu().numpy(), orc.vars[k]) < 1e-4, k
