@@ -15,12 +15,13 @@
 //      samples are 81-tap Gaussian-weighted sums of fde (m = 4 at every
 //      supported size), then sign, IFFT_n, sign, /4.
 // RT runs the exact adjoint: detector FFT with signs -> gs [zb][theta][n][Z];
-// a per-cell gather replaces the reference's atomic scatter: every spectral
-// cell visits only the angles whose line passes within 7.5 cells of it
-// (binary search in the sorted angles) and the few radial samples near it,
-// and re-checks window membership with the forward's own formulas, so R^T is
-// the exact transpose of R and deterministic; then column IFFT keeping the
-// central rows, row IFFT, crop, * phi.
+// a gather replaces the reference's atomic scatter: every
+// warp owns an 8 x 4 tile of cells and visits, uniformly across its lanes,
+// only the angles whose line passes near the tile (binary search in the
+// sorted angles) and the samples whose window can meet it; membership and
+// weights come from the forward's own formulas, so R^T is the exact
+// transpose of R and deterministic; then column IFFT keeping the central
+// rows, row IFFT, crop, * phi.
 //
 // Angle cosines and sines come from a table computed in double precision on
 // the host (the reference's __cosf/__sinf error of ~5e-7 moves R by up to
@@ -271,8 +272,18 @@ k_tsino_fft(const float2* __restrict__ sino, float2* __restrict__ gs, int ntheta
   }
 }
 
-// -------------------------------------------- RT 2: per-cell gather
-// gs [zb][ntheta][n][Z] -> fde [zb][2n][2n][Z];  grid (2n/16, 2n/16, nzb), block 16x16
+// -------------------------------------------- RT 2: sparse cell gather
+// The pairs (sample, spectral cell) of R's gridding and their weights depend
+// only on the angles, so ht_tomo_create lists them once per cell -- found by
+// a per-cell search (the angles whose line passes within 7.5 cells, by binary
+// search in the sorted angles; the radial samples near the cell; window
+// membership and weights from the forward's own formulas) -- in a sliced
+// ELLPACK layout: a small tile of CPS = 64/Z cells forms a slice, entry p of
+// the slice is CPS consecutive (sample, weight) pairs, shorter lists padded
+// with weight 0.  R^T runs one slice per warp with Z/2 lanes per cell, each
+// lane reading one float4 (two slices) of the sample's Z-vector, so a warp
+// load covers CPS whole 64-byte vectors; neighbouring cells share samples,
+// which L1 serves.  The exact transpose of R, deterministic, no atomics.
 constexpr float kLineReach = 7.5f;  // window cells lie within 5 sqrt(2) of the sample centre
 
 __device__ __forceinline__ int lower_bound_f(const float* a, int n, float v) {
@@ -287,9 +298,9 @@ __device__ __forceinline__ int lower_bound_f(const float* a, int n, float v) {
   return lo;
 }
 
-template <int Z>
-__device__ __forceinline__ void cell_angle(const GatherGeom& G, int j, float px, float py, int X, int Y,
-                                           const float2* __restrict__ g, float2 (&acc)[Z]) {
+// Visit (sample index j*n + t, weight) for every sample of angle j whose window holds cell (X, Y).
+template <class F>
+__device__ __forceinline__ void cell_angle_pairs(const GatherGeom& G, int j, float px, float py, int X, int Y, F& f) {
   const int n = G.n, twon = 2 * n;
   const float2 cs = G.cs[j];
   const float s = px * cs.x - py * cs.y;  // projection onto (cos, -sin)
@@ -308,23 +319,14 @@ __device__ __forceinline__ void cell_angle(const GatherGeom& G, int j, float px,
     i1 += (i1 < 0) ? twon : 0;
     i1 -= (i1 >= twon) ? twon : 0;
     if (i1 > 8) continue;
-    const float wt = wx_tap(G, w, i0) * wy_tap(G, w, i1);
-    zload_fma<Z>(acc, wt, g + ((long)j * n + tx) * Z);
+    f(j * n + tx, wx_tap(G, w, i0) * wy_tap(G, w, i1));
   }
 }
 
-template <int Z>
-__global__ void __launch_bounds__(256)
-k_tcell(const float2* __restrict__ gs, float2* __restrict__ fde, GatherGeom G) {
+// All pairs of cell (X, Y), in a fixed order.
+template <class F>
+__device__ void cell_pairs(const GatherGeom& G, int X, int Y, F& f) {
   const int n = G.n, twon = 2 * n;
-  const int X = blockIdx.x * 16 + threadIdx.x;
-  const int Y = blockIdx.y * 16 + threadIdx.y;
-  const int zb = blockIdx.z;
-  if (X >= twon || Y >= twon) return;
-  const float2* g = gs + (long)zb * G.ntheta * n * Z;
-  float2 acc[Z];
-#pragma unroll
-  for (int l = 0; l < Z; ++l) acc[l] = make_float2(0.f, 0.f);
   const float PI = 3.14159265358979f;
   const float lim = (float)n + 9.0f;
   for (int oy = -1; oy <= 1; ++oy) {
@@ -334,7 +336,7 @@ k_tcell(const float2* __restrict__ gs, float2* __restrict__ fde, GatherGeom G) {
       if (fabsf(px) > lim || fabsf(py) > lim) continue;
       const float R = sqrtf(px * px + py * py);
       if (R <= kLineReach) {
-        for (int j = 0; j < G.ntheta; ++j) cell_angle<Z>(G, j, px, py, X, Y, g, acc);
+        for (int j = 0; j < G.ntheta; ++j) cell_angle_pairs(G, j, px, py, X, Y, f);
         continue;
       }
       // angles with R |sin(theta + phi)| <= reach, theta taken mod pi
@@ -360,13 +362,121 @@ k_tcell(const float2* __restrict__ gs, float2* __restrict__ fde, GatherGeom G) {
       }
       for (int q = 0; q < ni; ++q)
         for (int i = lower_bound_f(G.th_sorted, G.ntheta, ia[q]); i < G.ntheta && G.th_sorted[i] <= ib[q]; ++i)
-          cell_angle<Z>(G, G.th_index[i], px, py, X, Y, g, acc);
+          cell_angle_pairs(G, G.th_index[i], px, py, X, Y, f);
     }
   }
-  float4* dst = reinterpret_cast<float4*>(fde + (((long)zb * twon + Y) * twon + X) * Z);
+}
+
+struct PairCount {
+  int n = 0;
+  __device__ void operator()(int, float) { ++n; }
+};
+
+// Slices: tiles of TW x TH = CPS cells (CPS = 64 / Z: 8, 16 or 32 cells).
+struct SliceShape {
+  int tw, th;
+};
+__host__ __device__ __forceinline__ SliceShape slice_shape(int cps) {
+  return cps == 8 ? SliceShape{4, 2} : (cps == 16 ? SliceShape{4, 4} : SliceShape{8, 4});
+}
+// slice s, cell k of the slice <-> cell (X, Y) (false: outside the grid)
+__device__ __forceinline__ bool slice_cell(long s, int k, int twon, SliceShape sh, int& X, int& Y) {
+  const long tiles_x = (twon + sh.tw - 1) / sh.tw;
+  X = (int)(s % tiles_x) * sh.tw + k % sh.tw;
+  Y = (int)(s / tiles_x) * sh.th + k / sh.tw;
+  return X < twon && Y < twon;
+}
+__device__ __forceinline__ void cell_slice(int X, int Y, int twon, SliceShape sh, long& s, int& k) {
+  s = (long)(Y / sh.th) * ((twon + sh.tw - 1) / sh.tw) + X / sh.tw;
+  k = (Y % sh.th) * sh.tw + X % sh.tw;
+}
+
+// pairs per cell;  cells c = Y * 2n + X
+__global__ void k_cell_count(GatherGeom G, int* __restrict__ cnt) {
+  const int twon = 2 * G.n;
+  const long c = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= (long)twon * twon) return;
+  PairCount f;
+  cell_pairs(G, (int)(c % twon), (int)(c / twon), f);
+  cnt[c] = f.n;
+}
+
+// slice length = the longest list of its cells
+__global__ void k_slice_len(const int* __restrict__ cnt, int twon, int cps, int* __restrict__ len, long nslices) {
+  const long s = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nslices) return;
+  const SliceShape sh = slice_shape(cps);
+  int mx = 0;
+  for (int k = 0; k < cps; ++k) {
+    int X, Y;
+    if (slice_cell(s, k, twon, sh, X, Y)) mx = max(mx, cnt[(long)Y * twon + X]);
+  }
+  len[s] = mx;
+}
+
+struct PairFillS {
+  int2* dst;  // this cell's first entry; entries cps apart
+  int cps;
+  int p = 0;
+  __device__ void operator()(int idx, float w) {
+    dst[(long)p * cps] = make_int2(idx, __float_as_int(w));
+    ++p;
+  }
+};
+
+__global__ void k_cell_fill(GatherGeom G, int cps, const long* __restrict__ off, int2* __restrict__ ent) {
+  const int twon = 2 * G.n;
+  const long c = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= (long)twon * twon) return;
+  const int X = (int)(c % twon), Y = (int)(c / twon);
+  long sl;
+  int k;
+  cell_slice(X, Y, twon, slice_shape(cps), sl, k);
+  PairFillS f{ent + off[sl] * cps + k, cps};
+  cell_pairs(G, X, Y, f);
+}
+
+// gs [zb][ntheta][n][Z] -> fde [zb][2n][2n][Z]; grid (ceil(slices * 32 / 256), ceil(nzb / ZG));
+// ZG slice batches per lane
+template <int Z, int ZG>
+__global__ void __launch_bounds__(256)
+k_tcell(const float2* __restrict__ gs, float2* __restrict__ fde, const int* __restrict__ len,
+        const long* __restrict__ off, const int2* __restrict__ ent, int twon, long nslices, long nsamp, int nzb) {
+  constexpr int Q = Z / 2;       // lanes per cell
+  constexpr int CPS = 32 / Q;    // cells per slice (warp)
+  const long tid = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long sl = tid / 32;
+  if (sl >= nslices) return;
+  const int lane = (int)(tid % 32), k = lane / Q, q = lane % Q;
+  int X, Y;
+  const bool live = slice_cell(sl, k, twon, slice_shape(CPS), X, Y);
+  const int zb0 = blockIdx.y * ZG;
+  const int nl = len[sl];
+  const int2* e = ent + off[sl] * CPS + k;
+  float4 acc[ZG];
 #pragma unroll
-  for (int i = 0; i < Z / 2; ++i)
-    dst[i] = make_float4(acc[2 * i].x, acc[2 * i].y, acc[2 * i + 1].x, acc[2 * i + 1].y);
+  for (int g = 0; g < ZG; ++g) acc[g] = make_float4(0.f, 0.f, 0.f, 0.f);
+  const float4* gb = reinterpret_cast<const float4*>(gs + (long)zb0 * nsamp * Z) + q;
+  for (int p = 0; p < nl; ++p) {
+    const int2 v = __ldg(&e[(long)p * CPS]);
+    const float w = __int_as_float(v.y);
+#pragma unroll
+    for (int g = 0; g < ZG; ++g)
+      if (zb0 + g < nzb) {
+        const float4 u = __ldg(&gb[((long)g * nsamp + v.x) * Q]);
+        acc[g].x += w * u.x;
+        acc[g].y += w * u.y;
+        acc[g].z += w * u.z;
+        acc[g].w += w * u.w;
+      }
+  }
+  if (!live) return;
+  const long c = (long)Y * twon + X, ncells = (long)twon * twon;
+#pragma unroll
+  for (int g = 0; g < ZG; ++g) {
+    if (zb0 + g >= nzb) break;
+    reinterpret_cast<float4*>(fde + ((long)(zb0 + g) * ncells + c) * Z)[q] = acc[g];
+  }
 }
 
 // ------------------------------------------- RT 3: column IFFT
@@ -454,10 +564,16 @@ static cudaError_t tomo_R_sized(const float2* obj, float2* sino, const float* ph
   return cudaGetLastError();
 }
 
+struct CellLists {
+  const int* len;   // [nslices]
+  const long* off;  // [nslices] first entry of each slice (in entries of 32)
+  const int2* ent;  // entries
+};
+
 template <int N2>
 static cudaError_t tomo_RT_sized(const float2* sino, float2* obj, const float* phi, float2* fab, float2* fde,
-                                 float2* gs, const GatherGeom& G, int nz, const float2* tw_n, const float2* tw_2n,
-                                 cudaStream_t st) {
+                                 float2* gs, const GatherGeom& G, const CellLists& L, int nz, const float2* tw_n,
+                                 const float2* tw_2n, cudaStream_t st) {
   constexpr int n = N2 / 2;
   constexpr int Z = TZ<N2>::Z;
   using C2 = ZCfg<N2, Z>;
@@ -471,7 +587,11 @@ static cudaError_t tomo_RT_sized(const float2* sino, float2* obj, const float* p
   count_launch();
   {
     KTimer kt("k_tcell", st, (double)nz);
-    k_tcell<Z><<<dim3((N2 + 15) / 16, (N2 + 15) / 16, nzb), dim3(16, 16), 0, st>>>(gs, fde, G);
+    constexpr int ZG = 2;
+    const SliceShape sh = slice_shape(64 / Z);
+    const long nsl = (long)((N2 + sh.tw - 1) / sh.tw) * ((N2 + sh.th - 1) / sh.th);
+    k_tcell<Z, ZG><<<dim3((unsigned)((nsl * 32 + 255) / 256), (unsigned)((nzb + ZG - 1) / ZG)), 256, 0, st>>>(
+        gs, fde, L.len, L.off, L.ent, N2, nsl, (long)G.ntheta * n, nzb);
   }
   count_launch();
   k_tcol_adj<N2><<<dim3(N2, nzb), C2::THREADS, C2::SMEM, st>>>(fde, fab, tw_2n);
@@ -504,7 +624,14 @@ struct ht_tomo_s {
   float2* gs;          // workspace [nzb][ntheta][n][Z]
   const float2* tw_n;
   const float2* tw_2n;
+  int* cl_len;         // R^T pair lists: [slices] entries per slice of 64/Z cells
+  long* cl_off;        // [slices] first entry of each slice
+  int2* cl_ent;        // [entries][64/Z] (sample index, weight bits)
 };
+
+namespace ht {
+static cudaError_t build_cell_lists(ht_tomo_s* t);
+}
 
 static bool tomo_size_ok(int n) {
   switch (n) {
@@ -525,6 +652,9 @@ static void tomo_free(ht_tomo_s* t) {
   cudaFree(t->fde);
   cudaFree(t->fab);
   cudaFree(t->gs);
+  cudaFree(t->cl_len);
+  cudaFree(t->cl_off);
+  cudaFree(t->cl_ent);
 }
 
 extern "C" int ht_tomo_create(int n, int nz, int ntheta, const float* theta_host, const float* phi_host,
@@ -585,6 +715,7 @@ extern "C" int ht_tomo_create(int n, int nz, int ntheta, const float* theta_host
   if (e == cudaSuccess) e = cudaMemcpy(t->cs, cs.data(), sizeof(float2) * ntheta, cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemcpy(t->th_sorted, ths.data(), sizeof(float) * ntheta, cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemcpy(t->th_index, idx.data(), sizeof(int) * ntheta, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = build_cell_lists(t);
   if (e != cudaSuccess || !t->tw_n || !t->tw_2n) {
     if (e != cudaSuccess) set_error(std::string("ht_tomo_create: ") + cudaGetErrorString(e));
     tomo_free(t);
@@ -615,6 +746,50 @@ static GatherGeom geom(const ht_tomo_s* t) {
   G.th_sorted = t->th_sorted;
   G.th_index = t->th_index;
   return G;
+}
+
+// The R^T pair lists (k_cell_count, k_slice_len, k_cell_fill) on a private
+// stream; the per-cell counts use the Fourier-grid workspace as scratch.
+static cudaError_t build_cell_lists(ht_tomo_s* t) {
+  const GatherGeom G = geom(t);
+  const int twon = 2 * t->n;
+  const int cps = 64 / tomo_Z(t->n);
+  const SliceShape sh = slice_shape(cps);
+  const long ncells = (long)twon * twon, nsl = (long)((twon + sh.tw - 1) / sh.tw) * ((twon + sh.th - 1) / sh.th);
+  int* cnt = reinterpret_cast<int*>(t->fde);
+  cudaStream_t st = nullptr;
+  cudaError_t e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+  if (e != cudaSuccess) return e;
+  std::vector<int> len(nsl);
+  std::vector<long> off(nsl);
+  long tot = 0;
+  e = cudaMalloc(&t->cl_len, sizeof(int) * nsl);
+  if (e == cudaSuccess) e = cudaMalloc(&t->cl_off, sizeof(long) * nsl);
+  if (e == cudaSuccess) {
+    k_cell_count<<<(unsigned)((ncells + 255) / 256), 256, 0, st>>>(G, cnt);
+    count_launch();
+    k_slice_len<<<(unsigned)((nsl + 255) / 256), 256, 0, st>>>(cnt, twon, cps, t->cl_len, nsl);
+    count_launch();
+    e = cudaMemcpyAsync(len.data(), t->cl_len, sizeof(int) * nsl, cudaMemcpyDeviceToHost, st);
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e == cudaSuccess) {
+    for (long i = 0; i < nsl; ++i) {
+      off[i] = tot;
+      tot += len[i];
+    }
+    e = cudaMemcpyAsync(t->cl_off, off.data(), sizeof(long) * nsl, cudaMemcpyHostToDevice, st);
+  }
+  if (e == cudaSuccess) e = cudaMalloc(&t->cl_ent, sizeof(int2) * cps * (size_t)std::max(tot, 1L));
+  if (e == cudaSuccess) e = cudaMemsetAsync(t->cl_ent, 0, sizeof(int2) * cps * (size_t)std::max(tot, 1L), st);
+  if (e == cudaSuccess) {
+    k_cell_fill<<<(unsigned)((ncells + 255) / 256), 256, 0, st>>>(G, cps, t->cl_off, t->cl_ent);
+    count_launch();
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  cudaStreamDestroy(st);
+  return e;
 }
 }  // namespace ht
 
@@ -653,7 +828,7 @@ extern "C" int ht_tomo_RT(ht_tomo_s* t, const void* sino, void* obj, int nz, voi
 #define X(A, B)                                                                                                 \
   case A:                                                                                                       \
     e = tomo_RT_sized<B>(static_cast<const float2*>(sino), static_cast<float2*>(obj), t->phi, t->fab, t->fde,    \
-                         t->gs, G, nz, t->tw_n, t->tw_2n, st);                                                  \
+                         t->gs, G, CellLists{t->cl_len, t->cl_off, t->cl_ent}, nz, t->tw_n, t->tw_2n, st);        \
     break;
     HT_TOMO_SIZES(X)
 #undef X
