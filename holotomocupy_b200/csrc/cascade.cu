@@ -481,32 +481,52 @@ __global__ void k_sum_theta(const float2* __restrict__ Pc, float2* __restrict__ 
 
 // ================================================= object gradient
 // gc[theta, iy, ix] = sum_k sum_ty py(ty -> iy) hbuf[theta, k, ty, ix]
-// (the vertical half of sum_k S_k^T Y22, gF3, rec_mpi.py:802-808).
+// (the vertical half of sum_k S_k^T Y22, gF3, rec_mpi.py:802-808).  Each
+// thread produces kVRows consecutive rows iy of one column ix, reading each
+// detector row that reaches them once (coalesced along ix); every output sums
+// its contributions in (k, ty) order.
+constexpr int kVRows = 8;
+
 template <class T>
 __global__ void __launch_bounds__(256)
 k_casc_vsum(T* __restrict__ gc, const T* __restrict__ hbuf, const float* __restrict__ pos,
             const float* __restrict__ mag, CascDims D) {
   const int ix = blockIdx.x * blockDim.x + threadIdx.x;
-  const int iy = blockIdx.y * blockDim.y + threadIdx.y;
+  const int iy0 = (blockIdx.y * blockDim.y + threadIdx.y) * kVRows;
   const long th = blockIdx.z;
-  if (ix >= D.nobj || iy >= D.nzobj) return;
-  T acc = El<T>::zero();
+  if (ix >= D.nobj || iy0 >= D.nzobj) return;
+  T acc[kVRows];
+#pragma unroll
+  for (int r = 0; r < kVRows; ++r) acc[r] = El<T>::zero();
   for (int k = 0; k < D.ndist; ++k) {
     const long img = th * D.ndist + k;
     const float m0 = mag[img];
     const float ry = pos[2 * img + 0];
-    int ty0, ty1;
-    cand_range(m0, -ry + (m0 - 1.0f) / 2.0f + (float)(D.nzobj / 2), iy, D.nz / 2, D.nz, ty0, ty1);
+    const float C0 = -ry + (m0 - 1.0f) / 2.0f + (float)(D.nzobj / 2);
+    int a0, a1, b0, b1;
+    cand_range(m0, C0, iy0, D.nz / 2, D.nz, a0, a1);
+    cand_range(m0, C0, min(iy0 + kVRows - 1, D.nzobj - 1), D.nz / 2, D.nz, b0, b1);
+    const int ty0 = min(a0, b0), ty1 = max(a1, b1);
     const T* hb = hbuf + img * (long)D.nz * D.nobj + ix;
     for (int ty = ty0; ty <= ty1; ++ty) {
       const float y = sample_y(D, m0, ry, ty);
       const int iyw = (int)floorf(y);
-      const int j = iy - iyw + 1;
-      if (j < 0 || j > 3) continue;
-      El<T>::fma(acc, bw0_tap(y - (float)iyw, j), __ldg(&hb[(long)ty * D.nobj]));
+      const int jr = iy0 - iyw + 1;          // tap index of row iy0
+      if (jr > 3 || jr + kVRows - 1 < 0) continue;
+      float w[4];
+      bw0(y - (float)iyw, w);
+      const T h = __ldg(&hb[(long)ty * D.nobj]);
+#pragma unroll
+      for (int r = 0; r < kVRows; ++r) {
+        const int j = jr + r;
+        const float wt = (j == 0) ? w[0] : (j == 1) ? w[1] : (j == 2) ? w[2] : (j == 3) ? w[3] : 0.f;
+        if (j >= 0 && j <= 3) El<T>::fma(acc[r], wt, h);
+      }
     }
   }
-  gc[(th * D.nzobj + iy) * D.nobj + ix] = acc;
+#pragma unroll
+  for (int r = 0; r < kVRows; ++r)
+    if (iy0 + r < D.nzobj) gc[(th * D.nzobj + iy0 + r) * D.nobj + ix] = acc[r];
 }
 
 // gpos[img] = (-Ay, -Ax)  (dsadj, cuda_kernels.py:744-761 with redot)
@@ -909,7 +929,7 @@ static cudaError_t grad_impl(ht_rec_s* r, const void* c, const float* pos, const
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   const long npix = (long)r->D.nz * N;
   k_sum_theta<<<(unsigned)((r->D.ndist * npix + 255) / 256), 256, 0, st>>>(r->P, gprb, r->ntheta, r->D.ndist, npix); ::ht::count_launch();
-  dim3 g2((r->D.nobj + 31) / 32, (r->D.nzobj + 7) / 8, r->ntheta);
+  dim3 g2((r->D.nobj + 31) / 32, (r->D.nzobj + 8 * kVRows - 1) / (8 * kVRows), r->ntheta);
   k_casc_vsum<T><<<g2, dim3(32, 8), 0, st>>>((T*)gc, hbuf, pos, mag, r->D); ::ht::count_launch();
   k_casc_gpos<<<(unsigned)((r->D.nimg + 255) / 256), 256, 0, st>>>(r->acc_img, gpos, r->D.nimg); ::ht::count_launch();
   return cudaGetLastError();
