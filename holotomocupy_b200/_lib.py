@@ -27,9 +27,12 @@ SIGNATURES = {
     "ht_tomo_destroy": [_vp],
     "ht_tomo_R": [_vp, _vp, _vp, _c_int, _vp],
     "ht_tomo_RT": [_vp, _vp, _vp, _c_int, _vp],
+    "ht_tomo_R_coeffx": [_vp, _vp, _vp, _c_int, _vp],
+    "ht_tomo_RT_coeffx": [_vp, _vp, _vp, _c_int, _vp],
     "ht_shift_create": [_c_int, _c_int, _c_int, _c_int, _c_int, ctypes.POINTER(_vp)],
     "ht_shift_destroy": [_vp],
     "ht_shift_coeff": [_vp, _vp, _vp, _c_long, _vp],
+    "ht_shift_coeff_z": [_vp, _vp, _c_long, _vp],
     "ht_shift_S": [_vp, _vp, _vp, _vp, _vp, _c_long, _vp],
     "ht_shift_Sadj": [_vp, _vp, _vp, _vp, _vp, _c_long, _vp],
     "ht_shift_dS": [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _c_long, _vp],

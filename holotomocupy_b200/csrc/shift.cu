@@ -445,6 +445,21 @@ extern "C" int ht_shift_coeff(ht_shift_s* s, const void* psi, void* out, long ba
   return kOk;
 }
 
+extern "C" int ht_shift_coeff_z(ht_shift_s* s, void* data, long ncols, void* stream) {
+  using namespace ht;
+  HT_REQUIRE(s && data, "ht_shift_coeff_z: null pointer");
+  HT_REQUIRE(ncols >= 0, "ht_shift_coeff_z: ncols must be non-negative");
+  if (!fft_size_supported(s->nzpsi)) {
+    set_error("ht_shift_coeff_z: nzpsi must be a supported FFT length");
+    return kUnsupported;
+  }
+  if (ncols == 0) return kOk;
+  HT_REQUIRE(ncols <= 0x7fffffffL, "ht_shift_coeff_z: ncols too large");
+  HT_CHECK_CUDA(symbol_cols(s->nzpsi, static_cast<float2*>(data), 1, (int)ncols, s->symy, s->tw_y,
+                            static_cast<cudaStream_t>(stream)));
+  return kOk;
+}
+
 template <int MODE>
 static int shift_stencil(ht_shift_s* s, void* out, const void* c, const void* c1, const void* c2, const float* r,
                          const float* mag, const float* d1, const float* d2, long batch, void* stream) {

@@ -185,7 +185,7 @@ constexpr int gather_max_regs() {
 template <int N, int THREADS = ZCfg<N, TZ<2 * N>::Z>::THREADS>
 __global__ void __maxnreg__(gather_max_regs<THREADS>())
 k_tgather(const float2* __restrict__ fde, float2* __restrict__ sino, GatherGeom G, int nz,
-          const float2* __restrict__ tw4) {
+          const float2* __restrict__ tw4, const float* __restrict__ symx) {
   constexpr int Z = TZ<2 * N>::Z;
   constexpr int Q = Z / 2;                       // lanes per sample
   constexpr int T = ZCfg<N, Z>::T;
@@ -225,8 +225,10 @@ k_tgather(const float2* __restrict__ fde, float2* __restrict__ sino, GatherGeom 
       acc.z += ey * ra.z;
       acc.w += ey * ra.w;
     }
-    // /n of the gather, (-1)^tx before the IFFT
-    const float s = ((tx & 1) ? -1.f : 1.f) / (float)N;
+    // /n of the gather, (-1)^tx before the IFFT; symx: the detector-axis
+    // filter, whose frequency kx sits at tx = kx - n/2 (mod n) here
+    float s = ((tx & 1) ? -1.f : 1.f) / (float)N;
+    if (symx) s *= __ldg(&symx[(tx + N / 2) % N]);
     zline<N, Z>(smem, 2 * q).st(tx, make_float2(s * acc.x, s * acc.y));
     zline<N, Z>(smem, 2 * q + 1).st(tx, make_float2(s * acc.z, s * acc.w));
   }
@@ -248,7 +250,7 @@ k_tgather(const float2* __restrict__ fde, float2* __restrict__ sino, GatherGeom 
 template <int N>
 __global__ void __launch_bounds__(ZCfg<N, TZ<2 * N>::Z>::THREADS)
 k_tsino_fft(const float2* __restrict__ sino, float2* __restrict__ gs, int ntheta, int nz,
-            const float2* __restrict__ tw4) {
+            const float2* __restrict__ tw4, const float* __restrict__ symx) {
   constexpr int Z = TZ<2 * N>::Z;
   constexpr int T = ZCfg<N, Z>::T;
   extern __shared__ float2 smem[];
@@ -267,8 +269,9 @@ k_tsino_fft(const float2* __restrict__ sino, float2* __restrict__ gs, int ntheta
   for (int idx = threadIdx.x; idx < N * Z; idx += blockDim.x) {
     const int tx = idx / Z, ll = idx % Z;
     float2 v = zline<N, Z>(smem, ll).ld(tx);
-    if (tx & 1) v = make_float2(-v.x, -v.y);
-    dst[idx] = v;
+    float sg = (tx & 1) ? -1.f : 1.f;
+    if (symx) sg *= __ldg(&symx[(tx + N / 2) % N]);  // detector-axis filter (see k_tgather)
+    dst[idx] = cscale(v, sg);
   }
 }
 
@@ -542,7 +545,7 @@ k_trow_adj(const float2* __restrict__ fb, const float* __restrict__ phi, float2*
 template <int N2>
 static cudaError_t tomo_R_sized(const float2* obj, float2* sino, const float* phi, float2* fa, float2* fde,
                                 const GatherGeom& G, int nz, const float2* tw_n, const float2* tw_2n,
-                                cudaStream_t st) {
+                                const float* symx, cudaStream_t st) {
   constexpr int n = N2 / 2;
   constexpr int Z = TZ<N2>::Z;
   using C2 = ZCfg<N2, Z>;
@@ -558,7 +561,7 @@ static cudaError_t tomo_R_sized(const float2* obj, float2* sino, const float* ph
   count_launch();
   {
     KTimer kt("k_tgather", st, (double)nz);
-    k_tgather<n><<<dim3(G.ntheta, nzb), C1::THREADS, C1::SMEM, st>>>(fde, sino, G, nz, tw_n);
+    k_tgather<n><<<dim3(G.ntheta, nzb), C1::THREADS, C1::SMEM, st>>>(fde, sino, G, nz, tw_n, symx);
   }
   count_launch();
   return cudaGetLastError();
@@ -573,7 +576,7 @@ struct CellLists {
 template <int N2>
 static cudaError_t tomo_RT_sized(const float2* sino, float2* obj, const float* phi, float2* fab, float2* fde,
                                  float2* gs, const GatherGeom& G, const CellLists& L, int nz, const float2* tw_n,
-                                 const float2* tw_2n, cudaStream_t st) {
+                                 const float2* tw_2n, const float* symx, cudaStream_t st) {
   constexpr int n = N2 / 2;
   constexpr int Z = TZ<N2>::Z;
   using C2 = ZCfg<N2, Z>;
@@ -583,7 +586,7 @@ static cudaError_t tomo_RT_sized(const float2* sino, float2* obj, const float* p
   if ((e = allow_smem(k_tsino_fft<n>, C1::SMEM)) != cudaSuccess) return e;
   if ((e = allow_smem(k_tcol_adj<N2>, C2::SMEM)) != cudaSuccess) return e;
   if ((e = allow_smem(k_trow_adj<N2>, C2::SMEM)) != cudaSuccess) return e;
-  k_tsino_fft<n><<<dim3(G.ntheta, nzb), C1::THREADS, C1::SMEM, st>>>(sino, gs, G.ntheta, nz, tw_n);
+  k_tsino_fft<n><<<dim3(G.ntheta, nzb), C1::THREADS, C1::SMEM, st>>>(sino, gs, G.ntheta, nz, tw_n, symx);
   count_launch();
   {
     KTimer kt("k_tcell", st, (double)nz);
@@ -627,6 +630,7 @@ struct ht_tomo_s {
   int* cl_len;         // R^T pair lists: [slices] entries per slice of 64/Z cells
   long* cl_off;        // [slices] first entry of each slice
   int2* cl_ent;        // [entries][64/Z] (sample index, weight bits)
+  float* symx;         // [n] 1 / (4 + 2 cos 2 pi k / n): the B-spline prefilter along the detector axis
 };
 
 namespace ht {
@@ -655,6 +659,7 @@ static void tomo_free(ht_tomo_s* t) {
   cudaFree(t->cl_len);
   cudaFree(t->cl_off);
   cudaFree(t->cl_ent);
+  cudaFree(t->symx);
 }
 
 extern "C" int ht_tomo_create(int n, int nz, int ntheta, const float* theta_host, const float* phi_host,
@@ -711,10 +716,14 @@ extern "C" int ht_tomo_create(int n, int nz, int ntheta, const float* theta_host
   alloc((void**)&t->fde, sizeof(float2) * nzp * 4 * n * n);
   alloc((void**)&t->fab, sizeof(float2) * nzp * 2 * n * n);
   alloc((void**)&t->gs, sizeof(float2) * nzp * ntheta * n);
+  alloc((void**)&t->symx, sizeof(float) * n);
+  std::vector<float> sx(n);
+  for (int k = 0; k < n; ++k) sx[k] = (float)(1.0 / (4.0 + 2.0 * std::cos(2.0 * M_PI * k / n)));
   if (e == cudaSuccess) e = cudaMemcpy(t->phi, phi_host, sizeof(float) * n * n, cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemcpy(t->cs, cs.data(), sizeof(float2) * ntheta, cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemcpy(t->th_sorted, ths.data(), sizeof(float) * ntheta, cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemcpy(t->th_index, idx.data(), sizeof(int) * ntheta, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(t->symx, sx.data(), sizeof(float) * n, cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = build_cell_lists(t);
   if (e != cudaSuccess || !t->tw_n || !t->tw_2n) {
     if (e != cudaSuccess) set_error(std::string("ht_tomo_create: ") + cudaGetErrorString(e));
@@ -793,19 +802,20 @@ static cudaError_t build_cell_lists(ht_tomo_s* t) {
 }
 }  // namespace ht
 
-extern "C" int ht_tomo_R(ht_tomo_s* t, const void* obj, void* sino, int nz, void* stream) {
-  using namespace ht;
+namespace ht {
+static int tomo_R(ht_tomo_s* t, const void* obj, void* sino, int nz, bool filt, void* stream) {
   HT_REQUIRE(t && obj && sino, "ht_tomo_R: null pointer");
   HT_REQUIRE(nz >= 0 && nz <= t->nz, "ht_tomo_R: nz exceeds the handle's slice capacity");
   if (nz == 0) return kOk;
   const GatherGeom G = geom(t);
   cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const float* symx = filt ? t->symx : nullptr;
   cudaError_t e = cudaErrorInvalidValue;
   switch (t->n) {
 #define X(A, B)                                                                                             \
   case A:                                                                                                   \
     e = tomo_R_sized<B>(static_cast<const float2*>(obj), static_cast<float2*>(sino), t->phi, t->fab, t->fde, G, \
-                        nz, t->tw_n, t->tw_2n, st);                                                         \
+                        nz, t->tw_n, t->tw_2n, symx, st);                                                   \
     break;
     HT_TOMO_SIZES(X)
 #undef X
@@ -816,19 +826,19 @@ extern "C" int ht_tomo_R(ht_tomo_s* t, const void* obj, void* sino, int nz, void
   return kOk;
 }
 
-extern "C" int ht_tomo_RT(ht_tomo_s* t, const void* sino, void* obj, int nz, void* stream) {
-  using namespace ht;
+static int tomo_RT(ht_tomo_s* t, const void* sino, void* obj, int nz, bool filt, void* stream) {
   HT_REQUIRE(t && obj && sino, "ht_tomo_RT: null pointer");
   HT_REQUIRE(nz >= 0 && nz <= t->nz, "ht_tomo_RT: nz exceeds the handle's slice capacity");
   if (nz == 0) return kOk;
   const GatherGeom G = geom(t);
   cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const float* symx = filt ? t->symx : nullptr;
   cudaError_t e = cudaErrorInvalidValue;
   switch (t->n) {
 #define X(A, B)                                                                                                 \
   case A:                                                                                                       \
     e = tomo_RT_sized<B>(static_cast<const float2*>(sino), static_cast<float2*>(obj), t->phi, t->fab, t->fde,    \
-                         t->gs, G, CellLists{t->cl_len, t->cl_off, t->cl_ent}, nz, t->tw_n, t->tw_2n, st);        \
+                         t->gs, G, CellLists{t->cl_len, t->cl_off, t->cl_ent}, nz, t->tw_n, t->tw_2n, symx, st); \
     break;
     HT_TOMO_SIZES(X)
 #undef X
@@ -837,4 +847,21 @@ extern "C" int ht_tomo_RT(ht_tomo_s* t, const void* sino, void* obj, int nz, voi
   }
   HT_CHECK_CUDA(e);
   return kOk;
+}
+}  // namespace ht
+
+extern "C" int ht_tomo_R(ht_tomo_s* t, const void* obj, void* sino, int nz, void* stream) {
+  return ht::tomo_R(t, obj, sino, nz, false, stream);
+}
+
+extern "C" int ht_tomo_RT(ht_tomo_s* t, const void* sino, void* obj, int nz, void* stream) {
+  return ht::tomo_RT(t, sino, obj, nz, false, stream);
+}
+
+extern "C" int ht_tomo_R_coeffx(ht_tomo_s* t, const void* obj, void* sino, int nz, void* stream) {
+  return ht::tomo_R(t, obj, sino, nz, true, stream);
+}
+
+extern "C" int ht_tomo_RT_coeffx(ht_tomo_s* t, const void* sino, void* obj, int nz, void* stream) {
+  return ht::tomo_RT(t, sino, obj, nz, true, stream);
 }

@@ -149,6 +149,11 @@ class Rec:
         self._hist = z(self._hist_cap, 2, dt=torch.float64)
         self._count = z(1, dt=torch.int32)
         self._graph = None
+        # BH keeps only the B-spline coefficients of proj up to date and applies
+        # the prefilter as Cx inside R / R^T and Cz on the volume (complex
+        # objects); vars/grads/etas "proj" are recomputed by bh_finish()
+        self._fold = self.complex_obj
+        self._vol = z(self.nzobj, self.nobj, self.nobj) if self._fold else None
 
     def _coeff_into(self, src, dst):
         """dst = coeff(src) (shift.py:74-82) for a [ntheta, nzobj, nobj] array."""
@@ -252,13 +257,15 @@ class Rec:
         """rec_mpi.py:498-507"""
         return self.cl_tomo.R(obj, out=out)
 
-    def min(self, prb, obj, pos, proj):
+    def min(self, prb, obj, pos, proj, prbfit_only=False):
         """rec_mpi.py:815-835: data term + probe-fit term."""
-        c = self._coeff_into(proj.contiguous(), torch.empty_like(proj))
-        _lib.call("ht_rec_forward", self._h, _lib.ptr(c), _lib.ptr(pos.contiguous()),
-                  _lib.ptr(self.eff_demagnifications), _lib.ptr(prb.contiguous()), _lib.ptr(self.data), None,
-                  _lib.ptr(self._scal), _lib.stream_ptr())
-        out = float(self._scal[0]) / self.data_size
+        out = 0.0
+        if not prbfit_only:
+            c = self._coeff_into(proj.contiguous(), torch.empty_like(proj))
+            _lib.call("ht_rec_forward", self._h, _lib.ptr(c), _lib.ptr(pos.contiguous()),
+                      _lib.ptr(self.eff_demagnifications), _lib.ptr(prb.contiguous()), _lib.ptr(self.data), None,
+                      _lib.ptr(self._scal), _lib.stream_ptr())
+            out = float(self._scal[0]) / self.data_size
         if self.lam_prbfit != 0:
             for j in range(self.ndist):
                 Dprb = self.cl_prop.D(prb[j: j + 1].contiguous(), j)[0]
@@ -344,7 +351,11 @@ class Rec:
         self._count.zero_()
 
     def bh_finish(self):
-        """End of BH (rec_mpi.py:229-232)."""
+        """End of BH (rec_mpi.py:229-232).  With the folded prefilter the proj
+        arrays, which are R of the obj arrays, are recomputed here."""
+        if self._fold:
+            for d in (self.vars, self.grads, self.etas):
+                self.fwd_tomo(d["obj"], out=d["proj"])
         self.vars["obj"] *= self.norm_const
         return self.vars
 
@@ -363,12 +374,23 @@ class Rec:
         gc, gpos, gprb = self._gradient_pass(C["vars"], vars["pos"], vars["prb"], persistent=True)
         torch.mul(gprb, rho["prb"], out=grads["prb"])
         torch.mul(gpos, rho["pos"], out=grads["pos"])
-        self._coeff_into(gc, grads["proj"])
-        grads["proj"] *= rho["obj"]
-        self.cl_tomo.RT(grads["proj"], out=grads["obj"])               # gF4
-        self.gradient_prbfit(grads["prb"], vars["prb"])
-        self.fwd_tomo(grads["obj"], out=grads["proj"])
-        self._coeff_into(grads["proj"], C["grads"])
+        if self._fold:
+            # grads obj = rho R^T coeff(gc) = rho Cz R^T Cx gc;  C grads = coeff(R grads obj) = Cx R Cz grads obj
+            st, nc = _lib.stream_ptr(), self.nobj * self.nobj
+            _lib.call("ht_tomo_RT_coeffx", self.cl_tomo._h, _lib.ptr(gc), _lib.ptr(grads["obj"]), self.nzobj, st)
+            _lib.call("ht_shift_coeff_z", self.cl_shift._hc, _lib.ptr(grads["obj"]), nc, st)
+            grads["obj"] *= rho["obj"]
+            self.gradient_prbfit(grads["prb"], vars["prb"])
+            self._vol.copy_(grads["obj"])
+            _lib.call("ht_shift_coeff_z", self.cl_shift._hc, _lib.ptr(self._vol), nc, st)
+            _lib.call("ht_tomo_R_coeffx", self.cl_tomo._h, _lib.ptr(self._vol), _lib.ptr(C["grads"]), self.nzobj, st)
+        else:
+            self._coeff_into(gc, grads["proj"])
+            grads["proj"] *= rho["obj"]
+            self.cl_tomo.RT(grads["proj"], out=grads["obj"])               # gF4
+            self.gradient_prbfit(grads["prb"], vars["prb"])
+            self.fwd_tomo(grads["obj"], out=grads["proj"])
+            self._coeff_into(grads["proj"], C["grads"])
         # ---- Hessian forms (rec_mpi.py:180-213)
         y = (C["grads"], grads["pos"], grads["prb"])
         z = None if first else (C["etas"], etas["pos"], etas["prb"])
@@ -384,12 +406,13 @@ class Rec:
         dots.zero_()
         for k, v in enumerate(("obj", "pos", "prb")):
             self._axpby_dev(etas[v], grads[v], beta, 1.0, None, -1.0, dots[k:k + 1])
-        self._axpby_dev(etas["proj"], grads["proj"], beta, 1.0, None, -1.0)
+        if not self._fold:
+            self._axpby_dev(etas["proj"], grads["proj"], beta, 1.0, None, -1.0)
         self._axpby_dev(C["etas"], C["grads"], beta, 1.0, None, -1.0)
         _lib.call("ht_bh_scalars", _lib.ptr(H), _lib.ptr(dots), int(first), 1, *rr, _lib.ptr(bh),
                   _lib.ptr(self._hist), self._hist_cap, _lib.ptr(self._count), st)
         alpha = ctypes.c_void_p(bh.data_ptr() + 8)
-        for v in ("obj", "prb", "pos", "proj"):
+        for v in ("obj", "prb", "pos") + (() if self._fold else ("proj",)):
             self._axpby_dev(vars[v], etas[v], None, 1.0, alpha, 1.0)
         self._axpby_dev(C["vars"], C["etas"], None, 1.0, alpha, 1.0)
         return None
@@ -417,13 +440,14 @@ class Rec:
         self._axpby(etas["obj"], grads["obj"], beta, -1, dots[0:1])
         self._axpby(etas["pos"], grads["pos"], beta, -1, dots[1:2])
         self._axpby(etas["prb"], grads["prb"], beta, -1, dots[2:3])
-        self._axpby(etas["proj"], grads["proj"], beta, -1)
+        if not self._fold:
+            self._axpby(etas["proj"], grads["proj"], beta, -1)
         self._axpby(C["etas"], C["grads"], beta, -1)
         d = dots.cpu().numpy()
         top = -(d[0] / rho["obj"] + d[1] / rho["pos"] + d[2] / rho["prb"])
         bottom = Hgg if first else beta * beta * Hee - 2 * beta * Hge_sym + Hgg
         alpha = top / bottom
-        for v in ("obj", "prb", "pos", "proj"):
+        for v in ("obj", "prb", "pos") + (() if self._fold else ("proj",)):
             self._axpby(vars[v], etas[v], 1, alpha)
         self._axpby(C["vars"], C["etas"], 1, alpha)
         return float(alpha), float(beta)
@@ -464,7 +488,15 @@ class Rec:
         """rec_mpi.py:862-880 (the convergence table is kept in self.table)."""
         if self.err_step == -1 or i % self.err_step != 0:
             return
-        err = self.min(vars["prb"], vars["obj"], vars["pos"], vars["proj"])
+        if self._fold and i >= 0:   # proj is not kept up to date inside BH: use its coefficients
+            _lib.call("ht_rec_forward", self._h, _lib.ptr(self._c["vars"]), _lib.ptr(vars["pos"]),
+                      _lib.ptr(self.eff_demagnifications), _lib.ptr(vars["prb"]), _lib.ptr(self.data), None,
+                      _lib.ptr(self._scal), _lib.stream_ptr())
+            err = float(self._scal[0]) / self.data_size
+            if self.lam_prbfit != 0:
+                err += self.min(vars["prb"], None, vars["pos"], None, prbfit_only=True)
+        else:
+            err = self.min(vars["prb"], vars["obj"], vars["pos"], vars["proj"])
         self.table.append((i, err, time.time() - self.time_start if i >= 0 else 0.0))
         self.time_start = time.time()
 

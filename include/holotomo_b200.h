@@ -72,6 +72,14 @@ int ht_tomo_R(ht_tomo_s* t, const void* obj, void* sino, int nz, void* stream);
 
 /* obj[nz, n, n] = R^T(sino[ntheta, nz, n]), complex64 (tomo.py:88-116). */
 int ht_tomo_RT(ht_tomo_s* t, const void* sino, void* obj, int nz, void* stream);
+/* R followed by the detector-axis half of the B-spline prefilter, and R^T
+ * preceded by it: Cx(R obj) and R^T(Cx sino), Cx the circulant filter with
+ * symbol 1 / (4 + 2 cos 2 pi k / n) along the last axis (shift.py:74-82, its
+ * row factor), applied in R's own detector spectrum at no extra pass.  With
+ * ht_shift_coeff_z on the volume they give coeff(R obj) = Cx R Cz obj and
+ * R^T coeff(sino) = Cz R^T Cx sino (the z factor commutes with R). */
+int ht_tomo_R_coeffx(ht_tomo_s* t, const void* obj, void* sino, int nz, void* stream);
+int ht_tomo_RT_coeffx(ht_tomo_s* t, const void* sino, void* obj, int nz, void* stream);
 
 /* ------------------------------------------------------------------------
  * Cubic B-spline shift family.  Replaces Shift.__init__/coeff/S/Sadj/
@@ -90,6 +98,10 @@ int ht_shift_destroy(ht_shift_s* s);
 /* out = ifft2(fft2(psi) / B3): the B-spline prefilter (shift.py:74-82);
  * complex64 [batch, nzpsi, npsi]; out may alias psi. */
 int ht_shift_coeff(ht_shift_s* s, const void* psi, void* out, long batch, void* stream);
+/* The z-axis half of the prefilter (the column factor of shift.py:74-82),
+ * in place on data [nzpsi, ncols] complex64 (a volume [nzpsi, ny, nx] has
+ * ncols = ny nx). */
+int ht_shift_coeff_z(ht_shift_s* s, void* data, long ncols, void* stream);
 
 /* out = S_{r,mag}(c) (shift.py:102-111; cuda_kernels.py:161-227). */
 int ht_shift_S(ht_shift_s* s, const void* c, const float* r, const float* mag, void* out, long batch, void* stream);

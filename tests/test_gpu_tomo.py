@@ -81,3 +81,31 @@ def test_slice_capacity_is_enforced():
     t = Tomo(32, 2, np.linspace(0, np.pi, 8, endpoint=False), 0)
     with pytest.raises(ValueError):
         t.R(torch.zeros(3, 32, 32, dtype=torch.complex64, device="cuda"))
+
+
+@pytest.mark.parametrize("n,ntheta,nz", [(64, 40, 24), (128, 90, 32)])
+def test_prefilter_folded_into_R_and_RT(n, ntheta, nz):
+    """coeff(R obj) = Cx R Cz obj and R^T coeff(sino) = Cz R^T Cx sino, with Cx
+    applied inside R's detector spectrum (ht_tomo_R_coeffx / ht_tomo_RT_coeffx)
+    and Cz on the volume (ht_shift_coeff_z): the BH iteration's form."""
+    from holotomocupy_b200 import Shift, Tomo, _lib
+    rng = np.random.default_rng(n + 1)
+    theta = np.linspace(0, np.pi, ntheta, endpoint=False).astype("float32")
+    t = Tomo(n, nz, theta, 0.9)
+    sh = Shift(n, n, nz, nz, "complex64")
+    cn = lambda *s: torch.from_numpy((rng.standard_normal(s) + 1j * rng.standard_normal(s)).astype("complex64")).cuda()
+    x, y = cn(nz, n, n), cn(ntheta, nz, n)
+    st = _lib.stream_ptr()
+    # forward
+    ref = sh.coeff(t.R(x))
+    xz = x.clone()
+    _lib.call("ht_shift_coeff_z", sh._hc, _lib.ptr(xz), n * n, st)
+    got = torch.empty(ntheta, nz, n, dtype=torch.complex64, device="cuda")
+    _lib.call("ht_tomo_R_coeffx", t._h, _lib.ptr(xz), _lib.ptr(got), nz, st)
+    assert rel_l2(got.cpu().numpy(), ref.cpu().numpy()) < 1e-5
+    # adjoint
+    ref = t.RT(sh.coeff(y))
+    got = torch.empty(nz, n, n, dtype=torch.complex64, device="cuda")
+    _lib.call("ht_tomo_RT_coeffx", t._h, _lib.ptr(y), _lib.ptr(got), nz, st)
+    _lib.call("ht_shift_coeff_z", sh._hc, _lib.ptr(got), n * n, st)
+    assert rel_l2(got.cpu().numpy(), ref.cpu().numpy()) < 1e-5
