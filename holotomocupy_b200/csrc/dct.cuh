@@ -7,7 +7,8 @@
 // w = exp(-i pi / 2N).  DCT-III (the transpose, y[t] = sum_k G[k] cos(...))
 // runs the transposed sequence: pre-combine, forward FFT, inverse reorder.
 //
-// All threads of the block must call these (they contain __syncthreads).
+// All threads of a line must call these (they barrier over the line's
+// threads, which are contiguous: line = threadIdx.x / T).
 #pragma once
 #include "lines.cuh"
 
@@ -24,7 +25,7 @@ __device__ __forceinline__ void dct2_put(const SmRow& sm, int g, float2 v) {
 template <int N, int T>
 __device__ __forceinline__ void dct2_finish(const SmRow& sm, int t, const float2* __restrict__ tw4, float2* dst,
                                             bool valid) {
-  fft_line<N, false>(sm, t, tw4);
+  fft_line<N, false>(sm, t, tw4, line_sync<T>());
   if (!valid) return;
   for (int k = t; k <= N / 2; k += T) {
     const float2 A = sm.ld(k), B = sm.ld(k == 0 ? 0 : N - k);
@@ -36,7 +37,8 @@ __device__ __forceinline__ void dct2_finish(const SmRow& sm, int t, const float2
 }
 
 // Load the DCT-III input G[0..N) from src, pre-combine and FFT.  Afterwards
-// output sample g is sm.ld(dct_perm(g, N)).  Includes the final barrier.
+// output sample g is sm.ld(dct_perm(g, N)).  Ends with a barrier over the
+// line's threads.
 template <int N, int T>
 __device__ __forceinline__ void dct3_start(const SmRow& sm, int t, const float2* __restrict__ tw4, const float2* src,
                                            bool valid) {
@@ -52,8 +54,8 @@ __device__ __forceinline__ void dct3_start(const SmRow& sm, int t, const float2*
       if (m != N / 2) sm.st(N - m, cscale(cmulc(csub(G, cmul_i(H)), w), 0.5f));
     }
   }
-  __syncthreads();
-  fft_line<N, false>(sm, t, tw4);
+  line_sync<T>()();
+  fft_line<N, false>(sm, t, tw4, line_sync<T>());
 }
 
 // Sums of K values over the T threads of each line, in double precision; the

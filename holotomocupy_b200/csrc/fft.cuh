@@ -140,15 +140,67 @@ HT_PLAN(3072, 24, 8, 8, 8, 2, 3)
 HT_PLAN(4096, 16, 8, 8, 8, 8)
 #undef HT_PLAN
 
+// ------------------------------------------------------ synchronisation
+// Barrier between the stages of one line's transform.  CtaSync: the whole
+// block (lines whose data other lines read).  LineSync<T>: only the T
+// threads of the line, which are contiguous (line = threadIdx.x / T): a
+// named barrier for T >= 64, the warp for T <= 32.
+struct CtaSync {
+  __device__ __forceinline__ void operator()() const { __syncthreads(); }
+};
+template <int T>
+struct LineSync {
+  int id;  // line index within the block (named barrier id + 1)
+  __device__ __forceinline__ void operator()() const {
+    if constexpr (T <= 32) {
+      const unsigned lanes = min(32u, blockDim.x - (threadIdx.x & ~31u));
+      __syncwarp(lanes == 32u ? 0xffffffffu : ((1u << lanes) - 1u));
+    } else {
+      static_assert(T % 32 == 0, "a named barrier counts whole warps");
+      asm volatile("bar.sync %0, %1;" ::"r"(id + 1), "n"(T) : "memory");
+    }
+  }
+};
+template <int T>
+__device__ __forceinline__ LineSync<T> line_sync() {
+  return LineSync<T>{(int)(threadIdx.x / T)};
+}
+
+// Twiddles W^(a j), j = 1..R-1, from two table reads: W^a and W^(2a) are
+// read, the others are products of them (a few ulps from the table values).
+template <int R, bool INV>
+__device__ __forceinline__ void twiddles(const float2* __restrict__ tw4, int a, int N, float2 (&w)[R]) {
+  w[0] = make_float2(1.f, 0.f);
+  float2 w1 = __ldg(&tw4[4 * a]);
+  if (INV) w1.y = -w1.y;
+  w[1] = w1;
+  if constexpr (R > 2) {
+    float2 w2 = __ldg(&tw4[4 * ((2 * a) % N)]);
+    if (INV) w2.y = -w2.y;
+    w[2] = w2;
+    if constexpr (R > 3) {
+      w[3] = cmul(w1, w2);
+      if constexpr (R > 4) {
+        const float2 w4 = cmul(w2, w2);
+        w[4] = w4;
+        w[5] = cmul(w1, w4);
+        w[6] = cmul(w2, w4);
+        w[7] = cmul(w[3], w4);
+      }
+    }
+  }
+}
+
 // ------------------------------------------------------------- one stage
 // tw4: table of exp(-2 pi i m / (4N)); W_N^a = tw4[4a].
-template <int N, int E, int R, int P, bool INV, bool LAST, class SM>
+template <int N, int E, int R, int P, bool INV, bool LAST, class SM, class SY>
 __device__ __forceinline__ void fft_stage(float2 (&v)[E], const SM& sm, int t,
-                                          const float2* __restrict__ tw4) {
+                                          const float2* __restrict__ tw4, const SY& sync) {
   constexpr int T = N / E;
   constexpr int NB = E / R;
   constexpr int NR = N / R;
   static_assert(E % R == 0, "radix must divide the samples per thread");
+  static_assert(R <= 8, "twiddles() covers radices up to 8");
 #pragma unroll
   for (int s = 0; s < NB; ++s) {
     const int b = t + s * T;
@@ -160,16 +212,14 @@ __device__ __forceinline__ void fft_stage(float2 (&v)[E], const SM& sm, int t,
     const int b = t + s * T;
     if constexpr (P > 1) {
       const int i = b % P;
+      float2 w[R];
+      twiddles<R, INV>(tw4, i * (N / (P * R)), N, w);
 #pragma unroll
-      for (int j = 1; j < R; ++j) {
-        float2 w = __ldg(&tw4[4 * (i * j * (N / (P * R)))]);
-        if (INV) w.y = -w.y;
-        v[s * R + j] = cmul(v[s * R + j], w);
-      }
+      for (int j = 1; j < R; ++j) v[s * R + j] = cmul(v[s * R + j], w[j]);
     }
     Dft<R, INV>::run(&v[s * R]);
   }
-  __syncthreads();
+  sync();
 #pragma unroll
   for (int s = 0; s < NB; ++s) {
     const int b = t + s * T;
@@ -177,26 +227,28 @@ __device__ __forceinline__ void fft_stage(float2 (&v)[E], const SM& sm, int t,
 #pragma unroll
     for (int j = 0; j < R; ++j) sm.st((b - i) * R + i + j * P, v[s * R + j]);
   }
-  __syncthreads();
+  sync();
 }
 
-template <int N, int E, int P, bool INV, class SM, int R, int... Rs>
+template <int N, int E, int P, bool INV, class SM, class SY, int R, int... Rs>
 __device__ __forceinline__ void fft_stages(float2 (&v)[E], const SM& sm, int t,
-                                           const float2* __restrict__ tw4, Radices<R, Rs...>) {
+                                           const float2* __restrict__ tw4, const SY& sync, Radices<R, Rs...>) {
   constexpr bool LAST = sizeof...(Rs) == 0;
-  fft_stage<N, E, R, P, INV, LAST>(v, sm, t, tw4);
-  if constexpr (!LAST) fft_stages<N, E, P * R, INV>(v, sm, t, tw4, Radices<Rs...>{});
+  fft_stage<N, E, R, P, INV, LAST>(v, sm, t, tw4, sync);
+  if constexpr (!LAST) fft_stages<N, E, P * R, INV>(v, sm, t, tw4, sync, Radices<Rs...>{});
 }
 
 // In-place FFT of the line held in shared memory (natural order in, natural
-// order out).  All T threads of the line must call it; every thread of the
-// block must reach it (it contains __syncthreads).  The caller synchronises
-// before (so the input is complete); the result is complete on return.
-template <int N, bool INV, class SM>
-__device__ __forceinline__ void fft_line(const SM& sm, int t, const float2* __restrict__ tw4) {
+// order out).  All T threads of the line must call it, and every thread the
+// barrier `sync` covers (it barriers between stages).  The caller
+// synchronises before (so the input is complete); the result is complete
+// for the threads `sync` covers on return.
+template <int N, bool INV, class SM, class SY = CtaSync>
+__device__ __forceinline__ void fft_line(const SM& sm, int t, const float2* __restrict__ tw4,
+                                         const SY& sync = SY{}) {
   using PL = Plan<N>;
   float2 v[PL::E];
-  fft_stages<N, PL::E, 1, INV>(v, sm, t, tw4, typename PL::R{});
+  fft_stages<N, PL::E, 1, INV>(v, sm, t, tw4, sync, typename PL::R{});
 }
 
 }  // namespace ht

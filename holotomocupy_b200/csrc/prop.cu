@@ -42,7 +42,7 @@ k_dct2_rows(const float2* in, float2* out, long nrows, const float2* __restrict_
   const float2* src = in + row * N;
   for (int g = t; g < N; g += T) sm.st(dct_perm_inv(g, N), valid ? src[g] : make_float2(0.f, 0.f));
   __syncthreads();
-  fft_line<N, false>(sm, t, tw4);
+  fft_line<N, false>(sm, t, tw4, line_sync<T>());
   if (!valid) return;
   float2* dst = out + row * N;
   for (int k = t; k <= N / 2; k += T) {
@@ -80,7 +80,7 @@ k_dct3_rows(const float2* in, float2* out, long nrows, const float2* __restrict_
     }
   }
   __syncthreads();
-  fft_line<N, false>(sm, t, tw4);
+  fft_line<N, false>(sm, t, tw4, line_sync<T>());
   if (!valid) return;
   float2* dst = out + row * N;
   for (int g = t; g < N; g += T) dst[g] = sm.ld(dct_perm(g, N));

@@ -290,10 +290,10 @@ k_symbol_rows(const float2* in, float2* out, long nrows, const float* __restrict
   SmRow sm{smem + line * SmRow::padded(N)};
   for (int k = t; k < N; k += T) sm.st(k, valid ? in[row * N + k] : make_float2(0.f, 0.f));
   __syncthreads();
-  fft_line<N, false>(sm, t, tw4);
+  fft_line<N, false>(sm, t, tw4, line_sync<T>());
   for (int k = t; k < N; k += T) sm.st(k, cscale(sm.ld(k), __ldg(&sym[k])));
   __syncthreads();
-  fft_line<N, true>(sm, t, tw4);
+  fft_line<N, true>(sm, t, tw4, line_sync<T>());
   if (!valid) return;
   for (int k = t; k < N; k += T) out[row * N + k] = sm.ld(k);
 }

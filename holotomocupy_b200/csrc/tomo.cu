@@ -234,7 +234,7 @@ k_tgather(const float2* __restrict__ fde, float2* __restrict__ sino, GatherGeom 
   }
   __syncthreads();
   const int l = threadIdx.x / T, t = threadIdx.x % T;
-  fft_line<N, true>(zline<N, Z>(smem, l), t, tw4);
+  fft_line<N, true>(zline<N, Z>(smem, l), t, tw4, line_sync<T>());
   const int z = zb * Z + l;
   if (z >= nz) return;
   float2* dst = sino + ((long)th * nz + z) * N;
@@ -530,7 +530,7 @@ k_trow_adj(const float2* __restrict__ fb, const float* __restrict__ phi, float2*
   }
   __syncthreads();
   SmRow sm = zline<N2, Z>(smem, l);
-  fft_line<N2, true>(sm, t, tw4);
+  fft_line<N2, true>(sm, t, tw4, line_sync<T>());
   const int z = zb * Z + l;
   if (z >= nz) return;
   const float s = 1.0f / (float)N2;
