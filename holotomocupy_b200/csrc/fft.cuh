@@ -143,8 +143,9 @@ HT_PLAN(4096, 16, 8, 8, 8, 8)
 // ------------------------------------------------------ synchronisation
 // Barrier between the stages of one line's transform.  CtaSync: the whole
 // block (lines whose data other lines read).  LineSync<T>: only the T
-// threads of the line, which are contiguous (line = threadIdx.x / T): a
-// named barrier for T >= 64, the warp for T <= 32.
+// threads of the line, which are contiguous (line = threadIdx.x / T): the
+// warp when T divides 32 (the line lies inside one warp), a named barrier
+// when T is a multiple of 32, else (T = 3: lines straddle warps) the block.
 struct CtaSync {
   __device__ __forceinline__ void operator()() const { __syncthreads(); }
 };
@@ -152,12 +153,13 @@ template <int T>
 struct LineSync {
   int id;  // line index within the block (named barrier id + 1)
   __device__ __forceinline__ void operator()() const {
-    if constexpr (T <= 32) {
+    if constexpr (32 % T == 0) {
       const unsigned lanes = min(32u, blockDim.x - (threadIdx.x & ~31u));
       __syncwarp(lanes == 32u ? 0xffffffffu : ((1u << lanes) - 1u));
-    } else {
-      static_assert(T % 32 == 0, "a named barrier counts whole warps");
+    } else if constexpr (T % 32 == 0) {
       asm volatile("bar.sync %0, %1;" ::"r"(id + 1), "n"(T) : "memory");
+    } else {
+      __syncthreads();
     }
   }
 };

@@ -133,7 +133,8 @@ k_trow_fwd(const float2* __restrict__ obj, const float* __restrict__ phi, float2
     sm.st(q, v);
   }
   __syncthreads();
-  fft_line<N2, false>(sm, t, tw4);
+  fft_line<N2, false>(sm, t, tw4, line_sync<T>());
+  __syncthreads();  // the stores below read every line
   float2* dst = fa + ((long)zb * n + r) * N2 * Z;
   for (int idx = threadIdx.x; idx < N2 * Z; idx += blockDim.x) {
     const int kx = idx / Z, ll = idx % Z;
@@ -161,7 +162,8 @@ k_tcol_fwd(const float2* __restrict__ fa, float2* __restrict__ fde, const float2
     zline<N2, Z>(smem, ll).st(pr, v);
   }
   __syncthreads();
-  fft_line<N2, false>(zline<N2, Z>(smem, l), t, tw4);
+  fft_line<N2, false>(zline<N2, Z>(smem, l), t, tw4, line_sync<T>());
+  __syncthreads();  // the stores below read every line
   float2* dst = fde + (long)zb * N2 * N2 * Z + (long)kx * Z;
   for (int idx = threadIdx.x; idx < N2 * Z; idx += blockDim.x) {
     const int ky = idx / Z, ll = idx % Z;
@@ -264,7 +266,8 @@ k_tsino_fft(const float2* __restrict__ sino, float2* __restrict__ gs, int ntheta
     sm.st(k, v);
   }
   __syncthreads();
-  fft_line<N, false>(sm, t, tw4);
+  fft_line<N, false>(sm, t, tw4, line_sync<T>());
+  __syncthreads();  // the stores below read every line
   float2* dst = gs + ((long)zb * ntheta + th) * N * Z;
   for (int idx = threadIdx.x; idx < N * Z; idx += blockDim.x) {
     const int tx = idx / Z, ll = idx % Z;
@@ -501,7 +504,8 @@ k_tcol_adj(const float2* __restrict__ fde, float2* __restrict__ fb, const float2
     zline<N2, Z>(smem, ll).st(ky, v);
   }
   __syncthreads();
-  fft_line<N2, true>(zline<N2, Z>(smem, l), t, tw4);
+  fft_line<N2, true>(zline<N2, Z>(smem, l), t, tw4, line_sync<T>());
+  __syncthreads();  // the stores below read every line
   float2* dst = fb + (long)zb * n * N2 * Z + (long)kx * Z;
   const float s = 1.0f / (float)N2;
   for (int idx = threadIdx.x; idx < n * Z; idx += blockDim.x) {
