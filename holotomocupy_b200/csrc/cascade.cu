@@ -63,15 +63,11 @@ __device__ __forceinline__ void bw2(float d, float (&w)[4]) {
   w[2] = -12.0f + 18.0f * e;
   w[3] = 6.0f * d;
 }
-// weight of tap j alone
+// weight of tap j alone, without branches (lanes of a warp hold different j)
 __device__ __forceinline__ float bw0_tap(float d, int j) {
-  const float e = 1.0f - d;
-  switch (j) {
-    case 0: return e * e * e;
-    case 1: return 4.0f - 6.0f * d * d + 3.0f * d * d * d;
-    case 2: return 4.0f - 6.0f * e * e + 3.0f * e * e * e;
-    default: return d * d * d;
-  }
+  float w[4];
+  bw0(d, w);
+  return (j == 0) ? w[0] : (j == 1) ? w[1] : (j == 2) ? w[2] : w[3];
 }
 
 // Object-side element: complex (complex64 objects) or real (float32 objects)
@@ -257,7 +253,7 @@ enum Glob : int { kF = 0, kQ0, kQ1, kQ2, kL10, kL11, kL12, kL20, kL21, kL22, kNG
 // ================================================= forward row pass
 // u = prb[k] exp(i S(c)) -> row DCT-II -> tmp
 template <int N, class T>
-__global__ void __launch_bounds__(StCfg<N, 1, 1>::THREADS)
+__global__ void __launch_bounds__(StCfg<N, 1, 1>::THREADS, 4)
 k_casc_fwd(const T* __restrict__ c, const float* __restrict__ pos, const float* __restrict__ mag,
            const float2* __restrict__ prb, float2* __restrict__ tmp, CascDims D, const float2* __restrict__ tw4) {
   using CF = StCfg<N, 1, 1>;
@@ -299,7 +295,7 @@ k_casc_fwd(const T* __restrict__ c, const float* __restrict__ pos, const float* 
 // tmp holds the column-processed spectrum of u.  MODE 0: x0 -> cache,
 // F, g0 -> DCT-II -> tmp.  MODE 1: F only.  MODE 2: out = |x0| (float).
 template <int N, int MODE>
-__global__ void __launch_bounds__(RowCfg<N>::THREADS)
+__global__ void __launch_bounds__(RowCfg<N>::THREADS, 4)
 k_casc_resid(float2* __restrict__ tmp, float2* __restrict__ x0c, const float* __restrict__ data,
              float* __restrict__ amp, double* __restrict__ glob, float scale, CascDims D,
              const float2* __restrict__ tw4) {
@@ -681,7 +677,7 @@ k_casc_hess_fwd(const T* __restrict__ c, const float* __restrict__ pos, const fl
 // ======================================== Hessian quadratic terms
 // y0_d = DCT-III rows of tmp[d];  Q pairs with x0 and the data.
 template <int N, int NDIR>
-__global__ void __launch_bounds__(RowCfg<N>::THREADS)
+__global__ void __launch_bounds__(RowCfg<N>::THREADS, 4)
 k_casc_hess_q(const float2* __restrict__ tmp, const float2* __restrict__ x0c, const float* __restrict__ data,
               double* __restrict__ glob, CascDims D, const float2* __restrict__ tw4) {
   constexpr int TT = RowCfg<N>::T;
