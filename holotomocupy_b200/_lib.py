@@ -39,6 +39,9 @@ SIGNATURES = {
     "ht_shift_d2S": [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _c_long, _vp],
     "ht_shift_dSadj": [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _c_long, _vp],
     "ht_filter_rows": [_c_int, _vp, _vp, _c_long, _vp, _vp],
+    "ht_laplacian_grad": [_vp, _vp, _c_int, _c_int, _c_int, _c_int, _c_float, _vp, _vp],
+    "ht_laplacian_dot": [_vp, _vp, _c_int, _c_int, _c_int, _c_int, _c_double, _vp, _vp, _vp, _vp, _vp],
+    "ht_laplacian_energy": [_vp, _c_int, _c_int, _c_int, _c_int, _c_double, _vp, _vp, _vp],
     "ht_axpby": [_vp, _vp, _c_float, _c_float, _c_long, _vp, _vp],
     "ht_dot": [_vp, _vp, _c_long, _vp, _vp],
     "ht_axpby_dev": [_vp, _vp, _vp, _c_float, _vp, _c_float, _c_long, _vp, _vp],

@@ -63,8 +63,6 @@ class Rec:
             self.lam_laplacian = 0
         if not hasattr(self, "lam_prbfit"):
             self.lam_prbfit = 0
-        if self.lam_laplacian != 0:
-            raise NotImplementedError("lam_laplacian != 0: the Laplacian regulariser is not built yet")
         self.device = torch.device("cuda", torch.cuda.current_device())
         dev = self.device
         self.F = [self.F0, self.F1, self.F2, self.F3]
@@ -154,6 +152,8 @@ class Rec:
         # objects); vars/grads/etas "proj" are recomputed by bh_finish()
         self._fold = self.complex_obj
         self._vol = z(self.nzobj, self.nobj, self.nobj) if self._fold else None
+        # Laplacian regulariser workspace (the inner Laplacian on nzobj + 2 slices)
+        self._lapw = z(self.nzobj + 2, self.nobj, self.nobj) if self.lam_laplacian != 0 else None
 
     def _coeff_into(self, src, dst):
         """dst = coeff(src) (shift.py:74-82) for a [ntheta, nzobj, nobj] array."""
@@ -252,6 +252,44 @@ class Rec:
         s = self.lam_prbfit / self.prb_size
         return out[0] * s, out[1] * s, out[2] * s
 
+    # ------------------------------------------ 3-D Laplacian regulariser
+    # rec_mpi.py:402-496 (ht_laplacian_*): gradient 2 lam/N B vars obj, Hessian
+    # form 2 lam/N Re<d, B etas obj> (the current etas obj, as the reference
+    # has it), energy lam/N |L vars obj|^2 over the object slices.
+    def _lap_args(self):
+        return self.nzobj, self.nobj, self.nobj, 1 if self.complex_obj else 0
+
+    def gradient_laplacian(self, grad_obj):
+        """rec_mpi.py:419-442"""
+        if self.lam_laplacian == 0:
+            return
+        scale = float(np.float32(2.0 * self.lam_laplacian / self.obj_size))
+        _lib.call("ht_laplacian_grad", _lib.ptr(self.vars["obj"]), _lib.ptr(grad_obj), *self._lap_args(), scale,
+                  _lib.ptr(self._lapw), _lib.stream_ptr())
+
+    def _lap_form(self, y, z, out, y2=None, out2=None):
+        """out += 2 lam/N Re<y, B z> (and out2 += ... for y2) on the device."""
+        _lib.call("ht_laplacian_dot", _lib.ptr(y), _lib.ptr(z), *self._lap_args(),
+                  2.0 * self.lam_laplacian / self.obj_size, _lib.ptr(self._lapw), out,
+                  _lib.ptr(y2) if y2 is not None else None, out2, _lib.stream_ptr())
+
+    def hessian_laplacian(self, dobj1):
+        """rec_mpi.py:444-470"""
+        if self.lam_laplacian == 0:
+            return 0.0
+        acc = torch.zeros(1, dtype=torch.float64, device=self.device)
+        self._lap_form(dobj1.contiguous(), self.etas["obj"], _lib.ptr(acc))
+        return float(acc)
+
+    def _lap_energy(self):
+        """rec_mpi.py:472-496"""
+        if self.lam_laplacian == 0:
+            return 0.0
+        acc = torch.zeros(1, dtype=torch.float64, device=self.device)
+        _lib.call("ht_laplacian_energy", _lib.ptr(self.vars["obj"]), *self._lap_args(),
+                  self.lam_laplacian / self.obj_size, _lib.ptr(self._lapw), _lib.ptr(acc), _lib.stream_ptr())
+        return float(acc)
+
     # ----------------------------------------------------- forward use
     def fwd_tomo(self, obj, out=None):
         """rec_mpi.py:498-507"""
@@ -270,6 +308,8 @@ class Rec:
             for j in range(self.ndist):
                 Dprb = self.cl_prop.D(prb[j: j + 1].contiguous(), j)[0]
                 out += self.lam_prbfit / self.prb_size * float(torch.linalg.norm(torch.abs(Dprb) - self.ref[j])) ** 2
+        if not prbfit_only:
+            out += self._lap_energy()   # of vars obj, as the reference's min has it
         return out
 
     def gen_sqrt_data(self, vars, out):
@@ -380,6 +420,7 @@ class Rec:
             _lib.call("ht_tomo_RT_coeffx", self.cl_tomo._h, _lib.ptr(gc), _lib.ptr(grads["obj"]), self.nzobj, st)
             _lib.call("ht_shift_coeff_z", self.cl_shift._hc, _lib.ptr(grads["obj"]), nc, st)
             grads["obj"] *= rho["obj"]
+            self.gradient_laplacian(grads["obj"])
             self.gradient_prbfit(grads["prb"], vars["prb"])
             self._vol.copy_(grads["obj"])
             _lib.call("ht_shift_coeff_z", self.cl_shift._hc, _lib.ptr(self._vol), nc, st)
@@ -388,6 +429,7 @@ class Rec:
             self._coeff_into(gc, grads["proj"])
             grads["proj"] *= rho["obj"]
             self.cl_tomo.RT(grads["proj"], out=grads["obj"])               # gF4
+            self.gradient_laplacian(grads["obj"])
             self.gradient_prbfit(grads["prb"], vars["prb"])
             self.fwd_tomo(grads["obj"], out=grads["proj"])
             self._coeff_into(grads["proj"], C["grads"])
@@ -395,6 +437,15 @@ class Rec:
         y = (C["grads"], grads["pos"], grads["prb"])
         z = None if first else (C["etas"], etas["pos"], etas["prb"])
         H = self._hessian_pass(C["vars"], vars["pos"], vars["prb"], y, z, out=self._H)
+        if self.lam_laplacian != 0:
+            # the regulariser's forms (B symmetric): H(g,g); H(g,eta) in both the
+            # reference's and the symmetric slot; H(eta,eta)
+            hp = H.data_ptr()
+            self._lap_form(grads["obj"], grads["obj"], ctypes.c_void_p(hp))
+            if not first:
+                self._lap_form(grads["obj"], etas["obj"], ctypes.c_void_p(hp + 8), etas["obj"],
+                               ctypes.c_void_p(hp + 16))
+                self._lap_form(grads["obj"], etas["obj"], ctypes.c_void_p(hp + 24))
         if sync or self.lam_prbfit != 0:
             return self._bh_update_host(H.cpu().numpy(), first)
         # ---- the same with the step sizes on the device
@@ -492,7 +543,7 @@ class Rec:
             _lib.call("ht_rec_forward", self._h, _lib.ptr(self._c["vars"]), _lib.ptr(vars["pos"]),
                       _lib.ptr(self.eff_demagnifications), _lib.ptr(vars["prb"]), _lib.ptr(self.data), None,
                       _lib.ptr(self._scal), _lib.stream_ptr())
-            err = float(self._scal[0]) / self.data_size
+            err = float(self._scal[0]) / self.data_size + self._lap_energy()
             if self.lam_prbfit != 0:
                 err += self.min(vars["prb"], None, vars["pos"], None, prbfit_only=True)
         else:
@@ -504,6 +555,7 @@ class Rec:
         """rec_mpi.py:305-325"""
         self.gradients_cascade(vars, grads)
         self.cl_tomo.RT(grads["proj"].contiguous(), out=grads["obj"])
+        self.gradient_laplacian(grads["obj"])
         self.gradient_prbfit(grads["prb"], vars["prb"])
 
     def hessian(self, vars, grads, etas):
@@ -511,7 +563,7 @@ class Rec:
         w = self.hessian_cascade(vars, grads, etas)
         if self.lam_prbfit != 0:
             w += self._prbfit_forms(vars["prb"], grads["prb"], etas["prb"])[1]
-        return w
+        return w + self.hessian_laplacian(grads["obj"])
 
     # ====================== cascade functions, operator by operator
     # (rec_mpi.py:517-813; used for derivative checks, not by BH())

@@ -210,6 +210,24 @@ int ht_rec_objective_noalloc(ht_prop_s* prop, int nobj, int nzobj, int ntheta, i
                              const float* pos, const float* mag, const void* prb, const float* data, double* fval,
                              void* stream);
 
+/* ------------------------------------------------------------------------
+ * 3-D Laplacian regulariser (rec_mpi.py:402-496).  Arrays [nz, ny, nx],
+ * complex64 (is_complex) or float32; work: (nz + 2) * ny * nx elements of the
+ * same type.  L: the 7-point Laplacian, periodic in y and x, of the object
+ * zero-padded in z; B = L o L with the inner L also on the ghost slice at each
+ * end, as the reference evaluates it.
+ * --------------------------------------------------------------------- */
+/* g += scale * B u  (gradient_laplacian, rec_mpi.py:419-442) */
+int ht_laplacian_grad(const void* u, void* g, int nz, int ny, int nx, int is_complex, float scale, void* work,
+                      void* stream);
+/* *out += scale * Re<y, B z>, and *out2 += scale * Re<y2, B z> if y2 != NULL (device
+ * doubles; hessian_laplacian, rec_mpi.py:444-470) */
+int ht_laplacian_dot(const void* y, const void* z, int nz, int ny, int nx, int is_complex, double scale, void* work,
+                     double* out, const void* y2, double* out2, void* stream);
+/* *out += scale * sum over the object slices of |L u|^2  (_lap_energy_local, rec_mpi.py:472-496) */
+int ht_laplacian_energy(const void* u, int nz, int ny, int nx, int is_complex, double scale, void* work, double* out,
+                        void* stream);
+
 /* Row filter: out[r] = IFFT(sym * FFT(in[r])) for each of nrows rows of
  * length N (complex64); sym: device float32 [N] in FFT order, carrying the
  * 1/N of the inverse transform.  Serves Tomo._filter_sino

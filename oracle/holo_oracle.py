@@ -549,11 +549,11 @@ class Rec:
         return self.d2F_dF[0](x, y, z, w, self.data)
 
     def hessian(self, vars, grads, etas):
-        """rec_mpi.py:234-248 (lam_prbfit = lam_laplacian = 0 terms omitted)"""
+        """rec_mpi.py:234-248"""
         w = self.hessian_cascade(vars, grads, etas)
         if self.lam_prbfit != 0:
             w += self.hessian_prbfit(vars["prb"], grads["prb"], etas["prb"])
-        return w
+        return w + self.hessian_laplacian(grads["obj"])
 
     def gradients_cascade(self, vars, grads):
         """rec_mpi.py:327-353"""
@@ -569,8 +569,50 @@ class Rec:
         """rec_mpi.py:305-325"""
         self.gradients_cascade(vars, grads)
         grads["obj"][:] = self.cl_tomo.RT(grads["proj"])               # gF4, rec_mpi.py:355-362
+        self.gradient_laplacian(grads["obj"])
         if self.lam_prbfit != 0:
             self.gradient_prbfit(grads["prb"], vars["prb"])
+
+    # ------------------------------------------ 3-D Laplacian regulariser
+    # rec_mpi.py:402-496: the 7-point Laplacian, periodic in y and x, applied
+    # to the object zero-padded by two slices in z.  The gradient and the
+    # Hessian form apply it twice (the inner Laplacian also on the two ghost
+    # slices next to the object), the energy once (object slices only).
+    @staticmethod
+    def _lap(a, b, c):
+        """rec_mpi.py:432-436"""
+        return (a + c + np.roll(b, -1, axis=1) + np.roll(b, 1, axis=1) + np.roll(b, -1, axis=2)
+                + np.roll(b, 1, axis=2) - 6 * b)
+
+    def _biharmonic(self, u):
+        p = np.zeros((u.shape[0] + 4,) + u.shape[1:], u.dtype)
+        p[2:-2] = u
+        lm = self._lap(p[:-4], p[1:-3], p[2:-2])
+        lz = self._lap(p[1:-3], p[2:-2], p[3:-1])
+        lp = self._lap(p[2:-2], p[3:-1], p[4:])
+        return self._lap(lm, lz, lp)
+
+    def gradient_laplacian(self, grad_obj):
+        """rec_mpi.py:419-442: grad_obj += 2 lam / obj_size (lap lap) vars obj."""
+        if self.lam_laplacian == 0:
+            return
+        grad_obj += (2.0 * self.lam_laplacian / self.obj_size) * self._biharmonic(self.vars["obj"])
+
+    def hessian_laplacian(self, dobj1):
+        """rec_mpi.py:444-470: 2 lam / obj_size Re<dobj1, (lap lap) etas obj> (always the
+        current etas obj, whatever directions the caller's Hessian form has)."""
+        if self.lam_laplacian == 0:
+            return 0.0
+        return 2.0 * self.lam_laplacian / self.obj_size * redot(dobj1, self._biharmonic(self.etas["obj"]))
+
+    def _lap_energy_local(self):
+        """rec_mpi.py:472-496: lam / obj_size ||lap vars obj||^2 over the object slices."""
+        if self.lam_laplacian == 0:
+            return 0.0
+        p = np.zeros((self.nzobj + 4, self.nobj, self.nobj), self.vars["obj"].dtype)
+        p[2:-2] = self.vars["obj"]
+        lap = self._lap(p[1:-3], p[2:-2], p[3:-1])
+        return self.lam_laplacian / self.obj_size * redot(lap, lap)
 
     def gradient_prbfit(self, grad_prb, prb):
         """rec_mpi.py:365-377"""
@@ -604,7 +646,7 @@ class Rec:
             if self.lam_prbfit != 0:
                 Dprb = self.cl_prop.D(prb[j: j + 1], j)[0]
                 out += self.lam_prbfit / self.prb_size * np.linalg.norm(np.abs(Dprb) - self.ref[j]) ** 2
-        return out
+        return out + self._lap_energy_local()
 
     def gen_sqrt_data(self, vars, out):
         """rec_mpi.py:882-897"""

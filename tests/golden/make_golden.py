@@ -201,14 +201,65 @@ def rec_cases(ns):
     np.savez_compressed(os.path.join(HERE, "rec.npz"), **out)
 
 
+def lap_cases(ns):
+    """The 3-D Laplacian regulariser (rec_mpi.py:402-496): its gradient, Hessian
+    form and energy at one point, and a 4-iteration BH run with lam_laplacian > 0."""
+    out = {}
+    n, ntheta, ndist, nobj = 32, 4, 1, 32
+    rng = np.random.default_rng(3)
+    args = rec_args(n, ntheta, ndist, nobj)
+    args.lam_laplacian = 0.7
+    rec = ns.rec_mpi.Rec(args)
+    u = crand(rng, (nobj, nobj, nobj), 0.3)
+    e = crand(rng, (nobj, nobj, nobj), 0.2)
+    d1 = crand(rng, (nobj, nobj, nobj), 0.2)
+    rec.vars["obj"][:] = u
+    rec.etas["obj"][:] = e
+    g = crand(rng, (nobj, nobj, nobj), 0.1)
+    g0 = g.copy()
+    rec.gradient_laplacian(g)
+    out.update({"l_dims": np.array([n, ntheta, ndist, nobj]), "l_lam": np.array(args.lam_laplacian),
+                "l_u": u, "l_e": e, "l_d1": d1, "l_g0": g0, "l_g": np.array(g),
+                "l_h": np.array(float(rec.hessian_laplacian(d1))),
+                "l_energy": np.array(float(rec._lap_energy_local()))})
+    # BH with the regulariser
+    n, ntheta, ndist, nobj, niter = 32, 12, 2, 32, 4
+    rng = np.random.default_rng(7)
+    args = rec_args(n, ntheta, ndist, nobj, niter)
+    args.lam_laplacian = 2e-3
+    rec = ns.rec_mpi.Rec(args)
+    obj = phantom(nobj, rng)
+    prb = (1 + 0.1 * crand(rng, (ndist, n, n))).astype("complex64")
+    pos = frand(rng, (ntheta, ndist, 2), 1.0)
+    pos_err = frand(rng, (ntheta, ndist, 2), 0.2)
+    rec.vars["obj"][:] = obj
+    rec.vars["prb"][:] = ns.cp.array(prb)
+    rec.vars["pos"][:] = ns.cp.array(pos)
+    rec.gen_sqrt_data(rec.vars, rec.data)
+    rec.vars["obj"][:] = 0
+    rec.vars["prb"][:] = ns.cp.array(1)
+    rec.vars["pos"][:] = ns.cp.array(pos + pos_err)
+    pairs = []
+    orig = rec.allreduce2
+    rec.allreduce2 = lambda a, b: (pairs.append((float(a), float(b))), orig(a, b))[1]
+    rec.BH()
+    out.update({
+        "lbh_dims": np.array([n, ntheta, ndist, nobj, niter]), "lbh_lam": np.array(args.lam_laplacian),
+        "lbh_obj": np.array(rec.vars["obj"]), "lbh_prb": np.asarray(rec.vars["prb"]),
+        "lbh_pos": np.asarray(rec.vars["pos"]), "lbh_proj": np.array(rec.vars["proj"]),
+        "lbh_topbottom": np.array(pairs, dtype="float64"),
+    })
+    np.savez_compressed(os.path.join(HERE, "lap.npz"), **out)
+
+
 def main():
     src = sys.argv[1] if len(sys.argv) > 1 else None
     if src is None:
         raise SystemExit("usage: make_golden.py <reference src dir>")
     ns = load_reference(src)
-    which = sys.argv[2:] or ["tomo", "prop", "shift", "rec"]
+    which = sys.argv[2:] or ["tomo", "prop", "shift", "rec", "lap"]
     for w in which:
-        {"tomo": tomo_cases, "prop": prop_cases, "shift": shift_cases, "rec": rec_cases}[w](ns)
+        {"tomo": tomo_cases, "prop": prop_cases, "shift": shift_cases, "rec": rec_cases, "lap": lap_cases}[w](ns)
         print("wrote", w)
 
 

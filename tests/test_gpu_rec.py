@@ -239,3 +239,48 @@ def test_bh_32_iterations_against_fp64_oracle(golden, mode):
     orc.BH()
     for k in ("obj", "prb", "pos"):
         assert rel_l2(rec.vars[k].cpu().numpy(), orc.vars[k]) < 1e-4, k
+
+
+def test_laplacian_terms_match_reference(golden):
+    """gradient_laplacian, hessian_laplacian and the energy against the
+    reference's own values (rec_mpi.py:402-496)."""
+    from holotomocupy_b200.rec import Rec
+    g = golden("lap")
+    n, ntheta, ndist, nobj = [int(v) for v in g["l_dims"]]
+    args = rec_args(n, ntheta, ndist, nobj)
+    args.lam_laplacian = float(g["l_lam"])
+    rec = Rec(args)
+    rec.vars["obj"][:] = cuda(g["l_u"])
+    rec.etas["obj"][:] = cuda(g["l_e"])
+    gr = cuda(g["l_g0"]).clone()
+    rec.gradient_laplacian(gr)
+    assert rel_l2((gr - cuda(g["l_g0"])).cpu().numpy(), g["l_g"] - g["l_g0"]) < TOL
+    assert abs(rec.hessian_laplacian(cuda(g["l_d1"])) / float(g["l_h"]) - 1) < TOL
+    assert abs(rec._lap_energy() / float(g["l_energy"]) - 1) < TOL
+
+
+@pytest.mark.parametrize("mode", ["host", "graph"])
+def test_bh_with_laplacian_matches_reference(golden, mode):
+    """4 BH iterations with lam_laplacian > 0 against the reference's run."""
+    from holotomocupy_b200.rec import Rec
+    gr = golden("rec")
+    g = golden("lap")
+    n, ntheta, ndist, nobj, niter = [int(v) for v in g["lbh_dims"]]
+    args = rec_args(n, ntheta, ndist, nobj, niter)
+    args.lam_laplacian = float(g["lbh_lam"])
+    rec = Rec(args)
+    rec.vars["obj"][:] = cuda(gr["bh_obj_true"])
+    rec.vars["prb"][:] = cuda(gr["bh_prb_true"])
+    rec.vars["pos"][:] = cuda(gr["bh_pos_true"])
+    rec.gen_sqrt_data(rec.vars, rec.data)
+    rec.vars["obj"][:] = 0
+    rec.vars["prb"][:] = 1
+    rec.vars["pos"][:] = cuda(gr["bh_pos_true"] + gr["bh_pos_err"])
+    record = []
+    rec.BH(record=record, mode=mode)
+    tb = g["lbh_topbottom"]
+    ref_alpha = [tb[0, 0] / tb[0, 1]] + [tb[2 * i, 0] / tb[2 * i, 1] for i in range(1, niter)]
+    for (i, a, b), ra in zip(record, ref_alpha):
+        assert abs(a / ra - 1) < 1e-4, (i, a, ra)
+    for k in ("obj", "prb", "pos", "proj"):
+        assert rel_l2(rec.vars[k].cpu().numpy(), g[f"lbh_{k}"]) < TOL, k

@@ -119,3 +119,40 @@ def test_bh(golden, dt, tol):
     rec.BH()
     for k in ("obj", "prb", "pos", "proj"):
         assert rel_l2(rec.vars[k], g[f"bh_{k}"]) < tol
+
+
+@pytest.mark.parametrize("dt,tol", [("complex64", TOL32), ("complex128", TOL64)])
+def test_laplacian_terms(golden, dt, tol):
+    """gradient_laplacian, hessian_laplacian and the energy (rec_mpi.py:402-496)."""
+    g = golden("lap")
+    n, ntheta, ndist, nobj = [int(v) for v in g["l_dims"]]
+    args = rec_args(n, ntheta, ndist, nobj)
+    args.lam_laplacian = float(g["l_lam"])
+    rec = O.Rec(args, dt)
+    rec.vars["obj"][:] = g["l_u"]
+    rec.etas["obj"][:] = g["l_e"]
+    gr = g["l_g0"].astype(rec.vars["obj"].dtype)
+    rec.gradient_laplacian(gr)
+    assert rel_l2(gr - g["l_g0"], g["l_g"] - g["l_g0"]) < 10 * tol
+    assert abs(rec.hessian_laplacian(g["l_d1"]) / float(g["l_h"]) - 1) < 10 * tol
+    assert abs(rec._lap_energy_local() / float(g["l_energy"]) - 1) < 10 * tol
+
+
+@pytest.mark.parametrize("dt,tol", [("complex64", 1e-5), ("complex128", 1e-5)])
+def test_bh_with_laplacian(golden, dt, tol):
+    gr = golden("rec")
+    g = golden("lap")
+    n, ntheta, ndist, nobj, niter = [int(v) for v in g["lbh_dims"]]
+    args = rec_args(n, ntheta, ndist, nobj, niter)
+    args.lam_laplacian = float(g["lbh_lam"])
+    rec = O.Rec(args, dt)
+    rec.vars["obj"][:] = gr["bh_obj_true"]
+    rec.vars["prb"][:] = gr["bh_prb_true"]
+    rec.vars["pos"][:] = gr["bh_pos_true"]
+    rec.gen_sqrt_data(rec.vars, rec.data)
+    rec.vars["obj"][:] = 0
+    rec.vars["prb"][:] = 1
+    rec.vars["pos"][:] = gr["bh_pos_true"] + gr["bh_pos_err"]
+    rec.BH()
+    for k in ("obj", "prb", "pos", "proj"):
+        assert rel_l2(rec.vars[k], g[f"lbh_{k}"]) < tol, k
