@@ -222,6 +222,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--serve-requests", type=int, default=12, help="requests in the mixed served stream (0: skip)")
     ap.add_argument("--serve-iters", type=int, default=16)
+    ap.add_argument("--c5", action="store_true",
+                    help="the 2048^3 x 1800 x 4 operator measurement (D, R, R^T on a 256-slice sub-volume) "
+                         "instead of the BH line")
     ap.add_argument("--profile", action="store_true",
                     help="time the device iterations only (no roofline, e2e or CPU legs): for ncu launch lists")
     a = ap.parse_args()
@@ -233,6 +236,9 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", 0))
     if a.impl == "reference":
         run_reference(a, rank)
+        return
+    if a.c5:
+        run_c5(a)
         return
 
     import torch
@@ -361,6 +367,68 @@ def main():
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()
+
+
+def run_c5(a, n=2048, ntheta=1800, ndist=4, nz_sub=256, nimg_chunk=256):
+    """Operators at the 2048^3, 1800-angle, 4-distance size: the propagator D
+    over image chunks and R, R^T of a 256-slice sub-volume (the full state,
+    ~430 GB, exceeds one GPU; the BH iteration at this size is not run).
+    Achieved = algorithmic bytes / CUDA-event time against the measured HBM
+    copy bandwidth."""
+    import torch
+    from holotomocupy_b200 import Propagation, Tomo, _lib
+    dev = torch.device("cuda", 0)
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    peak = float(peaks.get("hbm_gbs", 6650.0))
+    g = torch.Generator(device=dev).manual_seed(5)
+
+    def timed(fn, reps):
+        for _ in range(a.warmup):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps * 1e-3
+
+    out = {}
+    prop = Propagation(n, n, nimg_chunk, ndist, WAVELENGTH, VOXEL, DIST[:ndist])
+    x = torch.randn(nimg_chunk, n, n, dtype=torch.complex64, device=dev, generator=g)
+    y = torch.empty_like(x)
+    st = _lib.stream_ptr()
+    t = timed(lambda: _lib.call("ht_prop_D", prop._h, _lib.ptr(x), _lib.ptr(y), nimg_chunk, 0, st), a.steps)
+    alg = 16.0 * nimg_chunk * n * n + 32.0 * n * n
+    out["D"] = {"images_per_launch": nimg_chunk, "launch_ms": t * 1e3, "achieved_gbs": alg / t / 1e9,
+                "frac": alg / t / 1e9 / peak, "all_images_s": t * ntheta * ndist / nimg_chunk}
+    del x, y, prop
+    torch.cuda.empty_cache()
+    theta = np.linspace(0, np.pi, ntheta, endpoint=False).astype("float32")
+    tomo = Tomo(n, nz_sub, theta, 0.9)
+    obj = torch.randn(nz_sub, n, n, dtype=torch.complex64, device=dev, generator=g)
+    sino = torch.empty(ntheta, nz_sub, n, dtype=torch.complex64, device=dev)
+    back = torch.empty_like(obj)
+    t = timed(lambda: tomo.R(obj, out=sino), max(1, a.steps // 2))
+    alg = 8.0 * nz_sub * n * n + 8.0 * ntheta * nz_sub * n
+    out["R"] = {"slices": nz_sub, "launch_ms": t * 1e3, "achieved_gbs": alg / t / 1e9, "frac": alg / t / 1e9 / peak,
+                "full_volume_s": t * n / nz_sub}
+    t = timed(lambda: tomo.RT(sino, out=back), max(1, a.steps // 2))
+    out["RT"] = {"slices": nz_sub, "launch_ms": t * 1e3, "achieved_gbs": alg / t / 1e9, "frac": alg / t / 1e9 / peak,
+                 "full_volume_s": t * n / nz_sub}
+    line = {"metric": "operator HBM GB/s at 2048^3 x 1800 angles x 4 distances", "value": out["D"]["achieved_gbs"],
+            "unit": "GB/s", "n_gpus": 1, "steps": a.steps, "warmup": a.warmup, "higher_is_better": True,
+            "dtype": "c64", "data": "synthetic (seeded normal complex64)", "peak_gbs": peak,
+            "peak_source": "measured" if peaks else "fallback",
+            "config": {"workload": "D over 256-image chunks of 2048^2; R, R^T of a 256-slice 2048^2 sub-volume at "
+                                   "1800 angles", "n": n, "ntheta": ntheta, "ndist": ndist},
+            "operators": out}
+    print(json.dumps(line), flush=True)
 
 
 def served_vs_plain(nreq, niter, seed):

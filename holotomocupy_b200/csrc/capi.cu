@@ -10,11 +10,13 @@ extern "C" const char* ht_last_error(void) { return ht::last_error(); }
 extern "C" long ht_launch_count(void) { return ht::launch_count(); }
 
 // ------------------------------------------------------------ graphs
-// Record the work issued to `stream` (by this thread) until ht_graph_end into
-// a graph, instead of running it.
+// Record the work issued to `stream` until ht_graph_end into a graph, instead
+// of running it.  Relaxed mode: a free of unrelated memory made meanwhile
+// (say, by another request's object being destroyed) does not invalidate
+// the recording.
 extern "C" int ht_graph_begin(void* stream) {
   HT_REQUIRE(stream, "ht_graph_begin: capture needs a non-default stream");
-  HT_CHECK_CUDA(cudaStreamBeginCapture(static_cast<cudaStream_t>(stream), cudaStreamCaptureModeThreadLocal));
+  HT_CHECK_CUDA(cudaStreamBeginCapture(static_cast<cudaStream_t>(stream), cudaStreamCaptureModeRelaxed));
   return ht::kOk;
 }
 

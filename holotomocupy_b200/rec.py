@@ -21,6 +21,7 @@ Optional argument keys beyond the reference's: ``distance``, ``wavelength``,
 directly instead of deriving it from ``z1``/``energy`` (rec_mpi.py:55-60).
 """
 import ctypes
+import gc
 import math
 import time
 
@@ -517,12 +518,16 @@ class Rec:
             raise ValueError("graph capture needs lam_prbfit == 0 (the probe-fit forms are host-side)")
         self.release_graph()
         st = _lib.stream_ptr()
+        gc_on = gc.isenabled()
+        gc.disable()   # no collector-driven destructors (device frees) while recording
         _lib.call("ht_graph_begin", st)
         try:
             self.bh_iteration(self.start_iter + 1, sync=False)
         finally:
             ex = ctypes.c_void_p()
             _lib.call("ht_graph_end", st, ctypes.byref(ex))
+            if gc_on:
+                gc.enable()
         self._graph = ex
         return ex
 

@@ -237,7 +237,7 @@ int ht_filter_rows(int N, const void* in, void* out, long nrows, const float* sy
 /* ------------------------------------------------------------------------
  * CUDA graphs of a stream's work (the reference launches every kernel from
  * Python each iteration; no counterpart).  ht_graph_begin starts recording
- * the work this thread issues to `stream` (a non-default stream); nothing
+ * the work issued to `stream` (a non-default stream, relaxed capture mode); nothing
  * runs until the graph is launched.  ht_graph_end ends the recording and
  * returns an executable graph in *exec; ht_graph_launch runs it on a stream;
  * ht_graph_destroy frees it.  Everything recorded must already have run
