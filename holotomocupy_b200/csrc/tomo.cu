@@ -594,7 +594,7 @@ static cudaError_t tomo_RT_sized(const float2* sino, float2* obj, const float* p
   count_launch();
   {
     KTimer kt("k_tcell", st, (double)nz);
-    constexpr int ZG = 2;
+    constexpr int ZG = 2;  // slice batches per read of the pair lists
     const SliceShape sh = slice_shape(64 / Z);
     const long nsl = (long)((N2 + sh.tw - 1) / sh.tw) * ((N2 + sh.th - 1) / sh.th);
     k_tcell<Z, ZG><<<dim3((unsigned)((nsl * 32 + 255) / 256), (unsigned)((nzb + ZG - 1) / ZG)), 256, 0, st>>>(
