@@ -14,7 +14,10 @@ reconstructions resident at once:
   overlap on the GPU;
 * the loop never blocks on one request: it polls each stream's last event,
   records the per-iteration latency, launches the next iteration or retires
-  the request (results copied to the host) and frees its memory.
+  the request (results copied to the host);
+* a retired request's device memory is released lazily -- when an admission
+  needs it, or when the loop ends -- because releasing it synchronises the
+  whole device and would drain the other requests' queued work.
 
 Every request's arithmetic is the same as running it alone (the same kernels
 in the same order on its own buffers).
@@ -140,8 +143,17 @@ class Server:
         r.result = out
         r.t_done = time.perf_counter() - t0
         rec.release_graph()
+        self._retired.append((rec, slot.bytes))   # freed lazily (see _release)
         slot.rec = None
         self.done.append(r)
+
+    def _release(self):
+        """Free the retired reconstructions' device memory (synchronises the
+        device); returns the bytes released."""
+        freed = sum(b for _, b in self._retired)
+        self._retired.clear()
+        torch.cuda.synchronize(self.device)
+        return freed
 
     # ------------------------------------------------------------- loop
     def run(self, realtime=True):
@@ -152,11 +164,14 @@ class Server:
         self.queue = []
         active = []
         used = 0
+        self._retired = []
         t0 = time.perf_counter()
         while pending or active:
             now = time.perf_counter() - t0
             while pending and len(active) < self.max_active and (not realtime or pending[0].arrival <= now):
                 need = estimate_bytes(pending[0].args)
+                if used + need > self.budget and self._retired:
+                    used -= self._release()
                 if active and used + need > self.budget:
                     break
                 r = pending.pop(0)
@@ -179,7 +194,6 @@ class Server:
                     self._retire(slot, t0)
                     active.remove(slot)
                     self._streams.append(slot.stream)
-                    used -= slot.bytes
                     progressed = True
                     continue
                 self._launch(slot)
@@ -190,6 +204,7 @@ class Server:
                 else:
                     time.sleep(20e-6)
         self.wall = time.perf_counter() - t0
+        self._release()
         return self.done
 
     @staticmethod
