@@ -193,9 +193,22 @@ __device__ __forceinline__ void twiddles(const float2* __restrict__ tw4, int a, 
   }
 }
 
+// Loads through one view, stores through another: a first stage that reads
+// its line from global memory, or a last stage that writes it there.
+template <class L, class S>
+struct SplitView {
+  L l;
+  S s;
+  __device__ __forceinline__ float2 ld(int k) const { return l.ld(k); }
+  __device__ __forceinline__ void st(int k, float2 v) const { s.st(k, v); }
+};
+
 // ------------------------------------------------------------- one stage
-// tw4: table of exp(-2 pi i m / (4N)); W_N^a = tw4[4a].
-template <int N, int E, int R, int P, bool INV, bool LAST, class SM, class SY>
+// tw4: table of exp(-2 pi i m / (4N)); W_N^a = tw4[4a].  SYNC_MID: barrier
+// between the loads and the stores (needed when both are the same shared
+// line); SYNC_END: barrier after the stores (needed when the next stage
+// reads them).
+template <int N, int E, int R, int P, bool INV, bool SYNC_MID, bool SYNC_END, class SM, class SY>
 __device__ __forceinline__ void fft_stage(float2 (&v)[E], const SM& sm, int t,
                                           const float2* __restrict__ tw4, const SY& sync) {
   constexpr int T = N / E;
@@ -221,7 +234,7 @@ __device__ __forceinline__ void fft_stage(float2 (&v)[E], const SM& sm, int t,
     }
     Dft<R, INV>::run(&v[s * R]);
   }
-  sync();
+  if constexpr (SYNC_MID) sync();
 #pragma unroll
   for (int s = 0; s < NB; ++s) {
     const int b = t + s * T;
@@ -229,15 +242,36 @@ __device__ __forceinline__ void fft_stage(float2 (&v)[E], const SM& sm, int t,
 #pragma unroll
     for (int j = 0; j < R; ++j) sm.st((b - i) * R + i + j * P, v[s * R + j]);
   }
-  sync();
+  if constexpr (SYNC_END) sync();
 }
 
 template <int N, int E, int P, bool INV, class SM, class SY, int R, int... Rs>
 __device__ __forceinline__ void fft_stages(float2 (&v)[E], const SM& sm, int t,
                                            const float2* __restrict__ tw4, const SY& sync, Radices<R, Rs...>) {
   constexpr bool LAST = sizeof...(Rs) == 0;
-  fft_stage<N, E, R, P, INV, LAST>(v, sm, t, tw4, sync);
+  fft_stage<N, E, R, P, INV, true, true>(v, sm, t, tw4, sync);
   if constexpr (!LAST) fft_stages<N, E, P * R, INV>(v, sm, t, tw4, sync, Radices<Rs...>{});
+}
+
+// As fft_stages, with the first stage loading from `in` (GIN) and/or the last
+// stage storing to `out` (GOUT) instead of the shared line: a stage that
+// reads global memory needs no barrier before its stores, and a stage that
+// writes global memory none at all.
+template <int N, int E, int P, bool INV, bool GIN, bool GOUT, class IN, class SM, class OUT, class SY, int R,
+          int... Rs>
+__device__ __forceinline__ void fft_stages_io(float2 (&v)[E], const IN& in, const SM& sm, const OUT& out, int t,
+                                              const float2* __restrict__ tw4, const SY& sync, Radices<R, Rs...>) {
+  constexpr bool FIRST = P == 1;
+  constexpr bool LAST = sizeof...(Rs) == 0;
+  static_assert(!(FIRST && LAST), "a line transform here has at least two stages");
+  if constexpr (FIRST && GIN) {
+    fft_stage<N, E, R, P, INV, false, true>(v, SplitView<IN, SM>{in, sm}, t, tw4, sync);
+  } else if constexpr (LAST && GOUT) {
+    fft_stage<N, E, R, P, INV, false, false>(v, SplitView<SM, OUT>{sm, out}, t, tw4, sync);
+  } else {
+    fft_stage<N, E, R, P, INV, true, true>(v, sm, t, tw4, sync);
+  }
+  if constexpr (!LAST) fft_stages_io<N, E, P * R, INV, GIN, GOUT>(v, in, sm, out, t, tw4, sync, Radices<Rs...>{});
 }
 
 // In-place FFT of the line held in shared memory (natural order in, natural
@@ -251,6 +285,28 @@ __device__ __forceinline__ void fft_line(const SM& sm, int t, const float2* __re
   using PL = Plan<N>;
   float2 v[PL::E];
   fft_stages<N, PL::E, 1, INV>(v, sm, t, tw4, sync, typename PL::R{});
+}
+
+// FFT of a line read from `in` (any view with ld(k): sample k of the line),
+// result left in shared memory (complete for the threads `sync` covers).  No
+// barrier is needed before it.
+template <int N, bool INV, class IN, class SM, class SY = CtaSync>
+__device__ __forceinline__ void fft_line_from(const IN& in, const SM& sm, int t, const float2* __restrict__ tw4,
+                                              const SY& sync = SY{}) {
+  using PL = Plan<N>;
+  float2 v[PL::E];
+  fft_stages_io<N, PL::E, 1, INV, true, false>(v, in, sm, sm, t, tw4, sync, typename PL::R{});
+}
+
+// FFT of a line in shared memory (the caller synchronised after writing it),
+// result stored through `out` (any view with st(k, v)); the line is not
+// barriered afterwards.
+template <int N, bool INV, class SM, class OUT, class SY = CtaSync>
+__device__ __forceinline__ void fft_line_to(const SM& sm, const OUT& out, int t, const float2* __restrict__ tw4,
+                                            const SY& sync = SY{}) {
+  using PL = Plan<N>;
+  float2 v[PL::E];
+  fft_stages_io<N, PL::E, 1, INV, false, true>(v, sm, sm, out, t, tw4, sync, typename PL::R{});
 }
 
 }  // namespace ht

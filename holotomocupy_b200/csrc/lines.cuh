@@ -45,6 +45,9 @@ inline cudaError_t allow_smem(K kernel, int bytes) {
 __device__ __forceinline__ int dct_perm_inv(int g, int N) { return (g & 1) ? (N - 1 - (g >> 1)) : (g >> 1); }
 // Sample of the reordered sequence that lands on output position g.
 __device__ __forceinline__ int dct_perm(int g, int N) { return dct_perm_inv(g, N); }
+// Inverse of dct_perm_inv: the input sample at position p of the reordered
+// sequence (and the output sample that position p lands on).
+__device__ __forceinline__ int dct_sample_at(int p, int N) { return (2 * p < N) ? 2 * p : 2 * (N - 1 - p) + 1; }
 
 }  // namespace ht
 

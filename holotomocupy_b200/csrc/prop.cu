@@ -87,7 +87,32 @@ k_dct3_rows(const float2* in, float2* out, long nrows, const float2* __restrict_
 }
 
 // ------------------------------------- column DCT-II, x table, DCT-III
-// data: [nimg, NZ, n] in place; H: [NZ, n] (the j-th distance's Hw).
+// Column col of an image, read (ColIn) or written (ColOut) at position k of
+// the reordered sequence, i.e. at image row dct_sample_at(k).
+template <int NZ>
+struct ColIn {
+  const float2* p;  // row 0 of the column
+  int n;
+  bool valid;
+  __device__ __forceinline__ float2 ld(int k) const {
+    return valid ? p[(long)dct_sample_at(k, NZ) * n] : make_float2(0.f, 0.f);
+  }
+};
+template <int NZ>
+struct ColOut {
+  float2* p;
+  int n;
+  bool valid;
+  __device__ __forceinline__ void st(int k, float2 v) const {
+    if (valid) p[(long)dct_sample_at(k, NZ) * n] = v;
+  }
+};
+
+// data: [nimg, NZ, n] in place; H: [NZ, n] (the j-th distance's Hw).  The
+// first FFT stage loads the block's C columns straight from global memory and
+// the last one stores them there (a warp covers 32/C rows of C adjacent
+// columns per access), so the column tile passes through shared memory only
+// between stages.
 template <int NZ, bool CONJ>
 __global__ void __launch_bounds__(ColCfg<NZ>::THREADS)
 k_dct_cols(float2* data, int n, const float2* __restrict__ Hall, int ntab, const float2* __restrict__ tw4) {
@@ -97,17 +122,11 @@ k_dct_cols(float2* data, int n, const float2* __restrict__ Hall, int ntab, const
   constexpr int T = ColCfg<NZ>::T;
   extern __shared__ float2 tile[];
   const int c = threadIdx.x % C, t = threadIdx.x / C;
-  const int col0 = blockIdx.x * C;
-  float2* img = data + (long)blockIdx.y * NZ * n;
-  for (int idx = threadIdx.x; idx < NZ * C; idx += blockDim.x) {
-    const int r = idx / C, cc = idx % C;
-    const int col = col0 + cc;
-    tile[col_row<C>(dct_perm_inv(r, NZ)) * C + cc] = (col < n) ? img[(long)r * n + col] : make_float2(0.f, 0.f);
-  }
-  __syncthreads();
+  const bool valid = blockIdx.x * C + c < n;
+  const int col = min((int)blockIdx.x * C + c, n - 1);
+  float2* img = data + (long)blockIdx.y * NZ * n + col;
   SmCol<C> sm{tile + c};
-  fft_line<NZ, false>(sm, t, tw4);
-  const int col = min(col0 + c, n - 1);
+  fft_line_from<NZ, false>(ColIn<NZ>{img, n, valid}, sm, t, tw4);
   for (int k = t; k <= NZ / 2; k += T) {
     const float2 A = sm.ld(k), B = sm.ld(k == 0 ? 0 : NZ - k);
     const float2 w = __ldg(&tw4[k]);
@@ -128,12 +147,7 @@ k_dct_cols(float2* data, int n, const float2* __restrict__ Hall, int ntab, const
     }
   }
   __syncthreads();
-  fft_line<NZ, false>(sm, t, tw4);
-  for (int idx = threadIdx.x; idx < NZ * C; idx += blockDim.x) {
-    const int r = idx / C, cc = idx % C;
-    const int cl = col0 + cc;
-    if (cl < n) img[(long)r * n + cl] = tile[col_row<C>(dct_perm(r, NZ)) * C + cc];
-  }
+  fft_line_to<NZ, false>(sm, ColOut<NZ>{img, n, valid}, t, tw4);
 }
 
 // ---------------------------------------------------------------- launch
