@@ -200,17 +200,21 @@ __host__ __device__ constexpr int red_doubles(int K, int threads) {
 // Launch shape of a stencil row kernel: NFFT row lines of the DCT plus NSET
 // vertically reduced object rows (nobj <= N values each) per detector row,
 // with as many detector rows per CTA as keep the shared memory near 100 KB.
+// A detector row has TR = NFFT * T threads: the stencil work is spread over
+// all of them and each group of T transforms one of the row's NFFT lines, so
+// the threads per SM grow with the row's shared memory.
 template <int N, int NSET, int NFFT>
 struct StCfg {
   static constexpr int T = Plan<N>::T;
+  static constexpr int TR = NFFT * T;
   static constexpr int PER_LINE = NFFT * SmRow::padded(N) * 8 + NSET * N * 8;
   static constexpr int fit(int l) { return (l > 1 && l * PER_LINE > 100 * 1024) ? fit(l / 2) : l; }
-  static constexpr int LINES = fit(RowCfg<N>::LINES);
-  static constexpr int THREADS = LINES * T;
+  static constexpr int LINES = fit(RowCfg<N>::LINES / NFFT > 0 ? RowCfg<N>::LINES / NFFT : 1);
+  static constexpr int THREADS = LINES * TR;
   // dynamic shared memory: FFT lines, then reduction scratch, then the rows
   static constexpr int FFT_BYTES = LINES * NFFT * SmRow::padded(N) * 8;
   static int bytes(int K, int nobj, int elem) {
-    return FFT_BYTES + red_doubles<T>(K, THREADS) * 8 + LINES * NSET * nobj * elem;
+    return FFT_BYTES + red_doubles<TR>(K, THREADS) * 8 + LINES * NSET * nobj * elem;
   }
 };
 
@@ -547,7 +551,7 @@ k_casc_hess_fwd(const T* __restrict__ c, const float* __restrict__ pos, const fl
                 const float2* __restrict__ tw4) {
   constexpr int NS = 2 * (1 + NDIR);
   using CF = StCfg<N, NS, NDIR>;
-  constexpr int TT = CF::T;
+  constexpr int TT = CF::TR;  // threads of a detector row; CF::T of them per FFT line
   constexpr int LINES = CF::LINES;
   constexpr int K = (NDIR == 2) ? 10 : 4;
   extern __shared__ float2 smem[];
@@ -669,9 +673,10 @@ k_casc_hess_fwd(const T* __restrict__ c, const float* __restrict__ pos, const fl
     }
   }
   __syncthreads();
+  // direction d's line is transformed by the row's d-th group of CF::T threads
   const long nrow = D.nimg * D.nz;
-  dct2_finish<N, TT>(sm0, t, tw4, tmp + row * N, valid);
-  if (NDIR == 2) dct2_finish<N, TT>(sm1, t, tw4, tmp + (nrow + row) * N, valid);
+  const int d = t / CF::T;
+  dct2_finish<N, CF::T>(d == 0 ? sm0 : sm1, t % CF::T, tw4, tmp + (d * nrow + row) * N, valid);
 }
 
 // ======================================== Hessian quadratic terms
