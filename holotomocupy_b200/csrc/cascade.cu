@@ -63,12 +63,6 @@ __device__ __forceinline__ void bw2(float d, float (&w)[4]) {
   w[2] = -12.0f + 18.0f * e;
   w[3] = 6.0f * d;
 }
-// weight of tap j alone, without branches (lanes of a warp hold different j)
-__device__ __forceinline__ float bw0_tap(float d, int j) {
-  float w[4];
-  bw0(d, w);
-  return (j == 0) ? w[0] : (j == 1) ? w[1] : (j == 2) ? w[2] : w[3];
-}
 
 // Object-side element: complex (complex64 objects) or real (float32 objects)
 template <class T>
@@ -367,6 +361,33 @@ __device__ __forceinline__ void cand_range(float m0, float C0, int i, int nhalf,
   hi = min(nmax - 1, (int)ceilf(h) + 1);
 }
 
+// cand_range with the reciprocal rm0 = 1 / m0 computed once (0 when
+// |m0| <= 1e-3: every index is a candidate).  The quotient moves by an ulp at
+// most, well inside the one-index margin on either side.
+__device__ __forceinline__ float cand_rm0(float m0) { return (fabsf(m0) > 1e-3f) ? 1.0f / m0 : 0.f; }
+__device__ __forceinline__ void cand_range_r(float rm0, float C0, int i, int nhalf, int nmax, int& lo, int& hi) {
+  if (rm0 == 0.f) {
+    lo = 0;
+    hi = nmax - 1;
+    return;
+  }
+  const float a = ((float)(i - 2) - C0) * rm0 + (float)nhalf;
+  const float b = ((float)(i + 2) - C0) * rm0 + (float)nhalf;
+  const float l = fminf(fmaxf(fminf(a, b), -1e7f), 1e7f);
+  const float h = fminf(fmaxf(fmaxf(a, b), -1e7f), 1e7f);
+  lo = max(0, (int)floorf(l) - 1);
+  hi = min(nmax - 1, (int)ceilf(h) + 1);
+}
+
+// The adjoint's horizontal gather reads, per detector pixel, the first object
+// column of its stencil (int) and its four tap weights (float): 20 bytes, kept
+// where the vertically reduced rows were once those are consumed.  Elements of
+// T per detector row of that shared area:
+constexpr int kAdjTabBytes = 20;
+__host__ __device__ constexpr int adj_line_elems(int nobj, int n, int elem) {
+  return (3 * nobj * elem >= kAdjTabBytes * n) ? 3 * nobj : (kAdjTabBytes * n + elem - 1) / elem;
+}
+
 // ============================================== adjoint row pass
 // tmp holds the column-processed spectrum of g0.  G = DCT-III; recompute
 // x12; P = G conj(x12) -> cache; Y22 = -i conj(prb) P; per-image sums
@@ -384,7 +405,8 @@ k_casc_adj(const float2* __restrict__ tmp, float2* __restrict__ Pc, T* __restric
   extern __shared__ float2 smem[];
   double* red = reinterpret_cast<double*>(reinterpret_cast<char*>(smem) + CF::FFT_BYTES);
   const int line = threadIdx.x / TT, t = threadIdx.x % TT;
-  T* V = reinterpret_cast<T*>(red + red_doubles<TT>(5, CF::THREADS)) + (long)line * 3 * D.nobj;
+  T* V = reinterpret_cast<T*>(red + red_doubles<TT>(5, CF::THREADS)) +
+         (long)line * adj_line_elems(D.nobj, N, (int)sizeof(T));
   const long row = (long)blockIdx.x * CF::LINES + line;
   const bool valid = row < D.nimg * D.nz;
   const long img = valid ? row / D.nz : 0;
@@ -441,22 +463,35 @@ k_casc_adj(const float2* __restrict__ tmp, float2* __restrict__ Pc, T* __restric
     for (int i = 0; i < 5; ++i) atomicAdd(&acc_img[img * kNAcc + kAx + i], v[i]);
   }
   __syncthreads();
+  // Y22 into the FFT line; per detector pixel its stencil's first column + 1
+  // and tap weights into the gather tables (over V, which is consumed)
+  int* tcol = reinterpret_cast<int*>(V);
+  float* twt = reinterpret_cast<float*>(tcol + N);
 #pragma unroll
-  for (int i = 0; i < E; ++i) sm.st(t + i * TT, Yr[i]);
+  for (int i = 0; i < E; ++i) {
+    const int tx = t + i * TT;
+    sm.st(tx, Yr[i]);
+    const float x = sample_x(D, m0, r.y, tx);
+    const int ixw = (int)floorf(x);
+    float w[4];
+    bw0(x - (float)ixw, w);
+    tcol[tx] = ixw - 1;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) twt[j * N + tx] = w[j];
+  }
   __syncthreads();
   if (!valid) return;
   const float C0 = -r.y + (m0 - 1.0f) / 2.0f + (float)(D.nobj / 2);
+  const float rm0 = cand_rm0(m0);
   T* hrow = hbuf + row * (long)D.nobj;
   for (int ix = t; ix < D.nobj; ix += TT) {
     int lo, hi;
-    cand_range(m0, C0, ix, D.n / 2, D.n, lo, hi);
+    cand_range_r(rm0, C0, ix, D.n / 2, D.n, lo, hi);
     T acc = El<T>::zero();
     for (int tx = lo; tx <= hi; ++tx) {
-      const float x = sample_x(D, m0, r.y, tx);
-      const int ixw = (int)floorf(x);
-      const int j = ix - ixw + 1;
-      if (j < 0 || j > 3) continue;
-      El<T>::fma(acc, bw0_tap(x - (float)ixw, j), El<T>::from_sm(sm.ld(tx)));
+      const int j = ix - tcol[tx];  // tap of pixel tx that lands on column ix
+      if ((unsigned)j > 3u) continue;
+      El<T>::fma(acc, twt[j * N + tx], El<T>::from_sm(sm.ld(tx)));
     }
     hrow[ix] = acc;
   }
@@ -917,8 +952,13 @@ static cudaError_t grad_impl(ht_rec_s* r, const void* c, const float* pos, const
   if ((e = dct_cols(r->D.nz, true, r->tmp, r->D.nimg, N, hw, r->D.ndist, twz, st)) != cudaSuccess) return e;
   using CA = StCfg<N, 3, 1>;
   const long nrows = r->D.nimg * r->D.nz;
-  int smem = 0;
-  if ((e = stencil_smem<CA>(nullptr, 5, r->D.nobj, (int)sizeof(T), &smem)) != cudaSuccess) return e;
+  const int smem = CA::FFT_BYTES + red_doubles<CA::TR>(5, CA::THREADS) * (int)sizeof(double) +
+                   CA::LINES * adj_line_elems(r->D.nobj, N, (int)sizeof(T)) * (int)sizeof(T);
+  if (smem > 227 * 1024) {
+    set_error("fused cascade: nobj = " + std::to_string(r->D.nobj) + " needs " + std::to_string(smem) +
+              " bytes of shared memory per block (limit 227 KB)");
+    return cudaErrorInvalidValue;
+  }
   if ((e = allow_smem(k_casc_adj<N, T>, smem)) != cudaSuccess) return e;
   T* hbuf = reinterpret_cast<T*>(r->tmp + nrows * N);
   {
