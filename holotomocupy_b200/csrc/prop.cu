@@ -150,6 +150,111 @@ k_dct_cols(float2* data, int n, const float2* __restrict__ Hall, int ntab, const
   fft_line_to<NZ, false>(sm, ColOut<NZ>{img, n, valid}, t, tw4);
 }
 
+// ------------------- column pass at NZ = 512: the combine in registers
+// One group of 32 threads per column, 16 samples a thread, radices 8, 8, 8.
+// In the last stage of the DCT-II FFT and the first stage of the DCT-III FFT
+// thread t owns the butterflies t and 64 - t (thread 0: 0 and 32), whose
+// samples k = b + 64 j are closed under k -> 512 - k.  The k / N-k combine,
+// the table product and the DCT-III pre-combine of both samples of a pair
+// then happen in registers, so the spectrum makes no round trip through
+// shared memory between the two transforms.
+struct Col512 {
+  static constexpr int N = 512, E = 16, T = 32, C = 8, THREADS = C * T;
+  static constexpr int SMEM = N * C * (int)sizeof(float2);
+};
+
+// DCT-II output pair (X[k], X[N-k]) -> x Hw -> DCT-III input pair, 0 < k < N/2
+// (the general case of the combine in k_dct_cols).
+template <bool CONJ>
+__device__ __forceinline__ void col_combine(float2& lo, float2& hi, int k, const float2* __restrict__ H, int n,
+                                            const float2* __restrict__ tw4) {
+  const float2 w = __ldg(&tw4[k]);
+  const float2 P = cmul(w, lo), Q = cmulc(hi, w);
+  float2 hk = __ldg(&H[(long)k * n]), hn = __ldg(&H[(long)(512 - k) * n]);
+  if (CONJ) {
+    hk.y = -hk.y;
+    hn.y = -hn.y;
+  }
+  const float2 Gk = cmul(cscale(cadd(P, Q), 0.5f), hk);
+  const float2 Gn = cmul(cscale(cmul_i(csub(P, Q)), 0.5f), hn);
+  lo = cscale(cmul(w, cadd(Gk, cmul_i(Gn))), 0.5f);
+  hi = cscale(cmulc(csub(Gk, cmul_i(Gn)), w), 0.5f);
+}
+
+template <bool CONJ>
+__global__ void __launch_bounds__(Col512::THREADS)
+k_dct_cols512(float2* data, int n, const float2* __restrict__ Hall, int ntab, const float2* __restrict__ tw4) {
+  constexpr int N = 512, E = Col512::E, C = Col512::C;
+  const float2* __restrict__ H0 = Hall + (long)(blockIdx.y % ntab) * N * n;
+  extern __shared__ float2 tile[];
+  const int c = threadIdx.x % C, t = threadIdx.x / C;
+  const bool valid = blockIdx.x * C + c < n;
+  const int col = min((int)blockIdx.x * C + c, n - 1);
+  const float2* __restrict__ H = H0 + col;
+  float2* img = data + (long)blockIdx.y * N * n + col;
+  SmCol<C> sm{tile + c};
+  const CtaSync sync{};
+  float2 v[E];
+  // DCT-II FFT: stages 1 (from global memory) and 2
+  fft_stage<N, E, 8, 1, false, false, true>(v, SplitView<ColIn<N>, SmCol<C>>{ColIn<N>{img, n, valid}, sm}, t, tw4,
+                                            sync);
+  fft_stage<N, E, 8, 8, false, true, true>(v, sm, t, tw4, sync);
+  // stage 3 (P = 64) for the butterflies b0, b1, kept in registers: v[8 s + j] = X[b_s + 64 j]
+  const int b0 = t, b1 = (t == 0) ? 32 : 64 - t;
+#pragma unroll
+  for (int s = 0; s < 2; ++s) {
+    const int b = s ? b1 : b0;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) v[8 * s + j] = sm.ld(b + 64 * j);
+    float2 w[8];
+    twiddles<8, false>(tw4, b, N, w);
+#pragma unroll
+    for (int j = 1; j < 8; ++j) v[8 * s + j] = cmul(v[8 * s + j], w[j]);
+    Dft<8, false>::run(&v[8 * s]);
+  }
+  // combine, x Hw, pre-combine
+  if (t != 0) {
+    // pairs (b0 + 64 j, b1 + 64 (7 - j)); the first is the lower index for j < 4
+#pragma unroll
+    for (int j = 0; j < 4; ++j) col_combine<CONJ>(v[j], v[15 - j], t + 64 * j, H, n, tw4);
+#pragma unroll
+    for (int j = 4; j < 8; ++j) col_combine<CONJ>(v[15 - j], v[j], 64 - t + 64 * (7 - j), H, n, tw4);
+  } else {
+    // b0 = 0: 64 j pairs with 64 (8 - j); 0 and 256 pair with themselves
+    {
+      float2 h = __ldg(&H[0]);
+      if (CONJ) h.y = -h.y;
+      const float2 w = __ldg(&tw4[0]);
+      v[0] = cmul(cscale(cadd(cmul(w, v[0]), cmulc(v[0], w)), 0.5f), h);
+    }
+    {
+      float2 h = __ldg(&H[(long)256 * n]);
+      if (CONJ) h.y = -h.y;
+      const float2 w = __ldg(&tw4[256]);
+      const float2 G = cmul(cscale(cadd(cmul(w, v[4]), cmulc(v[4], w)), 0.5f), h);
+      v[4] = cscale(cmul(w, cadd(G, cmul_i(G))), 0.5f);
+    }
+#pragma unroll
+    for (int j = 1; j < 4; ++j) col_combine<CONJ>(v[j], v[8 - j], 64 * j, H, n, tw4);
+    // b1 = 32: 32 + 64 j pairs with 32 + 64 (7 - j)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) col_combine<CONJ>(v[8 + j], v[15 - j], 32 + 64 * j, H, n, tw4);
+  }
+  sync();  // every stage-3 load is done before the stores below
+  // DCT-III FFT: stage 1 (P = 1) on the same butterflies, then stages 2 and 3 (to global memory)
+#pragma unroll
+  for (int s = 0; s < 2; ++s) {
+    const int b = s ? b1 : b0;
+    Dft<8, false>::run(&v[8 * s]);
+#pragma unroll
+    for (int j = 0; j < 8; ++j) sm.st(b * 8 + j, v[8 * s + j]);
+  }
+  sync();
+  fft_stage<N, E, 8, 8, false, true, true>(v, sm, t, tw4, sync);
+  fft_stage<N, E, 8, 64, false, false, false>(v, SplitView<SmCol<C>, ColOut<N>>{sm, ColOut<N>{img, n, valid}}, t,
+                                              tw4, sync);
+}
+
 // ---------------------------------------------------------------- launch
 template <int N>
 static cudaError_t launch_dct_rows(bool inverse, const float2* in, float2* out, long nrows,
@@ -171,6 +276,19 @@ static cudaError_t launch_dct_rows(bool inverse, const float2* in, float2* out, 
 template <int NZ>
 static cudaError_t launch_dct_cols(bool conj, float2* data, long nimg, int n, const float2* H, int ntab,
                                    const float2* tw4, cudaStream_t st) {
+  if constexpr (NZ == 512) {
+    using CF = Col512;
+    dim3 grid((n + CF::C - 1) / CF::C, (unsigned)nimg);
+    auto kern = conj ? k_dct_cols512<true> : k_dct_cols512<false>;
+    cudaError_t e = allow_smem(kern, CF::SMEM);
+    if (e != cudaSuccess) return e;
+    {
+      KTimer kt("k_dct_cols", st, (double)nimg);
+      kern<<<grid, CF::THREADS, CF::SMEM, st>>>(data, n, H, ntab, tw4);
+    }
+    ::ht::count_launch();
+    return cudaGetLastError();
+  }
   using CF = ColCfg<NZ>;
   dim3 grid((n + CF::C - 1) / CF::C, (unsigned)nimg);
   if (conj) {
