@@ -305,6 +305,10 @@ k_casc_resid(float2* __restrict__ tmp, float2* __restrict__ x0c, const float* __
   const long row = (long)blockIdx.x * RowCfg<N>::LINES + line;
   const bool valid = row < D.nimg * D.nz;
   SmRow sm{smem + line * SmRow::padded(N)};
+  // the data row is loaded before the transform, so its latency overlaps it
+  float dv[E];
+#pragma unroll
+  for (int i = 0; i < E; ++i) dv[i] = (MODE != 2 && valid) ? data[row * N + t + i * TT] : 0.f;
   dct3_start<N, TT>(sm, t, tw4, tmp + row * N, valid);
   float2 g0[E];
   double acc[1] = {0.0};
@@ -319,7 +323,7 @@ k_casc_resid(float2* __restrict__ tmp, float2* __restrict__ x0c, const float* __
       if (MODE == 2) {
         amp[row * N + tx] = a;
       } else {
-        const float d = data[row * N + tx];
+        const float d = dv[i];
         const float e = a - d;
         facc += e * e;
         if (MODE == 0) {
@@ -717,7 +721,7 @@ k_casc_hess_fwd(const T* __restrict__ c, const float* __restrict__ pos, const fl
 // ======================================== Hessian quadratic terms
 // y0_d = DCT-III rows of tmp[d];  Q pairs with x0 and the data.
 template <int N, int NDIR>
-__global__ void __launch_bounds__(RowCfg<N>::THREADS, 4)
+__global__ void __launch_bounds__(RowCfg<N>::THREADS, 3)
 k_casc_hess_q(const float2* __restrict__ tmp, const float2* __restrict__ x0c, const float* __restrict__ data,
               double* __restrict__ glob, CascDims D, const float2* __restrict__ tw4) {
   constexpr int TT = RowCfg<N>::T;
@@ -730,10 +734,13 @@ k_casc_hess_q(const float2* __restrict__ tmp, const float2* __restrict__ x0c, co
   const long nrow = D.nimg * D.nz;
   SmRow sm0{smem + line * SmRow::padded(N)};
   SmRow sm1{smem + (LINES + line) * SmRow::padded(N)};
+  constexpr int E = Plan<N>::E;
   dct3_start<N, TT>(sm0, t, tw4, tmp + row * N, valid);
   if (NDIR == 2) dct3_start<N, TT>(sm1, t, tw4, tmp + (nrow + row) * N, valid);
   float s[3] = {0.f, 0.f, 0.f};
-  for (int tx = t; tx < N; tx += TT) {
+#pragma unroll
+  for (int i = 0; i < E; ++i) {
+    const int tx = t + i * TT;
     if (!valid) break;
     const float2 x0 = x0c[row * N + tx];
     const float d = data[row * N + tx];

@@ -42,16 +42,27 @@ __device__ __forceinline__ void dct2_finish(const SmRow& sm, int t, const float2
 template <int N, int T>
 __device__ __forceinline__ void dct3_start(const SmRow& sm, int t, const float2* __restrict__ tw4, const float2* src,
                                            bool valid) {
-  for (int m = t; m <= N / 2; m += T) {
-    const float2 z = make_float2(0.f, 0.f);
-    const float2 G = valid ? src[m] : z;
-    const float2 H = valid ? src[m == 0 ? 0 : N - m] : z;
+  // every load of the line is issued before the first store, so the thread
+  // waits for global memory once
+  constexpr int NM = (N / 2) / T + 1;  // m = t + i T covers 0..N/2
+  float2 G[NM], H[NM];
+#pragma unroll
+  for (int i = 0; i < NM; ++i) {
+    const int m = t + i * T;
+    const bool ok = valid && m <= N / 2;
+    G[i] = ok ? src[m] : make_float2(0.f, 0.f);
+    H[i] = ok ? src[m == 0 ? 0 : N - m] : make_float2(0.f, 0.f);
+  }
+#pragma unroll
+  for (int i = 0; i < NM; ++i) {
+    const int m = t + i * T;
+    if (m > N / 2) break;
     if (m == 0) {
-      sm.st(0, G);
+      sm.st(0, G[i]);
     } else {
       const float2 w = __ldg(&tw4[m]);
-      sm.st(m, cscale(cmul(w, cadd(G, cmul_i(H))), 0.5f));
-      if (m != N / 2) sm.st(N - m, cscale(cmulc(csub(G, cmul_i(H)), w), 0.5f));
+      sm.st(m, cscale(cmul(w, cadd(G[i], cmul_i(H[i]))), 0.5f));
+      if (m != N / 2) sm.st(N - m, cscale(cmulc(csub(G[i], cmul_i(H[i])), w), 0.5f));
     }
   }
   line_sync<T>()();

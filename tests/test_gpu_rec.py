@@ -174,14 +174,14 @@ def test_taylor_orders():
     assert 3.0 < e2[0] / e2[1] < 5.0 and 6.0 < e3[0] / e3[1] < 10.0
 
 
-def test_cascade_at_large_magnifications_matches_oracle():
-    """Magnifications from 0 to 3.5: above about 2.7 a detector-row chunk of
-    the Hessian pass reaches more object columns than its staging rows hold
-    and the block takes the direct path.  Gradient and Hessian forms against
-    the FP64 oracle (rel <= 1e-4)."""
+@pytest.mark.parametrize("n", [64, 512])
+def test_cascade_at_large_magnifications_matches_oracle(n):
+    """Magnifications from 0 to 3.5, detector and object n = 64 and 512 (the
+    512-row transforms have their own kernels).  Gradient and Hessian forms
+    against the FP64 oracle (rel <= 1e-4)."""
     from oracle import holo_oracle as O
     from holotomocupy_b200.rec import Rec
-    n, ntheta, ndist = 64, 3, 2
+    ntheta, ndist = 3, 2
     args = rec_args(n, ntheta, ndist, n)
     rec = Rec(args)
     orc = O.Rec(args, "complex128")
