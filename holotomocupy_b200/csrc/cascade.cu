@@ -247,6 +247,10 @@ __device__ __forceinline__ void vrow4(const T* __restrict__ V, const int (&xx)[4
 enum Acc : int { kAx = 0, kAy, kHxx, kHxy, kHyy, kAyx, kAyy, kAzx, kAzy, kNAcc };
 // Global accumulator slots
 enum Glob : int { kF = 0, kQ0, kQ1, kQ2, kL10, kL11, kL12, kL20, kL21, kL22, kNGlob };
+// Per-row sum slots the row kernels write (see k_rows_img)
+constexpr int kHessRowK = 10;  // the Hessian row pass's slots
+constexpr int kRowKMax = 10;
+constexpr int kRedThreads = 256;
 
 // ================================================= forward row pass
 // u = prb[k] exp(i S(c)) -> row DCT-II -> tmp
@@ -295,8 +299,8 @@ k_casc_fwd(const T* __restrict__ c, const float* __restrict__ pos, const float* 
 template <int N, int MODE>
 __global__ void __launch_bounds__(RowCfg<N>::THREADS, 4)
 k_casc_resid(float2* __restrict__ tmp, float2* __restrict__ x0c, const float* __restrict__ data,
-             float* __restrict__ amp, double* __restrict__ glob, float scale, CascDims D,
-             const float2* __restrict__ tw4) {
+             float* __restrict__ amp, double* __restrict__ glob, double* __restrict__ rows, float scale,
+             CascDims D, const float2* __restrict__ tw4) {
   constexpr int TT = RowCfg<N>::T;
   constexpr int E = Plan<N>::E;
   extern __shared__ float2 smem[];
@@ -338,7 +342,12 @@ k_casc_resid(float2* __restrict__ tmp, float2* __restrict__ x0c, const float* __
   if (MODE != 2) {
     acc[0] = facc;
     line_sums<TT, 1>(acc, red, line, t);
-    if (t == 0 && valid) atomicAdd(&glob[kF], acc[0]);
+    if (t == 0 && valid) {
+      if (rows)
+        rows[row] = acc[0];  // summed by k_rows_img / k_imgs_glob
+      else
+        atomicAdd(&glob[kF], acc[0]);
+    }
   }
   if (MODE != 0) return;
   __syncthreads();
@@ -402,7 +411,7 @@ template <int N, class T>
 __global__ void __launch_bounds__(StCfg<N, 3, 1>::THREADS)
 k_casc_adj(const float2* __restrict__ tmp, float2* __restrict__ Pc, T* __restrict__ hbuf, const T* __restrict__ c,
            const float* __restrict__ pos, const float* __restrict__ mag, const float2* __restrict__ prb,
-           double* __restrict__ acc_img, CascDims D, const float2* __restrict__ tw4) {
+           double* __restrict__ rows, CascDims D, const float2* __restrict__ tw4) {
   using CF = StCfg<N, 3, 1>;
   constexpr int TT = CF::T;
   constexpr int E = Plan<N>::E;
@@ -464,7 +473,7 @@ k_casc_adj(const float2* __restrict__ tmp, float2* __restrict__ Pc, T* __restric
   line_sums<TT, 5>(v, red, line, t);  // contains barriers: G is no longer read
   if (t == 0 && valid) {
 #pragma unroll
-    for (int i = 0; i < 5; ++i) atomicAdd(&acc_img[img * kNAcc + kAx + i], v[i]);
+    for (int i = 0; i < 5; ++i) rows[row * 5 + i] = v[i];  // per-image sums: k_rows_img
   }
   __syncthreads();
   // Y22 into the FFT line; per detector pixel its stencil's first column + 1
@@ -586,7 +595,7 @@ k_casc_hess_fwd(const T* __restrict__ c, const float* __restrict__ pos, const fl
                 const float2* __restrict__ prb, const float2* __restrict__ Pc, const T* __restrict__ c0,
                 const float* __restrict__ pos0, const float2* __restrict__ prb0, const T* __restrict__ c1,
                 const float* __restrict__ pos1, const float2* __restrict__ prb1, float2* __restrict__ tmp,
-                double* __restrict__ acc_img, double* __restrict__ glob, CascDims D,
+                double* __restrict__ rows, CascDims D,
                 const float2* __restrict__ tw4) {
   constexpr int NS = 2 * (1 + NDIR);
   using CF = StCfg<N, NS, NDIR>;
@@ -692,23 +701,19 @@ k_casc_hess_fwd(const T* __restrict__ c, const float* __restrict__ pos, const fl
     v[3] = s[7];
   }
   line_sums<TT, K>(v, red, line, t);
+  // per-row sums in the slots L1 00,01,11, L2 00,01,11, Ayx, Ayy, Azx, Azy
+  // (reduced by k_rows_img / k_imgs_glob)
   if (t == 0 && valid) {
+    double* rw = rows + row * kHessRowK;
     if (NDIR == 2) {
-      atomicAdd(&glob[kL10], v[0]);
-      atomicAdd(&glob[kL20], v[3]);
-      atomicAdd(&acc_img[img * kNAcc + kAyx], v[6]);
-      atomicAdd(&acc_img[img * kNAcc + kAyy], v[7]);
-      atomicAdd(&glob[kL11], v[1]);
-      atomicAdd(&glob[kL12], v[2]);
-      atomicAdd(&glob[kL21], v[4]);
-      atomicAdd(&glob[kL22], v[5]);
-      atomicAdd(&acc_img[img * kNAcc + kAzx], v[8]);
-      atomicAdd(&acc_img[img * kNAcc + kAzy], v[9]);
+#pragma unroll
+      for (int i = 0; i < K; ++i) rw[i] = v[i];
     } else {
-      atomicAdd(&glob[kL10], v[0]);
-      atomicAdd(&glob[kL20], v[1]);
-      atomicAdd(&acc_img[img * kNAcc + kAyx], v[2]);
-      atomicAdd(&acc_img[img * kNAcc + kAyy], v[3]);
+      rw[0] = v[0];
+      rw[3] = v[1];
+      rw[6] = v[2];
+      rw[7] = v[3];
+      rw[1] = rw[2] = rw[4] = rw[5] = rw[8] = rw[9] = 0.0;
     }
   }
   __syncthreads();
@@ -723,7 +728,7 @@ k_casc_hess_fwd(const T* __restrict__ c, const float* __restrict__ pos, const fl
 template <int N, int NDIR>
 __global__ void __launch_bounds__(RowCfg<N>::THREADS, 3)
 k_casc_hess_q(const float2* __restrict__ tmp, const float2* __restrict__ x0c, const float* __restrict__ data,
-              double* __restrict__ glob, CascDims D, const float2* __restrict__ tw4) {
+              double* __restrict__ rows, CascDims D, const float2* __restrict__ tw4) {
   constexpr int TT = RowCfg<N>::T;
   constexpr int LINES = RowCfg<N>::LINES;
   extern __shared__ float2 smem[];
@@ -760,11 +765,65 @@ k_casc_hess_q(const float2* __restrict__ tmp, const float2* __restrict__ x0c, co
   double v[3] = {s[0], s[1], s[2]};
   line_sums<TT, 3>(v, red, line, t);
   if (t == 0 && valid) {
-    atomicAdd(&glob[kQ0], v[0]);
-    if (NDIR == 2) {
-      atomicAdd(&glob[kQ1], v[1]);
-      atomicAdd(&glob[kQ2], v[2]);
-    }
+#pragma unroll
+    for (int i = 0; i < 3; ++i) rows[row * 3 + i] = v[i];  // Q0, Q1, Q2: k_rows_img / k_imgs_glob
+  }
+}
+
+// ============================================ row sums -> image / total sums
+// The row kernels write each detector row's sums (FP64, reduced over the
+// row's threads) to rows [nimg * nz][K]; these two kernels add them up in a
+// fixed order, so the sums do not depend on scheduling and no two rows
+// contend for one accumulator.
+
+// imgs[img][i] = sum over the image's nz rows of rows[.][i] (one block per
+// image); the slots i0 .. i0 + na - 1 are also added to acc_img[img][a0 + .].
+__global__ void __launch_bounds__(kRedThreads)
+k_rows_img(const double* __restrict__ rows, int K, int nz, double* __restrict__ imgs, double* __restrict__ acc_img,
+           int a0, int i0, int na) {
+  const long img = blockIdx.x;
+  __shared__ double red[kRowKMax][kRedThreads / 32];
+  double s[kRowKMax];
+#pragma unroll
+  for (int i = 0; i < kRowKMax; ++i) s[i] = 0.0;
+  for (int ty = threadIdx.x; ty < nz; ty += kRedThreads) {
+    const double* rw = rows + (img * nz + ty) * K;
+#pragma unroll
+    for (int i = 0; i < kRowKMax; ++i)
+      if (i < K) s[i] += rw[i];
+  }
+#pragma unroll
+  for (int i = 0; i < kRowKMax; ++i) {
+    if (i >= K) break;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s[i] += __shfl_down_sync(0xffffffffu, s[i], o);
+    if ((threadIdx.x & 31) == 0) red[i][threadIdx.x / 32] = s[i];
+  }
+  __syncthreads();
+  if (threadIdx.x < K) {
+    const int i = threadIdx.x;
+    double tot = 0.0;
+    for (int w = 0; w < kRedThreads / 32; ++w) tot += red[i][w];
+    imgs[img * K + i] = tot;
+    if (i >= i0 && i < i0 + na) acc_img[img * kNAcc + a0 + (i - i0)] += tot;
+  }
+}
+
+// glob[g0 + i] += sum over images of imgs[img][i]  (block i)
+__global__ void __launch_bounds__(kRedThreads)
+k_imgs_glob(const double* __restrict__ imgs, int K, long nimg, double* __restrict__ glob, int g0) {
+  const int i = blockIdx.x;
+  __shared__ double red[kRedThreads / 32];
+  double s = 0.0;
+  for (long img = threadIdx.x; img < nimg; img += kRedThreads) s += imgs[img * K + i];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x / 32] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double tot = 0.0;
+    for (int w = 0; w < kRedThreads / 32; ++w) tot += red[w];
+    glob[g0 + i] += tot;
   }
 }
 
@@ -831,6 +890,8 @@ struct ht_rec_s {
   float2* tmp;     // [2, nimg, nz, n]
   double* acc_img; // [nimg, kNAcc]
   double* glob;    // [kNGlob]
+  double* rows;    // [nimg * nz, kRowKMax] per-row sums of the row kernels
+  double* imgs;    // [nimg, kRowKMax] their per-image sums
 };
 
 extern "C" int ht_rec_create(int n, int nz, int nobj, int nzobj, int ntheta, int ndist, int is_complex,
@@ -864,6 +925,8 @@ extern "C" int ht_rec_create(int n, int nz, int nobj, int nzobj, int ntheta, int
   if (e == cudaSuccess) e = cudaMalloc(&r->tmp, sizeof(float2) * (img + std::max(img, hrow)));
   if (e == cudaSuccess) e = cudaMalloc(&r->acc_img, sizeof(double) * (size_t)ntheta * ndist * kNAcc);
   if (e == cudaSuccess) e = cudaMalloc(&r->glob, sizeof(double) * kNGlob);
+  if (e == cudaSuccess) e = cudaMalloc(&r->rows, sizeof(double) * (size_t)ntheta * ndist * nz * kRowKMax);
+  if (e == cudaSuccess) e = cudaMalloc(&r->imgs, sizeof(double) * (size_t)ntheta * ndist * kRowKMax);
   if (e != cudaSuccess) {
     set_error(std::string("ht_rec_create: ") + cudaGetErrorString(e));
     cudaFree(r->x0);
@@ -871,6 +934,8 @@ extern "C" int ht_rec_create(int n, int nz, int nobj, int nzobj, int ntheta, int
     cudaFree(r->tmp);
     cudaFree(r->acc_img);
     cudaFree(r->glob);
+    cudaFree(r->rows);
+    cudaFree(r->imgs);
     delete r;
     return kCudaError;
   }
@@ -885,6 +950,8 @@ extern "C" int ht_rec_destroy(ht_rec_s* r) {
   cudaFree(r->tmp);
   cudaFree(r->acc_img);
   cudaFree(r->glob);
+  cudaFree(r->rows);
+  cudaFree(r->imgs);
   delete r;
   return ht::kOk;
 }
@@ -903,6 +970,19 @@ static cudaError_t stencil_smem(const void* kernel, int K, int nobj, int elem, i
     return cudaErrorInvalidValue;
   }
   return cudaSuccess;
+}
+
+// Sum the per-row values a row kernel left in r->rows (K a row): per image
+// into r->imgs (slots i0.. i0+na-1 also into acc_img[.][a0..]), and slots
+// 0..ng-1 over all images into glob[g0..].
+static cudaError_t reduce_rows(ht_rec_s* r, int K, int a0, int i0, int na, int g0, int ng, cudaStream_t st) {
+  k_rows_img<<<(unsigned)r->D.nimg, kRedThreads, 0, st>>>(r->rows, K, r->D.nz, r->imgs, r->acc_img, a0, i0, na);
+  ::ht::count_launch();
+  if (ng > 0) {
+    k_imgs_glob<<<(unsigned)ng, kRedThreads, 0, st>>>(r->imgs, K, r->D.nimg, r->glob, g0);
+    ::ht::count_launch();
+  }
+  return cudaGetLastError();
 }
 
 template <int N, class T>
@@ -941,11 +1021,12 @@ static cudaError_t resid_pass(ht_rec_s* r, const float* data, float* amp, float 
   const long nrows = r->D.nimg * r->D.nz;
   {
     KTimer kt(MODE == 0 ? "k_casc_resid" : "k_casc_resid_f", st, (double)r->D.nimg);
-    k_casc_resid<N, MODE><<<HT_ROWS_GRID(N, nrows), CF::THREADS, smem, st>>>(r->tmp, r->x0, data, amp, r->glob,
-                                                                             scale, r->D, twn);
+    k_casc_resid<N, MODE><<<HT_ROWS_GRID(N, nrows), CF::THREADS, smem, st>>>(
+        r->tmp, r->x0, data, amp, r->glob, MODE == 2 ? nullptr : r->rows, scale, r->D, twn);
   }
   ::ht::count_launch();
-  return cudaGetLastError();
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  return MODE == 2 ? cudaSuccess : reduce_rows(r, 1, 0, 0, 0, kF, 1, st);
 }
 
 template <int N, class T>
@@ -971,10 +1052,11 @@ static cudaError_t grad_impl(ht_rec_s* r, const void* c, const float* pos, const
   {
     KTimer kt("k_casc_adj", st, (double)r->D.nimg);
     k_casc_adj<N, T><<<(unsigned)((nrows + CA::LINES - 1) / CA::LINES), CA::THREADS, smem, st>>>(
-        r->tmp, r->P, hbuf, (const T*)c, pos, mag, prb, r->acc_img, r->D, twn);
+        r->tmp, r->P, hbuf, (const T*)c, pos, mag, prb, r->rows, r->D, twn);
   }
   ::ht::count_launch();
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  if ((e = reduce_rows(r, 5, kAx, 0, 5, 0, 0, st)) != cudaSuccess) return e;
   const long npix = (long)r->D.nz * N;
   k_sum_theta<<<(unsigned)((r->D.ndist * npix + 255) / 256), 256, 0, st>>>(r->P, gprb, r->ntheta, r->D.ndist, npix); ::ht::count_launch();
   dim3 g2((r->D.nobj + 31) / 32, (r->D.nzobj + 8 * kVRows - 1) / (8 * kVRows), r->ntheta);
@@ -999,21 +1081,24 @@ static cudaError_t hess_impl(ht_rec_s* r, const void* c, const float* pos, const
   {
     KTimer kt("k_casc_hess_fwd", st, (double)NDIR * r->D.nimg);
     k_casc_hess_fwd<N, T, NDIR><<<(unsigned)((nrows + CH::LINES - 1) / CH::LINES), CH::THREADS, smem, st>>>(
-        (const T*)c, pos, mag, prb, r->P, (const T*)c0, p0, q0, (const T*)c1, p1, q1, r->tmp, r->acc_img, r->glob,
+        (const T*)c, pos, mag, prb, r->P, (const T*)c0, p0, q0, (const T*)c1, p1, q1, r->tmp, r->rows,
         r->D, twn);
   }
   ::ht::count_launch();
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  // rows slots 0-5: L1/L2 sums (glob kL10..kL22); 6-9: Ayx, Ayy, Azx, Azy (acc_img)
+  if ((e = reduce_rows(r, kHessRowK, kAyx, 6, 4, kL10, 6, st)) != cudaSuccess) return e;
   if ((e = dct_cols(r->D.nz, false, r->tmp, NDIR * r->D.nimg, N, hw, r->D.ndist, twz, st)) != cudaSuccess) return e;
   const int smq = NDIR * CF::SMEM + red_doubles<CF::T>(3, CF::THREADS) * (int)sizeof(double);
   if ((e = allow_smem(k_casc_hess_q<N, NDIR>, smq)) != cudaSuccess) return e;
   {
     KTimer kt("k_casc_hess_q", st, (double)NDIR * r->D.nimg);
-    k_casc_hess_q<N, NDIR><<<HT_ROWS_GRID(N, nrows), CF::THREADS, smq, st>>>(r->tmp, r->x0, data, r->glob, r->D,
+    k_casc_hess_q<N, NDIR><<<HT_ROWS_GRID(N, nrows), CF::THREADS, smq, st>>>(r->tmp, r->x0, data, r->rows, r->D,
                                                                              twn);
   }
   ::ht::count_launch();
-  return cudaGetLastError();
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  return reduce_rows(r, 3, 0, 0, 0, kQ0, 3, st);
 }
 
 
@@ -1166,7 +1251,7 @@ static cudaError_t noalloc_chunks(const ht_prop_s* prop, int nz, int nobj, int n
     if (e != cudaSuccess) break;
     if ((e = dct_cols(nz, false, tmp, D.nimg, N, hw, ndist, twz, st)) != cudaSuccess) break;
     k_casc_resid<N, 1><<<HT_ROWS_GRID(N, nrows), CF::THREADS, smr, st>>>(
-        tmp, nullptr, data + (long)th0 * ndist * nz * N, nullptr, acc, 0.f, D, twn);
+        tmp, nullptr, data + (long)th0 * ndist * nz * N, nullptr, acc, nullptr, 0.f, D, twn);
     count_launch();
     e = cudaGetLastError();
   }
