@@ -470,8 +470,7 @@ def served_vs_plain(nreq, niter, seed):
 # outputs written once, at their stored types; a unit is one detector image
 # for the cascade and column kernels -- one image and one direction for the
 # two Hessian kernels -- and one object slice for the Radon kernels), and the
-# DRAM bytes per unit one ncu capture measured (256^3 object, 448 angles, 4
-# distances: 1792 images, 256 slices).
+# DRAM bytes of one launch that ncu captured (below).
 KERNEL_BYTES = {
     # c read (its share per image), u's DCT-II rows written
     "k_casc_fwd": lambda r: 8 * r.nz * r.n + 8 * r.nzobj * r.nobj / r.ndist,
@@ -490,26 +489,30 @@ KERNEL_BYTES = {
     # sinogram spectra read; the 2n x 2n Fourier grid written
     "k_tcell": lambda r: 8 * r.ntheta * r.nobj + 32 * r.nobj ** 2,
 }
-# (dram__bytes_read.sum + dram__bytes_write.sum) of one captured launch and its
-# work units, at the 256^3 / 448-angle capture; traffic at other sizes is this
-# ratio to the algorithmic bytes times the algorithmic bytes there.
-_NCU_CASE = types.SimpleNamespace(n=256, nz=256, nobj=256, nzobj=256, ntheta=448, ndist=4)
+# (dram__bytes_read.sum + dram__bytes_write.sum) of one captured launch, its
+# work units and the case it ran on; traffic at other sizes is this ratio to
+# the algorithmic bytes times the algorithmic bytes there.  The Radon kernels'
+# capture keeps the benchmark's angle density (448 angles at 256, 900 at 512),
+# since k_tcell's pair lists grow with it.
+_CASE_512_96 = types.SimpleNamespace(n=512, nz=512, nobj=512, nzobj=512, ntheta=96, ndist=4)
+_CASE_256_448 = types.SimpleNamespace(n=256, nz=256, nobj=256, nzobj=256, ntheta=448, ndist=4)
 NCU_CAPTURE = {
-    "k_casc_fwd": (1.122054e9, 1792),
-    "k_casc_resid": (3.231463e9, 1792),
-    "k_casc_adj": (3.006611e9, 1792),
-    "k_casc_hess_fwd": (3.505698e9, 2 * 1792),
-    "k_dct_cols": (1.828466e9, 1792),
-    "k_tgather": (0.651061e9, 256),
-    "k_tcell": (1.994837e9, 256),   # includes the pair lists, read once per two slice batches
+    "k_casc_fwd": (1.122054e9, 1792, _CASE_256_448),
+    "k_casc_resid": (2.761909e9, 384, _CASE_512_96),
+    "k_casc_adj": (2.661818e9, 384, _CASE_512_96),
+    "k_casc_hess_fwd": (3.384108e9, 2 * 384, _CASE_512_96),
+    "k_casc_hess_q": (2.827706e9, 2 * 384, _CASE_512_96),
+    "k_dct_cols": (1.569498e9, 384, _CASE_512_96),
+    "k_tgather": (0.651061e9, 256, _CASE_256_448),
+    "k_tcell": (1.994837e9, 256, _CASE_256_448),   # includes the pair lists, read once per two slice batches
 }
 
 
 def ncu_traffic_ratio(k):
     if k not in NCU_CAPTURE:
         return None
-    b, units = NCU_CAPTURE[k]
-    return b / (KERNEL_BYTES[k](_NCU_CASE) * units)
+    b, units, case = NCU_CAPTURE[k]
+    return b / (KERNEL_BYTES[k](case) * units)
 
 
 def kernel_times(rec):
@@ -552,7 +555,8 @@ def roofline(kt):
     return {"bound": "hbm", "kernel": dom, "achieved": d["achieved"], "peak": peak, "unit": "GB/s",
             "frac": d["frac"], "traffic": d["traffic"], "peak_source": "measured" if peaks else "fallback",
             "launch_ms": d["launch_ms"],
-            "traffic_source": "ncu dram bytes / algorithmic bytes of one launch at 256^3, 448 angles, times the "
+            "traffic_source": "ncu dram bytes / algorithmic bytes of one captured launch (512^3 x 96 angles; "
+                              "256^3 x 448 angles for the Radon kernels and k_casc_fwd), times the "
                               "algorithmic bytes of this launch",
             "kernels": rows}
 
