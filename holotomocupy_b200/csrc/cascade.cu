@@ -28,6 +28,7 @@
 // Row kernels handle one detector row of one image per line, with the
 // propagator's DCT passes fused in; the column passes are the propagator's.
 #include "dct.cuh"
+#include "row512.cuh"
 #include "holotomo_b200_internal.h"
 
 #include <algorithm>
@@ -355,6 +356,115 @@ k_casc_resid(float2* __restrict__ tmp, float2* __restrict__ x0c, const float* __
   for (int i = 0; i < E; ++i) dct2_put<N>(sm, t + i * TT, g0[i]);
   __syncthreads();
   dct2_finish<N, TT>(sm, t, tw4, tmp + row * N, valid);
+}
+
+// ------------------------------------------- 512-sample rows, a warp a row
+// k_casc_resid and k_casc_hess_q at N = 512 on the warp-per-line transforms
+// of row512.cuh: the DCT-III's pixels stay in registers for the residual and
+// go on to the DCT-II from there, and the row sums are warp reductions.
+constexpr int kR512Lines = 4;  // rows (warps) per block
+
+template <int MODE>
+__global__ void __launch_bounds__(32 * kR512Lines)
+k_casc_resid512(float2* __restrict__ tmp, float2* __restrict__ x0c, const float* __restrict__ data,
+                float* __restrict__ amp, double* __restrict__ glob, double* __restrict__ rows, float scale,
+                CascDims D, const float2* __restrict__ tw4) {
+  constexpr int N = kR512;
+  __shared__ float2 smem[kR512Lines * SmRow::padded(N)];
+  const int line = threadIdx.x / 32, t = threadIdx.x % 32;
+  const long row = (long)blockIdx.x * kR512Lines + line;
+  const bool valid = row < D.nimg * D.nz;
+  SmRow sm{smem + line * SmRow::padded(N)};
+  // the data row is loaded first, so its latency overlaps the transform
+  float dv[16];
+#pragma unroll
+  for (int i = 0; i < 16; ++i) dv[i] = (MODE != 2 && valid) ? data[row * N + dct_sample_at(r512_pos(t, i), N)] : 0.f;
+  float2 v[16];
+  r512_dct3_head(v, tmp + row * N, valid, sm, t, tw4);
+  r512_finish_to_regs(v, sm, t, tw4);
+  float facc = 0.f;
+#pragma unroll
+  for (int i = 0; i < 16; ++i) {
+    const int tx = dct_sample_at(r512_pos(t, i), N);
+    const float2 x0 = v[i];
+    v[i] = make_float2(0.f, 0.f);
+    if (!valid) continue;
+    const float a = sqrtf(x0.x * x0.x + x0.y * x0.y);
+    if (MODE == 2) {
+      amp[row * N + tx] = a;
+    } else {
+      const float d = dv[i];
+      const float e = a - d;
+      facc += e * e;
+      if (MODE == 0) {
+        x0c[row * N + tx] = x0;
+        // rec_mpi.py:557-559: scale * (x - y * (x / |x|))
+        const float2 l = make_float2(x0.x / a, x0.y / a);
+        v[i] = make_float2(scale * (x0.x - d * l.x), scale * (x0.y - d * l.y));
+      }
+    }
+  }
+  if (MODE != 2) {
+    const double acc = warp_sum((double)facc);
+    if (t == 0 && valid) {
+      if (rows)
+        rows[row] = acc;
+      else
+        atomicAdd(&glob[kF], acc);
+    }
+  }
+  if (MODE != 0) return;
+  r512_dct2_tail(v, sm, t, tw4, tmp + row * N, valid);
+}
+
+template <int NDIR>
+__global__ void __launch_bounds__(32 * kR512Lines, 6)
+k_casc_hess_q512(const float2* __restrict__ tmp, const float2* __restrict__ x0c, const float* __restrict__ data,
+                 double* __restrict__ rows, CascDims D, const float2* __restrict__ tw4) {
+  constexpr int N = kR512;
+  __shared__ float2 smem[NDIR * kR512Lines * SmRow::padded(N)];
+  const int line = threadIdx.x / 32, t = threadIdx.x % 32;
+  const long row = (long)blockIdx.x * kR512Lines + line;
+  const long nrow = D.nimg * D.nz;
+  const bool valid = row < nrow;
+  SmRow sm0{smem + line * SmRow::padded(N)};
+  SmRow sm1{smem + (NDIR - 1) * kR512Lines * SmRow::padded(N) + line * SmRow::padded(N)};
+  float2 v[16];
+  r512_dct3_head(v, tmp + row * N, valid, sm0, t, tw4);
+  r512_finish_to_regs(v, sm0, t, tw4);
+  if (NDIR == 2) {
+    // direction 0's pixels go back to sm0 (each thread its own positions)
+    __syncwarp();
+#pragma unroll
+    for (int i = 0; i < 16; ++i) sm0.st(r512_pos(t, i), v[i]);
+    r512_dct3_head(v, tmp + (nrow + row) * N, valid, sm1, t, tw4);
+    r512_finish_to_regs(v, sm1, t, tw4);
+  }
+  float s[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+  for (int i = 0; i < 16; ++i) {
+    if (!valid) break;
+    const int tx = dct_sample_at(r512_pos(t, i), N);
+    const float2 x0 = x0c[row * N + tx];
+    const float d = data[row * N + tx];
+    const float a = sqrtf(x0.x * x0.x + x0.y * x0.y);
+    const float2 l0 = make_float2(x0.x / a, x0.y / a);
+    const float d0 = d / a;
+    const float2 y0 = (NDIR == 2) ? sm0.ld(r512_pos(t, i)) : v[i];
+    const float ly = l0.x * y0.x + l0.y * y0.y;  // Re(conj(l0) y0)
+    s[0] += (1.f - d0) * (y0.x * y0.x + y0.y * y0.y) + d0 * ly * ly;
+    if (NDIR == 2) {
+      const float2 y1 = v[i];
+      const float lz = l0.x * y1.x + l0.y * y1.y;
+      s[1] += (1.f - d0) * (y0.x * y1.x + y0.y * y1.y) + d0 * ly * lz;
+      s[2] += (1.f - d0) * (y1.x * y1.x + y1.y * y1.y) + d0 * lz * lz;
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    const double x = warp_sum((double)s[i]);
+    if (t == 0 && valid) rows[row * 3 + i] = x;  // Q0, Q1, Q2: k_rows_img / k_imgs_glob
+  }
 }
 
 // Detector columns [lo, hi] whose stencil can reach object index i (a
@@ -1019,7 +1129,11 @@ static cudaError_t resid_pass(ht_rec_s* r, const float* data, float* amp, float 
   cudaError_t e = allow_smem(k_casc_resid<N, MODE>, smem);
   if (e != cudaSuccess) return e;
   const long nrows = r->D.nimg * r->D.nz;
-  {
+  if constexpr (N == kR512) {
+    KTimer kt(MODE == 0 ? "k_casc_resid" : "k_casc_resid_f", st, (double)r->D.nimg);
+    k_casc_resid512<MODE><<<(unsigned)((nrows + kR512Lines - 1) / kR512Lines), 32 * kR512Lines, 0, st>>>(
+        r->tmp, r->x0, data, amp, r->glob, MODE == 2 ? nullptr : r->rows, scale, r->D, twn);
+  } else {
     KTimer kt(MODE == 0 ? "k_casc_resid" : "k_casc_resid_f", st, (double)r->D.nimg);
     k_casc_resid<N, MODE><<<HT_ROWS_GRID(N, nrows), CF::THREADS, smem, st>>>(
         r->tmp, r->x0, data, amp, r->glob, MODE == 2 ? nullptr : r->rows, scale, r->D, twn);
@@ -1091,7 +1205,11 @@ static cudaError_t hess_impl(ht_rec_s* r, const void* c, const float* pos, const
   if ((e = dct_cols(r->D.nz, false, r->tmp, NDIR * r->D.nimg, N, hw, r->D.ndist, twz, st)) != cudaSuccess) return e;
   const int smq = NDIR * CF::SMEM + red_doubles<CF::T>(3, CF::THREADS) * (int)sizeof(double);
   if ((e = allow_smem(k_casc_hess_q<N, NDIR>, smq)) != cudaSuccess) return e;
-  {
+  if constexpr (N == kR512) {
+    KTimer kt("k_casc_hess_q", st, (double)NDIR * r->D.nimg);
+    k_casc_hess_q512<NDIR><<<(unsigned)((nrows + kR512Lines - 1) / kR512Lines), 32 * kR512Lines, 0, st>>>(
+        r->tmp, r->x0, data, r->rows, r->D, twn);
+  } else {
     KTimer kt("k_casc_hess_q", st, (double)NDIR * r->D.nimg);
     k_casc_hess_q<N, NDIR><<<HT_ROWS_GRID(N, nrows), CF::THREADS, smq, st>>>(r->tmp, r->x0, data, r->rows, r->D,
                                                                              twn);

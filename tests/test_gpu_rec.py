@@ -212,6 +212,20 @@ def test_cascade_at_large_magnifications_matches_oracle(n):
     orc.gradients_cascade(o(v), ref)
     for k in ("prb", "proj", "pos"):
         assert rel_l2(out[k].cpu().numpy(), ref[k]) < 1e-4, k
+    # the forward model alone: objective (min) and amplitudes (the gen_sqrt_data form)
+    gv, ov = g(v), o(v)
+    f = rec.min(gv["prb"], None, gv["pos"], gv["proj"])
+    fo = orc.min(ov["prb"], None, ov["pos"], ov["proj"])
+    assert abs(f / fo - 1) < 1e-4, (f, fo)
+    from holotomocupy_b200 import _lib
+    c = rec._coeff_into(gv["proj"], torch.empty_like(gv["proj"]))
+    amp = torch.empty(ntheta, ndist, n, n, dtype=torch.float32, device="cuda")
+    _lib.call("ht_rec_forward", rec._h, _lib.ptr(c), _lib.ptr(gv["pos"]), _lib.ptr(rec.eff_demagnifications),
+              _lib.ptr(gv["prb"]), None, _lib.ptr(amp), None, _lib.stream_ptr())
+    y = [ov["prb"], ov["proj"], ov["pos"]]
+    for i in range(1, len(orc.F))[::-1]:
+        y = orc.F[i](y)
+    assert rel_l2(amp.cpu().numpy(), np.abs(y)) < 1e-4
 
 
 @pytest.mark.parametrize("mode", ["host", "graph"])
