@@ -32,6 +32,8 @@ SIGNATURES = {
     "ht_shift_create": [_c_int, _c_int, _c_int, _c_int, _c_int, ctypes.POINTER(_vp)],
     "ht_shift_destroy": [_vp],
     "ht_shift_coeff": [_vp, _vp, _vp, _c_long, _vp],
+    "ht_shift_filter": [_vp, _vp, _vp, _c_long, _vp, _vp, _vp],
+    "ht_shift_Sback": [_vp, _vp, _vp, _vp, ctypes.c_int, _vp, _c_long, _vp],
     "ht_shift_coeff_z": [_vp, _vp, _c_long, _vp],
     "ht_shift_S": [_vp, _vp, _vp, _vp, _vp, _c_long, _vp],
     "ht_shift_Sadj": [_vp, _vp, _vp, _vp, _vp, _c_long, _vp],

@@ -276,6 +276,54 @@ k_shift_dpos(double* __restrict__ acc, const T* __restrict__ c, const T* __restr
   }
 }
 
+// ------------------------------------------- back-projection shift
+// Sback (shift.py:138-148; cuda_kernels.py:294-370, dir = 1): every detector
+// pixel (tx, ty) of image b adds g * phi((dx - jx) / m) phi((dy - jy) / m) to
+// the coefficient cell (iy + jy, ix + jx), the B-spline stretched by the
+// image's magnification m.  The taps run over jx in [ceil(dx - 2m),
+// (int)(dx + 2m)) and likewise jy, as in the reference (whose upper bound
+// drops the last tap of non-zero weight when dx + 2m is not an integer).
+// Cells outside the grid are skipped; contributions meet in float atomics.
+__device__ __forceinline__ float sback_phi(float t, float m) {
+  t /= m;
+  const float a = fabsf(t);
+  if (t > -2.f && t <= -1.f) return (t + 2.f) * (t + 2.f) * (t + 2.f);
+  if (t > -1.f && t <= 1.f) return 4.f - 6.f * t * t + 3.f * a * t * t;
+  if (t > 1.f && t <= 2.f) return (2.f - t) * (2.f - t) * (2.f - t);
+  return 0.f;
+}
+
+__global__ void k_sback(const float2* __restrict__ g, float2* __restrict__ f, const float* __restrict__ r,
+                        const float* __restrict__ mag, int nmag, ShiftDims S, long batch) {
+  const int tx = blockIdx.x * blockDim.x + threadIdx.x;
+  const int ty = blockIdx.y * blockDim.y + threadIdx.y;
+  const long b = blockIdx.z;
+  if (tx >= S.n || ty >= S.nz || b >= batch) return;
+  const float m0 = mag[nmag == 1 ? 0 : b];
+  const float half = (m0 - 1.0f) / 2.0f;
+  const float x = (m0 * (float)(tx - S.n / 2) - r[2 * b + 1] + half) + (float)(S.npsi / 2);
+  const float y = (m0 * (float)(ty - S.nz / 2) - r[2 * b + 0] + half) + (float)(S.nzpsi / 2);
+  const int ix = (int)floorf(x), iy = (int)floorf(y);
+  const float dx = x - (float)ix, dy = y - (float)iy;
+  const float span = 2.0f * m0;
+  const float2 v = g[(b * S.nz + ty) * S.n + tx];
+  float2* fb = f + b * (long)S.nzpsi * S.npsi;
+  const int jx0 = (int)ceilf(dx - span), jx1 = (int)(dx + span);
+  for (int jy = (int)ceilf(dy - span); jy < (int)(dy + span); ++jy) {
+    const int yy = iy + jy;
+    if (yy < 0 || yy >= S.nzpsi) continue;
+    const float wy = sback_phi(dy - (float)jy, m0);
+    for (int jx = jx0; jx < jx1; ++jx) {
+      const int xx = ix + jx;
+      if (xx < 0 || xx >= S.npsi) continue;
+      const float w = sback_phi(dx - (float)jx, m0) * wy;
+      float2* cell = fb + (long)yy * S.npsi + xx;
+      atomicAdd(&cell->x, w * v.x);
+      atomicAdd(&cell->y, w * v.y);
+    }
+  }
+}
+
 // -------------------------------------------------- prefilter passes
 // data [nrows, N] in place: FFT, * sym[k], IFFT (sym carries 1/N)
 template <int N>
@@ -457,6 +505,39 @@ extern "C" int ht_shift_coeff_z(ht_shift_s* s, void* data, long ncols, void* str
   HT_REQUIRE(ncols <= 0x7fffffffL, "ht_shift_coeff_z: ncols too large");
   HT_CHECK_CUDA(symbol_cols(s->nzpsi, static_cast<float2*>(data), 1, (int)ncols, s->symy, s->tw_y,
                             static_cast<cudaStream_t>(stream)));
+  return kOk;
+}
+
+extern "C" int ht_shift_filter(ht_shift_s* s, const void* psi, void* out, long batch, const float* symx,
+                               const float* symy, void* stream) {
+  using namespace ht;
+  HT_REQUIRE(s && psi && out && symx && symy, "ht_shift_filter: null pointer");
+  if (!fft_size_supported(s->npsi) || !fft_size_supported(s->nzpsi)) {
+    set_error("ht_shift_filter: npsi and nzpsi must be supported FFT lengths");
+    return kUnsupported;
+  }
+  HT_REQUIRE(batch >= 0, "ht_shift_filter: batch must be non-negative");
+  if (batch == 0) return kOk;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  HT_CHECK_CUDA(symbol_rows(s->npsi, static_cast<const float2*>(psi), static_cast<float2*>(out), batch * s->nzpsi,
+                            symx, s->tw_x, st));
+  HT_CHECK_CUDA(symbol_cols(s->nzpsi, static_cast<float2*>(out), batch, s->npsi, symy, s->tw_y, st));
+  return kOk;
+}
+
+extern "C" int ht_shift_Sback(ht_shift_s* s, const void* g, const float* r, const float* mag, int nmag, void* out,
+                              long batch, void* stream) {
+  using namespace ht;
+  HT_REQUIRE(s && g && r && mag && out, "ht_shift_Sback: null pointer");
+  HT_REQUIRE(nmag == 1 || nmag == batch, "ht_shift_Sback: nmag must be 1 or batch");
+  HT_REQUIRE(batch >= 0 && batch <= 65535, "ht_shift_Sback: batch must be in [0, 65535]");
+  if (batch == 0) return kOk;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  HT_CHECK_CUDA(cudaMemsetAsync(out, 0, sizeof(float2) * batch * s->nzpsi * s->npsi, st));
+  k_sback<<<out_grid(s, batch), kBlock, 0, st>>>(static_cast<const float2*>(g), static_cast<float2*>(out), r, mag,
+                                                 nmag, dims(s), batch);
+  count_launch();
+  HT_CHECK_CUDA(cudaGetLastError());
   return kOk;
 }
 

@@ -3,7 +3,8 @@
 Reference: ``src/holotomocupy/shift.py:15-221``.  Same constructor
 ``Shift(n, npsi, nz, nzpsi, obj_dtype, nchunk=None)`` and methods ``phi``,
 ``coeff``, ``S``, ``Sadj``, ``curlyS``, ``curlySc``, ``dcurlySc``,
-``dcurlySadjc`` (returns ``[out1, out2]``) and ``d2curlySc``, on CUDA torch
+``dcurlySadjc`` (returns ``[out1, out2]``), ``d2curlySc`` and the Paganin
+back-projection helpers ``Sback``, ``coeffback``, ``curlySback``, on CUDA torch
 tensors.  Positions are ``[..., 0] = y``, ``[..., 1] = x`` pixel shifts and
 ``m`` the per-angle magnification, exactly as in the reference.
 """
@@ -132,6 +133,57 @@ class Shift:
         self._call("ht_shift_dSadj", self._h, _lib.ptr(c), _lib.ptr(r), _lib.ptr(m), _lib.ptr(g), _lib.ptr(out1),
                    _lib.ptr(out2), c.shape[0])
         return [out1, out2.to(out2_dtype)]
+
+    # ------------------------------------- Paganin back-projection helpers
+    def coeffback(self, psi, m):
+        """The prefilter of the B-spline stretched by the magnification m
+        (shift.py:84-96): ifft2(fft2(psi) / (B_m(y) B_m(x))) with
+        B_m = phi(0) + 2 sum_{k=1..4} phi(k / m) cos(2 pi k f).  One
+        magnification, as the reference's callers pass it (the first element
+        when m holds several)."""
+        _lib.require_cuda(psi, "psi")
+        m = float(np.asarray(m.cpu() if isinstance(m, torch.Tensor) else m, dtype=np.float64).reshape(-1)[0])
+        x = np.linspace(-1 / 2, 1 / 2 - 1 / self.npsi, self.npsi).astype("float32")
+        y = np.linspace(-1 / 2, 1 / 2 - 1 / self.nzpsi, self.nzpsi).astype("float32")
+        dx = np.float32(self.phi(0))
+        dy = np.float32(self.phi(0))
+        for k in range(1, 5):
+            pk = np.float32(self.phi(np.float32(k / m)))
+            dx = (dx + 2 * pk * np.cos(2 * np.pi * k * x)).astype("float32")
+            dy = (dy + 2 * pk * np.cos(2 * np.pi * k * y)).astype("float32")
+        # FFT order, each axis carrying its 1/N
+        symx = torch.from_numpy((1.0 / (self.npsi * np.fft.fftshift(dx).astype(np.float64))).astype("float32"))
+        symy = torch.from_numpy((1.0 / (self.nzpsi * np.fft.fftshift(dy).astype(np.float64))).astype("float32"))
+        symx, symy = symx.to(psi.device), symy.to(psi.device)
+        x = psi.to(torch.complex64).contiguous()
+        out = torch.empty_like(x)
+        b = x.numel() // (self.nzpsi * self.npsi)
+        self._call("ht_shift_filter", self._hc, _lib.ptr(x), _lib.ptr(out), b, _lib.ptr(symx), _lib.ptr(symy))
+        return out
+
+    def Sback(self, spsi, r, m):
+        """Back-projection shift (shift.py:138-148): detector images
+        [batch, nz, n] onto the coefficient grid [batch, nzpsi, npsi]
+        (complex64) with the B-spline stretched by m -- one magnification, or
+        one per image."""
+        _lib.require_cuda(spsi, "spsi")
+        if spsi.ndim != 3 or tuple(spsi.shape[1:]) != (self.nz, self.n):
+            raise ValueError(f"spsi must be [batch, {self.nz}, {self.n}], got {tuple(spsi.shape)}")
+        g = spsi.to(torch.complex64).contiguous()
+        r = _f32(r, g.device).reshape(-1)
+        m = _f32(m if isinstance(m, (torch.Tensor, np.ndarray)) else np.asarray(m, np.float32), g.device).reshape(-1)
+        if m.numel() not in (1, g.shape[0]):
+            raise ValueError(f"m must hold 1 or {g.shape[0]} magnifications, got {m.numel()}")
+        if r.numel() != 2 * g.shape[0]:
+            raise ValueError(f"r must be [{g.shape[0]}, 2]")
+        out = torch.empty(g.shape[0], self.nzpsi, self.npsi, dtype=torch.complex64, device=g.device)
+        self._call("ht_shift_Sback", self._hc, _lib.ptr(g), _lib.ptr(r), _lib.ptr(m), int(m.numel()), _lib.ptr(out),
+                   g.shape[0])
+        return out
+
+    def curlySback(self, psi, r, m):
+        """coeffback o Sback (shift.py:152-153)."""
+        return self.coeffback(self.Sback(psi, r, m), m)
 
     def d2curlySc(self, c, r, m, c1, Deltar1, c2, Deltar2):
         """Second-order term (shift.py:206-221)."""

@@ -103,6 +103,22 @@ int ht_shift_coeff(ht_shift_s* s, const void* psi, void* out, long batch, void* 
  * ncols = ny nx). */
 int ht_shift_coeff_z(ht_shift_s* s, void* data, long ncols, void* stream);
 
+/* out = ifft2(fft2(psi) * (symy (x) symx)): a separable periodic filter with
+ * caller-given device symbols symx [npsi], symy [nzpsi] in FFT order, each
+ * carrying its 1/N.  Shift.coeffback (shift.py:84-96) is this filter with
+ * the stretched B-spline's inverse symbol; complex64 [batch, nzpsi, npsi],
+ * out may alias psi. */
+int ht_shift_filter(ht_shift_s* s, const void* psi, void* out, long batch, const float* symx, const float* symy,
+                    void* stream);
+
+/* out = Sback_{r,mag}(g) (shift.py:138-148; sback, cuda_kernels.py:294-370):
+ * the back-projection of detector images g [batch, nz, n] complex64 onto the
+ * coefficient grid [batch, nzpsi, npsi] complex64 with the B-spline stretched
+ * by mag (nmag = 1: one magnification for every image; nmag = batch: one
+ * each); out is zeroed first. */
+int ht_shift_Sback(ht_shift_s* s, const void* g, const float* r, const float* mag, int nmag, void* out, long batch,
+                   void* stream);
+
 /* out = S_{r,mag}(c) (shift.py:102-111; cuda_kernels.py:161-227). */
 int ht_shift_S(ht_shift_s* s, const void* c, const float* r, const float* mag, void* out, long batch, void* stream);
 

@@ -192,6 +192,42 @@ class Shift:
         """shift.py:128-132"""
         return self.S(self.coeff(psi), r, m)
 
+    @staticmethod
+    def phi(t):
+        """shift.py:54-59 (the host-side x6 cubic B-spline)"""
+        return ((-2 < t) * (t <= -1) * (t + 2) ** 3 + (-1 < t) * (t <= 1) * (4 - 6 * t ** 2 + 3 * t ** 3 * np.sign(t))
+                + (1 < t) * (t <= 2) * (2 - t) ** 3)
+
+    def coeffback(self, psi, m):
+        """shift.py:84-96: the prefilter of the B-spline stretched by m (one
+        magnification: the first if an array is given), periodic, in the
+        Fourier domain."""
+        rdt = self.rdt
+        m = float(np.asarray(m).reshape(-1)[0])
+        x = np.linspace(-1 / 2, 1 / 2 - 1 / self.npsi, self.npsi).astype(rdt)
+        y = np.linspace(-1 / 2, 1 / 2 - 1 / self.nzpsi, self.nzpsi).astype(rdt)
+        dx = self.phi(rdt(0))
+        dy = self.phi(rdt(0))
+        for k in range(1, 5):
+            pk = self.phi(rdt(k / m))
+            dx = (dx + 2 * pk * np.cos(2 * np.pi * k * x)).astype(rdt)
+            dy = (dy + 2 * pk * np.cos(2 * np.pi * k * y)).astype(rdt)
+        ifb = (1 / np.fft.fftshift(np.outer(dy, dx), axes=(-1, -2))).astype(rdt)
+        return ifft2(fft2(psi) * ifb).astype(self.cdt)
+
+    def Sback(self, spsi, r, m):
+        """shift.py:138-148 + sback (cuda_kernels.py:294-370): [B, nz, n] ->
+        [B, nzpsi, npsi] (complex) with the B-spline stretched by m."""
+        nt = spsi.shape[0]
+        c = np.zeros((nt, self.nzpsi, self.npsi), dtype=self.cdt)
+        K.sback_kernel(np.ascontiguousarray(spsi).astype(self.cdt), c, r, m, self.n, self.npsi, self.nz,
+                       self.nzpsi, nt, 1)
+        return c
+
+    def curlySback(self, psi, r, m):
+        """shift.py:152-153"""
+        return self.coeffback(self.Sback(psi, r, m), m)
+
     def dcurlySc(self, c, r, m, c1, Deltar):
         """shift.py:170-183"""
         nt = c.shape[0]

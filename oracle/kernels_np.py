@@ -286,3 +286,46 @@ def dsadj_kernel(f, dt1, dt2, c, g, r, mag, n, npsi, nz, nzpsi, ntheta):
             np.add.at(ff, idx[valid], (w3 * g0)[valid])
     dt1.reshape(-1)[: ntheta * nz * n] = a1.reshape(-1)
     dt2.reshape(-1)[: ntheta * nz * n] = a2.reshape(-1)
+
+
+# ----------------------------------------------------------------------------
+# Back-projection shift -- cuda_kernels.py:294-370 (`sback`, Paganin init)
+# ----------------------------------------------------------------------------
+def sback_kernel(g, f, r, mag, n, npsi, nz, nzpsi, ntheta, direction):
+    """dir=1: f += Sback^T(g) with the B-spline stretched by mag, phi(t / mag),
+    over the taps jx in [ceil(dx - 2 mag), (int)(dx + 2 mag)) (the kernel's
+    bounds: the upper one drops a tap of non-zero weight when dx + 2 mag is not
+    an integer), likewise jy; dir=0: g = the matching gather.
+    g: [ntheta, nz, n], f: [ntheta, nzpsi, npsi]."""
+    rt = _real_dtype(g)
+    mg = np.asarray(mag, dtype=rt).reshape(-1)
+    mg = np.broadcast_to(mg, (ntheta,)) if mg.size == 1 else mg[:ntheta]   # one magnification for all
+    ix, iy, dx, dy = _spline_geometry(r, mg, n, npsi, nz, nzpsi, ntheta, rt)
+    gsh = g.reshape(-1)[: ntheta * nz * n].reshape(ntheta, nz, n)
+    fsh = f.reshape(-1)[: ntheta * nzpsi * npsi].reshape(ntheta, nzpsi, npsi)
+    for tz in range(ntheta):
+        m0 = mg[tz]
+        span = rt(2) * m0
+        lox = np.ceil(dx[tz] - span).astype(np.int64)
+        hix = np.trunc(dx[tz] + span).astype(np.int64)
+        loy = np.ceil(dy[tz] - span).astype(np.int64)
+        hiy = np.trunc(dy[tz] + span).astype(np.int64)
+        acc = np.zeros((nz, n), dtype=g.dtype) if direction == 0 else None
+        g0 = gsh[tz].copy() if direction != 0 else None
+        ff = fsh[tz].reshape(-1)
+        for jy in range(int(loy.min()), int(hiy.max())):
+            indy = iy[tz] + jy
+            oky = (jy >= loy) & (jy < hiy) & (indy >= 0) & (indy < nzpsi)
+            pdym = bphi(((dy[tz] - rt(jy)) / m0).astype(rt))
+            for jx in range(int(lox.min()), int(hix.max())):
+                indx = ix[tz] + jx
+                okx = (jx >= lox) & (jx < hix) & (indx >= 0) & (indx < npsi)
+                w = (bphi(((dx[tz] - rt(jx)) / m0).astype(rt))[None, :] * pdym[:, None]).astype(rt)
+                ok = oky[:, None] & okx[None, :]
+                idx = np.clip(indy, 0, nzpsi - 1)[:, None] * npsi + np.clip(indx, 0, npsi - 1)[None, :]
+                if direction == 0:
+                    acc += np.where(ok, w * ff[idx], 0)
+                else:
+                    np.add.at(ff, idx[ok], (w * g0)[ok])
+        if direction == 0:
+            gsh[tz] = acc

@@ -123,6 +123,9 @@ class _KernelStandIn:
         elif n == "dsadj":
             f, dt1, dt2, c, g, r, mag = a[:7]
             K.dsadj_kernel(f, dt1, dt2, c, g, r, mag, *[int(v) for v in a[7:]])
+        elif n == "sback":
+            g, f, r, mag = a[:4]
+            K.sback_kernel(g, f, r, mag, *[int(v) for v in a[4:]])
         else:
             raise NotImplementedError(f"kernel {n} has no stand-in")
 

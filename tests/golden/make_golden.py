@@ -107,6 +107,37 @@ def shift_cases(ns):
     np.savez_compressed(os.path.join(HERE, "shift.npz"), **out)
 
 
+def sback_cases(ns):
+    """Shift.Sback / coeffback / curlySback (shift.py:84-96, 138-153), the
+    Paganin back-projection helpers: one image and a scalar magnification as
+    the reference's callers use them (experimental/*/steps15.py), plus a
+    three-image Sback with per-image magnifications."""
+    out = {}
+    cases = [(32, 48, 24, 36, 1, 0.8, "a"), (32, 32, 32, 32, 1, 1.0, "b"), (24, 32, 24, 32, 1, 1.55, "c"),
+             (32, 36, 24, 48, 3, None, "d")]
+    for (n, npsi, nz, nzpsi, nt, m, tag) in cases:
+        rng = np.random.default_rng(700 + n + npsi + nz)
+        s = ns.shift.Shift(n, npsi, nz, nzpsi, "complex64")
+        g = crand(rng, (nt, nz, n))
+        psi = crand(rng, (nt, nzpsi, npsi))
+        r = rng.uniform(-3, 3, (nt, 2)).astype("float32")
+        C = lambda x: ns.cp.array(x)
+        key = f"sb_{tag}"
+        out.update({f"{key}_dims": np.array([n, npsi, nz, nzpsi, nt]), f"{key}_g": g, f"{key}_psi": psi,
+                    f"{key}_r": r})
+        if m is None:
+            mm = np.array([0.8, 1.0, 1.3], "float32")
+            out[f"{key}_m"] = mm
+            out[f"{key}_Sback"] = s.Sback(C(g), C(r), C(mm)).get()
+        else:
+            mm = np.array(m, "float32")        # a 0-d array, as the callers pass it
+            out[f"{key}_m"] = mm
+            out[f"{key}_Sback"] = s.Sback(C(g), C(r), C(mm)).get()
+            out[f"{key}_coeffback"] = s.coeffback(C(psi), C(mm)).get()
+            out[f"{key}_curlySback"] = s.curlySback(C(g), C(r), C(mm)).get()
+    np.savez_compressed(os.path.join(HERE, "sback.npz"), **out)
+
+
 def rec_args(n, ntheta, ndist, nobj, niter=1):
     return types.SimpleNamespace(
         energy=17.1, detector_pixelsize=1.4760147601476e-6 * 2 * 2048 / n,
@@ -257,9 +288,10 @@ def main():
     if src is None:
         raise SystemExit("usage: make_golden.py <reference src dir>")
     ns = load_reference(src)
-    which = sys.argv[2:] or ["tomo", "prop", "shift", "rec", "lap"]
+    which = sys.argv[2:] or ["tomo", "prop", "shift", "rec", "lap", "sback"]
     for w in which:
-        {"tomo": tomo_cases, "prop": prop_cases, "shift": shift_cases, "rec": rec_cases, "lap": lap_cases}[w](ns)
+        {"tomo": tomo_cases, "prop": prop_cases, "shift": shift_cases, "rec": rec_cases, "lap": lap_cases,
+         "sback": sback_cases}[w](ns)
         print("wrote", w)
 
 

@@ -72,6 +72,61 @@ def test_shift(golden, key, dt, tol):
     assert rel_l2(o2, G("dSadj2")) < tol
 
 
+@pytest.mark.parametrize("dt,tol", [("complex64", TOL32), ("complex128", TOL64)])
+@pytest.mark.parametrize("tag", ["a", "b", "c", "d"])
+def test_shift_back(golden, tag, dt, tol):
+    """Sback, coeffback and curlySback (shift.py:84-96, 138-153) against the
+    reference run under the shim."""
+    g = golden("sback")
+    G = lambda k: g[f"sb_{tag}_{k}"]
+    n, npsi, nz, nzpsi, nt = [int(v) for v in G("dims")]
+    s = O.Shift(n, npsi, nz, nzpsi, "complex64", dt)
+    assert rel_l2(s.Sback(G("g"), G("r"), G("m")), G("Sback")) < tol
+    if tag != "d":
+        # the stretched spline's symbol dips to ~0.1 at m = 1.55, so its inverse
+        # amplifies FP32 rounding about tenfold: 1e-5 for the back-filter
+        tb = max(tol, 1e-5)
+        assert rel_l2(s.coeffback(G("psi"), G("m")), G("coeffback")) < tb
+        assert rel_l2(s.curlySback(G("g"), G("r"), G("m")), G("curlySback")) < tb
+
+
+def _sback_loops(g, r, mag, n, npsi, nz, nzpsi):
+    """The sback kernel (cuda_kernels.py:305-370, dir = 1) as plain loops over
+    pixels and taps, in float64: a check on the vectorised restatement."""
+    f = np.zeros((g.shape[0], nzpsi, npsi), complex)
+    for tz in range(g.shape[0]):
+        m0 = float(mag[tz])
+        half = (m0 - 1.0) / 2.0
+        span = 2.0 * m0
+        for ty in range(nz):
+            for tx in range(n):
+                x = (m0 * (tx - n // 2) - r[tz, 1] + half) + npsi // 2
+                y = (m0 * (ty - nz // 2) - r[tz, 0] + half) + nzpsi // 2
+                ix, iy = int(np.floor(x)), int(np.floor(y))
+                dx, dy = x - ix, y - iy
+                for jy in range(int(np.ceil(dy - span)), int(dy + span)):
+                    if not 0 <= iy + jy < nzpsi:
+                        continue
+                    pdym = O.K.bphi(np.float64((dy - jy) / m0))
+                    for jx in range(int(np.ceil(dx - span)), int(dx + span)):
+                        if not 0 <= ix + jx < npsi:
+                            continue
+                        f[tz, iy + jy, ix + jx] += O.K.bphi(np.float64((dx - jx) / m0)) * pdym * g[tz, ty, tx]
+    return f
+
+
+@pytest.mark.parametrize("mag", [[0.8], [1.0], [1.55], [0.8, 1.3]])
+def test_sback_restatement_matches_kernel_loops(mag):
+    rng = np.random.default_rng(11)
+    n, npsi, nz, nzpsi = 8, 12, 6, 10
+    nt = len(mag)
+    g = rng.standard_normal((nt, nz, n)) + 1j * rng.standard_normal((nt, nz, n))
+    r = rng.uniform(-2, 2, (nt, 2))
+    mg = np.array(mag)
+    s = O.Shift(n, npsi, nz, nzpsi, "complex64", "complex128")
+    assert rel_l2(s.Sback(g, r, mg), _sback_loops(g, r, mg, n, npsi, nz, nzpsi)) < 1e-12
+
+
 def rec_args(n, ntheta, ndist, nobj, niter=1):
     """The solver arguments make_golden.py used."""
     return types.SimpleNamespace(
