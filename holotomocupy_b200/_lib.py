@@ -19,6 +19,8 @@ SIGNATURES = {
     "ht_version": [],
     "ht_last_error": [],
     "ht_launch_count": [],
+    "ht_host_register": [_vp, _c_long, _vp],
+    "ht_host_unregister": [_vp],
     "ht_prop_create": [_c_int, _c_int, _c_int, _vp, ctypes.POINTER(_vp)],
     "ht_prop_destroy": [_vp],
     "ht_prop_D": [_vp, _vp, _vp, _c_long, _c_int, _vp],

@@ -9,6 +9,29 @@ extern "C" const char* ht_last_error(void) { return ht::last_error(); }
 
 extern "C" long ht_launch_count(void) { return ht::launch_count(); }
 
+// ------------------------------------------------------- host memory
+// Page-lock host memory for asynchronous copies (the host arrays a chunked
+// call streams).  A range that is already page-locked is not an error: it is
+// reported with *registered = 0, and the runtime's pending error is cleared.
+extern "C" int ht_host_register(void* ptr, long bytes, int* registered) {
+  HT_REQUIRE(ptr && registered && bytes > 0, "ht_host_register: null pointer or empty range");
+  const cudaError_t e = cudaHostRegister(ptr, (size_t)bytes, cudaHostRegisterDefault);
+  if (e == cudaErrorHostMemoryAlreadyRegistered) {
+    (void)cudaGetLastError();
+    *registered = 0;
+    return ht::kOk;
+  }
+  HT_CHECK_CUDA(e);
+  *registered = 1;
+  return ht::kOk;
+}
+
+extern "C" int ht_host_unregister(void* ptr) {
+  HT_REQUIRE(ptr, "ht_host_unregister: null pointer");
+  HT_CHECK_CUDA(cudaHostUnregister(ptr));
+  return ht::kOk;
+}
+
 // ------------------------------------------------------------ graphs
 // Record the work issued to `stream` until ht_graph_end into a graph, instead
 // of running it.  Relaxed mode: a free of unrelated memory made meanwhile

@@ -31,6 +31,14 @@ const char* ht_last_error(void);
  * threads); no counterpart in the reference. */
 long ht_launch_count(void);
 
+/* Page-lock [ptr, ptr + bytes) of host memory so that copies from and to it
+ * run asynchronously (the host arrays Chunking.gpu_batch streams,
+ * src/holotomocupy/chunking.py:100-200).  *registered = 1 if this call
+ * locked it, 0 if it was page-locked already (not an error). */
+int ht_host_register(void* ptr, long bytes, int* registered);
+/* Undo ht_host_register. */
+int ht_host_unregister(void* ptr);
+
 /* ------------------------------------------------------------------------
  * Fresnel propagator.  Replaces Propagation.__init__/D/DT
  * (src/holotomocupy/propagation.py:14-44, 70-89, 91-112) and the cuFFTDx
