@@ -14,7 +14,7 @@ only) and `value` is the sum over ranks; time is the max over ranks.
 and the iteration replayed from a CUDA graph.  `plain` is the same
 reconstruction iterated the reference's way (step sizes on the host, one
 round trip per iteration).  `served` runs a mixed stream of requests
-(grid n in {128, 256, 384, 512} with probabilities 0.4/0.3/0.2/0.1,
+(64 requests, grid n in {128, 256, 384, 512} with probabilities 0.4/0.3/0.2/0.1,
 1.75 n angles, 4 distances, Poisson arrivals at 2/s, 16 iterations each)
 through the continuous-batching server and, on the same requests, one at a
 time through the plain path, with p50/p99 per-iteration latencies.
@@ -26,6 +26,7 @@ as rec_mpi.py runs them) for one angle and R + R^T for one slice, scaled to
 900 angles and 512 slices.
 """
 import argparse
+import gc
 import json
 import os
 import subprocess
@@ -220,7 +221,7 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--e2e-iters", type=int, default=4)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--serve-requests", type=int, default=12, help="requests in the mixed served stream (0: skip)")
+    ap.add_argument("--serve-requests", type=int, default=64, help="requests in the mixed served stream (0: skip)")
     ap.add_argument("--serve-iters", type=int, default=16)
     ap.add_argument("--c5", action="store_true",
                     help="the 2048^3 x 1800 x 4 operator measurement (D, R, R^T on a 256-slice sub-volume) "
@@ -336,6 +337,7 @@ def main():
     served = None
     if a.serve_requests > 0 and not a.profile:
         del rec, data, obj_true, prb_true, pos_true
+        gc.collect()   # the reconstruction's device handles go with it (cudaMalloc'd outside torch's cache)
         torch.cuda.synchronize()
         torch.cuda.empty_cache()
         served = served_vs_plain(a.serve_requests, a.serve_iters, 4321 + rank)
@@ -485,6 +487,7 @@ def served_vs_plain(nreq, niter, seed):
     for rid, (n, t) in enumerate(zip(sizes, arrivals)):
         args, data, prb0, pos0, _ = make_problem(int(n), int(round(1.75 * n)), 4, seed + 10 * rid, host=True)
         reqs.append(Request(rid=rid, args=args, data=data, prb0=prb0, pos0=pos0, niter=niter, arrival=float(t)))
+        gc.collect()
         torch.cuda.synchronize()
         torch.cuda.empty_cache()
     total = nreq * niter

@@ -66,10 +66,6 @@ class Rec:
             self.lam_prbfit = 0
         self.device = torch.device("cuda", torch.cuda.current_device())
         dev = self.device
-        self.F = [self.F0, self.F1, self.F2, self.F3]
-        self.gF = [self.gF0, self.gF1, self.gF2, self.gF3]
-        self.dF = [self.dF0, self.dF1, self.dF2, self.dF3]
-        self.d2F_dF = [self.d2F_dF0, self.d2F_dF1, self.d2F_dF2, self.d2F_dF3]
         if getattr(self, "distance", None) is None:                      # rec_mpi.py:55-60
             wavelength = 1.24e-09 / self.energy
             z1 = np.asarray(self.z1)
@@ -101,7 +97,27 @@ class Rec:
         self._h = h
         self._scal = torch.zeros(8, dtype=torch.float64, device=dev)
 
-    def __del__(self):
+    # the reference's operator lists (rec_mpi.py:38-45), built on access so
+    # that the object holds no reference to itself and is freed when dropped
+    @property
+    def F(self):
+        return [self.F0, self.F1, self.F2, self.F3]
+
+    @property
+    def gF(self):
+        return [self.gF0, self.gF1, self.gF2, self.gF3]
+
+    @property
+    def dF(self):
+        return [self.dF0, self.dF1, self.dF2, self.dF3]
+
+    @property
+    def d2F_dF(self):
+        return [self.d2F_dF0, self.d2F_dF1, self.d2F_dF2, self.d2F_dF3]
+
+    def close(self):
+        """Release the device state now (the handle, the recorded graph and
+        the arrays); the object is unusable afterwards."""
         try:
             self.release_graph()
         except Exception:
@@ -113,6 +129,15 @@ class Rec:
             except Exception:
                 pass
             self._h = None
+        try:
+            for name in ("vars", "grads", "etas", "data", "ref"):
+                if isinstance(getattr(self, name, None), (dict, torch.Tensor)):
+                    setattr(self, name, None)
+        except Exception:   # interpreter shutdown
+            pass
+
+    def __del__(self):
+        self.close()
 
     # ------------------------------------------------------------ state
     def alloc_arrays(self):

@@ -28,6 +28,7 @@ from dataclasses import dataclass, field
 import numpy as np
 import torch
 
+from . import _lib
 from .rec import Rec
 
 
@@ -151,8 +152,13 @@ class Server:
         """Free the retired reconstructions' device memory (synchronises the
         device); returns the bytes released."""
         freed = sum(b for _, b in self._retired)
-        self._retired.clear()
         torch.cuda.synchronize(self.device)
+        for rec, _ in self._retired:
+            rec.close()
+        self._retired.clear()
+        # the library allocates outside torch's caching allocator: hand the
+        # cached blocks back so that its next allocations find them
+        torch.cuda.empty_cache()
         return freed
 
     # ------------------------------------------------------------- loop
@@ -177,7 +183,18 @@ class Server:
                 r = pending.pop(0)
                 slot = _Slot(r, self._streams.pop())
                 r.t_admit = time.perf_counter() - t0
-                self._admit(slot)
+                try:
+                    self._admit(slot)
+                except (torch.OutOfMemoryError, _lib.HoloError) as err:
+                    # the estimate fitted but the device did not (fragmentation,
+                    # other users of the GPU): free what is retired and retry
+                    # once the active requests have made room
+                    self._streams.append(slot.stream)
+                    pending.insert(0, r)
+                    self._release()
+                    if not active or "out of memory" not in str(err):
+                        raise
+                    break
                 active.append(slot)
                 used += slot.bytes
                 self.peak_bytes = max(self.peak_bytes, used)
@@ -243,6 +260,7 @@ def run_plain(reqs, realtime=False):
             lat.append(e0.elapsed_time(e1))
         rec.bh_finish()
         results.append({k: rec.vars[k].cpu() for k in ("obj", "prb", "pos")})
+        rec.close()
         del rec
     torch.cuda.synchronize()
     return time.perf_counter() - t0, lat, results

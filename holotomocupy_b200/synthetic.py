@@ -113,6 +113,7 @@ def make_problem(n, ntheta, ndist, seed, photons=1e4, device="cuda", pos_amp=2.0
     gen = torch.Generator(device=device).manual_seed(seed + 4)
     pos0 = pos + pos_err * (2 * torch.rand(pos.shape, generator=gen, device=device) - 1)
     prb0 = torch.ones_like(prb)
+    rec.close()
     del rec
     if host:
         data, prb0, pos0 = (t.cpu().pin_memory() for t in (data, prb0, pos0))
