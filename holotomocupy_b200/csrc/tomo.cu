@@ -442,21 +442,27 @@ __global__ void k_cell_fill(GatherGeom G, int cps, const long* __restrict__ off,
   cell_pairs(G, X, Y, f);
 }
 
-// gs [zb][ntheta][n][Z] -> fde [zb][2n][2n][Z]; grid (ceil(slices * 32 / 256), ceil(nzb / ZG));
-// ZG slice batches per lane
+// gs [zb][ntheta][n][Z] -> fde [zb][2n][2n][Z]; grid ceil(slices * 32 / 256) * ceil(nzb / ZG)
+// blocks (see the block order below); ZG slice batches per lane
 template <int Z, int ZG>
 __global__ void __launch_bounds__(256)
 k_tcell(const float2* __restrict__ gs, float2* __restrict__ fde, const int* __restrict__ len,
-        const long* __restrict__ off, const int2* __restrict__ ent, int twon, long nslices, long nsamp, int nzb) {
+        const long* __restrict__ off, const int2* __restrict__ ent, int twon, long nslices, long nsamp, int nzb,
+        int ngroups) {
   constexpr int Q = Z / 2;       // lanes per cell
   constexpr int CPS = 32 / Q;    // cells per slice (warp)
-  const long tid = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  // block b handles the cells of block b / ngroups for the slice batches of
+  // group b % ngroups: the ngroups consecutive blocks that read one stretch of
+  // the pair lists run together, so the lists come from DRAM once and from L2
+  // for the other groups
+  const int grp = (int)(blockIdx.x % ngroups);
+  const long tid = (long)(blockIdx.x / ngroups) * blockDim.x + threadIdx.x;
   const long sl = tid / 32;
   if (sl >= nslices) return;
   const int lane = (int)(tid % 32), k = lane / Q, q = lane % Q;
   int X, Y;
   const bool live = slice_cell(sl, k, twon, slice_shape(CPS), X, Y);
-  const int zb0 = blockIdx.y * ZG;
+  const int zb0 = grp * ZG;
   const int nl = len[sl];
   const int2* e = ent + off[sl] * CPS + k;
   float4 acc[ZG];
@@ -597,8 +603,10 @@ static cudaError_t tomo_RT_sized(const float2* sino, float2* obj, const float* p
     constexpr int ZG = 2;  // slice batches per read of the pair lists
     const SliceShape sh = slice_shape(64 / Z);
     const long nsl = (long)((N2 + sh.tw - 1) / sh.tw) * ((N2 + sh.th - 1) / sh.th);
-    k_tcell<Z, ZG><<<dim3((unsigned)((nsl * 32 + 255) / 256), (unsigned)((nzb + ZG - 1) / ZG)), 256, 0, st>>>(
-        gs, fde, L.len, L.off, L.ent, N2, nsl, (long)G.ntheta * n, nzb);
+    const int ngroups = (nzb + ZG - 1) / ZG;
+    const long nblk = (nsl * 32 + 255) / 256;
+    k_tcell<Z, ZG><<<(unsigned)(nblk * ngroups), 256, 0, st>>>(gs, fde, L.len, L.off, L.ent, N2, nsl,
+                                                            (long)G.ntheta * n, nzb, ngroups);
   }
   count_launch();
   k_tcol_adj<N2><<<dim3(N2, nzb), C2::THREADS, C2::SMEM, st>>>(fde, fab, tw_2n);
