@@ -298,6 +298,17 @@ __device__ __forceinline__ void fft_line_from(const IN& in, const SM& sm, int t,
   fft_stages_io<N, PL::E, 1, INV, true, false>(v, in, sm, sm, t, tw4, sync, typename PL::R{});
 }
 
+// FFT of a line read from `in` and written to `out` (the first stage loads
+// from `in`, the last stage stores to `out`, the stages between pass through
+// shared memory); no barrier is needed before it, none is made after it.
+template <int N, bool INV, class IN, class SM, class OUT, class SY = CtaSync>
+__device__ __forceinline__ void fft_line_io(const IN& in, const SM& sm, const OUT& out, int t,
+                                            const float2* __restrict__ tw4, const SY& sync = SY{}) {
+  using PL = Plan<N>;
+  float2 v[PL::E];
+  fft_stages_io<N, PL::E, 1, INV, true, true>(v, in, sm, out, t, tw4, sync, typename PL::R{});
+}
+
 // FFT of a line in shared memory (the caller synchronised after writing it),
 // result stored through `out` (any view with st(k, v)); the line is not
 // barriered afterwards.

@@ -145,32 +145,38 @@ k_trow_fwd(const float2* __restrict__ obj, const float* __restrict__ phi, float2
 }
 
 // --------------------------------------------------- 2: columns (R)
-// fa [zb][n][2n][Z] -> fde [zb][2n][2n][Z];  grid (2n, nzb)
+// fa [zb][n][2n][Z] -> fde [zb][2n][2n][Z];  grid (2n, nzb).  Thread
+// (t, l = threadIdx.x % Z) works on slice l, so a warp reads and writes whole
+// Z-vectors of 32 / Z rows; the first FFT stage loads from fa (zero outside
+// the central n rows) and the last stores to fde (with the (-1)^ky sign), so
+// the column passes shared memory only between stages.
+template <int Z>
+struct TColFwdIn {
+  const float2* p;  // fa at row 0 of this column and slice
+  int n, rowstride;
+  __device__ __forceinline__ float2 ld(int k) const {
+    return (k >= n / 2 && k < 3 * n / 2) ? p[(long)(k - n / 2) * rowstride] : make_float2(0.f, 0.f);
+  }
+};
+struct TColFwdOut {
+  float2* p;  // fde at row 0 of this column and slice
+  int rowstride;
+  __device__ __forceinline__ void st(int k, float2 v) const {
+    p[(long)k * rowstride] = (k & 1) ? make_float2(-v.x, -v.y) : v;
+  }
+};
+
 template <int N2>
 __global__ void __launch_bounds__(ZCfg<N2, TZ<N2>::Z>::THREADS)
 k_tcol_fwd(const float2* __restrict__ fa, float2* __restrict__ fde, const float2* __restrict__ tw4) {
   constexpr int Z = TZ<N2>::Z;
-  constexpr int T = ZCfg<N2, Z>::T;
   constexpr int n = N2 / 2;
   extern __shared__ float2 smem[];
-  const int l = threadIdx.x / T, t = threadIdx.x % T;
+  const int l = threadIdx.x % Z, t = threadIdx.x / Z;
   const int kx = blockIdx.x, zb = blockIdx.y;
-  const float2* src = fa + (long)zb * n * N2 * Z + (long)kx * Z;
-  for (int idx = threadIdx.x; idx < N2 * Z; idx += blockDim.x) {
-    const int pr = idx / Z, ll = idx % Z;
-    const float2 v = (pr >= n / 2 && pr < 3 * n / 2) ? src[(long)(pr - n / 2) * N2 * Z + ll] : make_float2(0.f, 0.f);
-    zline<N2, Z>(smem, ll).st(pr, v);
-  }
-  __syncthreads();
-  fft_line<N2, false>(zline<N2, Z>(smem, l), t, tw4, line_sync<T>());
-  __syncthreads();  // the stores below read every line
-  float2* dst = fde + (long)zb * N2 * N2 * Z + (long)kx * Z;
-  for (int idx = threadIdx.x; idx < N2 * Z; idx += blockDim.x) {
-    const int ky = idx / Z, ll = idx % Z;
-    float2 v = zline<N2, Z>(smem, ll).ld(ky);
-    if (ky & 1) v = make_float2(-v.x, -v.y);
-    dst[(long)ky * N2 * Z + ll] = v;
-  }
+  const float2* src = fa + (long)zb * n * N2 * Z + (long)kx * Z + l;
+  float2* dst = fde + (long)zb * N2 * N2 * Z + (long)kx * Z + l;
+  fft_line_io<N2, false>(TColFwdIn<Z>{src, n, N2 * Z}, SmCol<Z>{smem + l}, TColFwdOut{dst, N2 * Z}, t, tw4);
 }
 
 // ------------------------------------- 3: gather + detector IFFT (R)
@@ -492,33 +498,37 @@ k_tcell(const float2* __restrict__ gs, float2* __restrict__ fde, const int* __re
 }
 
 // ------------------------------------------- RT 3: column IFFT
-// fde [zb][2n][2n][Z] -> fb [zb][n][2n][Z] (central rows);  grid (2n, nzb)
+// fde [zb][2n][2n][Z] -> fb [zb][n][2n][Z] (central rows);  grid (2n, nzb).
+// Thread layout and direct global first/last stages as in k_tcol_fwd.
+struct TColAdjIn {
+  const float2* p;  // fde at row 0 of this column and slice
+  int rowstride, kx;
+  __device__ __forceinline__ float2 ld(int k) const {
+    const float2 v = p[(long)k * rowstride];
+    return ((k + kx) & 1) ? make_float2(-v.x, -v.y) : v;  // pre-sign (-1)^(ky+kx)
+  }
+};
+struct TColAdjOut {
+  float2* p;  // fb at row 0 of this column and slice
+  int n, rowstride;
+  float s;    // 1 / 2n
+  __device__ __forceinline__ void st(int k, float2 v) const {
+    if (k >= n / 2 && k < 3 * n / 2) p[(long)(k - n / 2) * rowstride] = cscale(v, (k & 1) ? -s : s);  // post sign
+  }
+};
+
 template <int N2>
 __global__ void __launch_bounds__(ZCfg<N2, TZ<N2>::Z>::THREADS)
 k_tcol_adj(const float2* __restrict__ fde, float2* __restrict__ fb, const float2* __restrict__ tw4) {
   constexpr int Z = TZ<N2>::Z;
-  constexpr int T = ZCfg<N2, Z>::T;
   constexpr int n = N2 / 2;
   extern __shared__ float2 smem[];
-  const int l = threadIdx.x / T, t = threadIdx.x % T;
+  const int l = threadIdx.x % Z, t = threadIdx.x / Z;
   const int kx = blockIdx.x, zb = blockIdx.y;
-  const float2* src = fde + (long)zb * N2 * N2 * Z + (long)kx * Z;
-  for (int idx = threadIdx.x; idx < N2 * Z; idx += blockDim.x) {
-    const int ky = idx / Z, ll = idx % Z;
-    float2 v = src[(long)ky * N2 * Z + ll];
-    if ((ky + kx) & 1) v = make_float2(-v.x, -v.y);  // pre-sign (-1)^(ky+kx)
-    zline<N2, Z>(smem, ll).st(ky, v);
-  }
-  __syncthreads();
-  fft_line<N2, true>(zline<N2, Z>(smem, l), t, tw4, line_sync<T>());
-  __syncthreads();  // the stores below read every line
-  float2* dst = fb + (long)zb * n * N2 * Z + (long)kx * Z;
-  const float s = 1.0f / (float)N2;
-  for (int idx = threadIdx.x; idx < n * Z; idx += blockDim.x) {
-    const int r = idx / Z, ll = idx % Z;
-    const int pr = r + n / 2;
-    dst[(long)r * N2 * Z + ll] = cscale(zline<N2, Z>(smem, ll).ld(pr), (pr & 1) ? -s : s);  // post row sign
-  }
+  const float2* src = fde + (long)zb * N2 * N2 * Z + (long)kx * Z + l;
+  float2* dst = fb + (long)zb * n * N2 * Z + (long)kx * Z + l;
+  fft_line_io<N2, true>(TColAdjIn{src, N2 * Z, kx}, SmCol<Z>{smem + l}, TColAdjOut{dst, n, N2 * Z, 1.0f / (float)N2},
+                        t, tw4);
 }
 
 // ---------------------------------------------- RT 4: row IFFT
