@@ -346,7 +346,28 @@ k_symbol_rows(const float2* in, float2* out, long nrows, const float* __restrict
   for (int k = t; k < N; k += T) out[row * N + k] = sm.ld(k);
 }
 
-// data [nimg, N, ncols] in place along the column axis
+// data [nimg, N, ncols] in place along the column axis.  The forward FFT's
+// first stage loads the block's C columns from global memory and the inverse
+// FFT's last stage stores them back (a warp covers 32 / C rows of C adjacent
+// columns per access); the tile passes shared memory only between stages.
+template <int N>
+struct SymColIn {
+  const float2* p;  // row 0 of the column
+  int ncols;
+  bool valid;
+  __device__ __forceinline__ float2 ld(int k) const {
+    return valid ? p[(long)k * ncols] : make_float2(0.f, 0.f);
+  }
+};
+struct SymColOut {
+  float2* p;
+  int ncols;
+  bool valid;
+  __device__ __forceinline__ void st(int k, float2 v) const {
+    if (valid) p[(long)k * ncols] = v;
+  }
+};
+
 template <int N>
 __global__ void __launch_bounds__(ColCfg<N>::THREADS)
 k_symbol_cols(float2* data, int ncols, const float* __restrict__ sym, const float2* __restrict__ tw4) {
@@ -354,22 +375,14 @@ k_symbol_cols(float2* data, int ncols, const float* __restrict__ sym, const floa
   constexpr int T = ColCfg<N>::T;
   extern __shared__ float2 tile[];
   const int c = threadIdx.x % C, t = threadIdx.x / C;
-  const int col0 = blockIdx.x * C;
-  float2* img = data + (long)blockIdx.y * N * ncols;
-  for (int idx = threadIdx.x; idx < N * C; idx += blockDim.x) {
-    const int rr = idx / C, cc = idx % C;
-    tile[col_row<C>(rr) * C + cc] = (col0 + cc < ncols) ? img[(long)rr * ncols + col0 + cc] : make_float2(0.f, 0.f);
-  }
-  __syncthreads();
+  const bool valid = blockIdx.x * C + c < ncols;
+  const int col = min((int)blockIdx.x * C + c, ncols - 1);
+  float2* img = data + (long)blockIdx.y * N * ncols + col;
   SmCol<C> sm{tile + c};
-  fft_line<N, false>(sm, t, tw4);
+  fft_line_from<N, false>(SymColIn<N>{img, ncols, valid}, sm, t, tw4);
   for (int k = t; k < N; k += T) sm.st(k, cscale(sm.ld(k), __ldg(&sym[k])));
   __syncthreads();
-  fft_line<N, true>(sm, t, tw4);
-  for (int idx = threadIdx.x; idx < N * C; idx += blockDim.x) {
-    const int rr = idx / C, cc = idx % C;
-    if (col0 + cc < ncols) img[(long)rr * ncols + col0 + cc] = tile[col_row<C>(rr) * C + cc];
-  }
+  fft_line_to<N, true>(sm, SymColOut{img, ncols, valid}, t, tw4);
 }
 
 template <int N>
