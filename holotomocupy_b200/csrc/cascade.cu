@@ -782,17 +782,24 @@ k_casc_hess_fwd(const T* __restrict__ c, const float* __restrict__ pos, const fl
       // v_d = x12 (prb_d + i prb y22_d)   (dF2 then dF1, rec_mpi.py:591, 664)
       v0 = cmul(x12, cadd(q0, cmul_i(cmul(pr, Y0))));
       if (NDIR == 2) v1 = cmul(x12, cadd(q1, cmul_i(cmul(pr, Y1))));
-      // L1(a,b) = Re(conj(P) i (q_a y22_b + q_b y22_a));  L2(a,b) = -Re(conj(P) prb y22_a y22_b)
+      // L1(a,b) = Re(conj(P) i (q_a y22_b + q_b y22_a));  L2(a,b) = -Re(conj(P) prb y22_a y22_b),
+      // with the factors the forms share formed once: u_d = i conj(P) q_d, A = conj(P) prb
       const float2 cP = cconj(P);
-      s[0] += cmul(cP, cmul_i(cscale(cmul(q0, Y0), 2.f))).x;
-      s[3] += -cmul(cP, cmul(pr, cmul(Y0, Y0))).x;
+      const float2 iP = cmul_i(cP);
+      const float2 u0 = cmul(iP, q0);
+      const float2 A = cmul(cP, pr);
+      const float2 a0 = cmul(A, Y0);
+      auto re = [](float2 x, float2 y) { return x.x * y.x - x.y * y.y; };  // Re(x y)
+      s[0] += 2.f * re(u0, Y0);
+      s[3] -= re(a0, Y0);
       s[6] += El<T>::redot(Y, ax0);
       s[7] += El<T>::redot(Y, ay0);
       if (NDIR == 2) {
-        s[1] += cmul(cP, cmul_i(cadd(cmul(q0, Y1), cmul(q1, Y0)))).x;
-        s[2] += cmul(cP, cmul_i(cscale(cmul(q1, Y1), 2.f))).x;
-        s[4] += -cmul(cP, cmul(pr, cmul(Y0, Y1))).x;
-        s[5] += -cmul(cP, cmul(pr, cmul(Y1, Y1))).x;
+        const float2 u1 = cmul(iP, q1);
+        s[1] += re(u0, Y1) + re(u1, Y0);
+        s[2] += 2.f * re(u1, Y1);
+        s[4] -= re(a0, Y1);
+        s[5] -= re(cmul(A, Y1), Y1);
         s[8] += El<T>::redot(Y, ax1);
         s[9] += El<T>::redot(Y, ay1);
       }
