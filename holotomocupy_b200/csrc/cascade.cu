@@ -186,10 +186,11 @@ __device__ __forceinline__ float2 ld_pos(const float* pos, long img) {
   return make_float2(pos[2 * img + 0], pos[2 * img + 1]);
 }
 
-// Doubles of shared scratch line_sums<T, K> needs for a block of THREADS.
+// Doubles of shared scratch line_sums<T, K> needs for a block of THREADS,
+// rounded up to an even count so that what follows it stays 16-byte aligned.
 template <int T>
 __host__ __device__ constexpr int red_doubles(int K, int threads) {
-  return (T % 32 == 0) ? K * (threads / 32) : K * threads;
+  return ((T % 32 == 0 ? K * (threads / 32) : K * threads) + 1) / 2 * 2;
 }
 
 // Launch shape of a stencil row kernel: NFFT row lines of the DCT plus NSET
@@ -242,6 +243,59 @@ template <class T>
 __device__ __forceinline__ void vrow4(const T* __restrict__ V, const int (&xx)[4], T (&v)[4]) {
 #pragma unroll
   for (int j = 0; j < 4; ++j) v[j] = V[xx[j]];
+}
+
+// Two adjacent elements of T moved as one vector (16 bytes for complex, 8 for
+// real): the interleaved vertical rows store the sets of one object column
+// side by side, so a tap's sets load in NS / 2 accesses.
+template <class T>
+struct Pair;
+template <>
+struct Pair<float2> {
+  static __device__ __forceinline__ void st(float2* p, float2 a, float2 b) {
+    *reinterpret_cast<float4*>(p) = make_float4(a.x, a.y, b.x, b.y);
+  }
+  static __device__ __forceinline__ void ld(const float2* p, float2& a, float2& b) {
+    const float4 q = *reinterpret_cast<const float4*>(p);
+    a = make_float2(q.x, q.y);
+    b = make_float2(q.z, q.w);
+  }
+};
+template <>
+struct Pair<float> {
+  static __device__ __forceinline__ void st(float* p, float a, float b) {
+    *reinterpret_cast<float2*>(p) = make_float2(a, b);
+  }
+  static __device__ __forceinline__ void ld(const float* p, float& a, float& b) {
+    const float2 q = *reinterpret_cast<const float2*>(p);
+    a = q.x;
+    b = q.y;
+  }
+};
+
+// vrows for two weight sets into the interleaved layout V[ix * NST + base + {0, 1}]
+// (the same sums, in the same order, as vrows)
+template <class T, int NST>
+__device__ __forceinline__ void vrows_pair(T* __restrict__ V, int base, int nobj, const T* __restrict__ cb,
+                                           const int (&yy)[4], const float* __restrict__ w0,
+                                           const float* __restrict__ w1, int t, int TT) {
+  const T* r0 = cb + (long)yy[0] * nobj;
+  const T* r1 = cb + (long)yy[1] * nobj;
+  const T* r2 = cb + (long)yy[2] * nobj;
+  const T* r3 = cb + (long)yy[3] * nobj;
+  for (int ix = t; ix < nobj; ix += TT) {
+    const T v0 = __ldg(&r0[ix]), v1 = __ldg(&r1[ix]), v2 = __ldg(&r2[ix]), v3 = __ldg(&r3[ix]);
+    T a = El<T>::zero(), b = El<T>::zero();
+    El<T>::fma(a, w0[0], v0);
+    El<T>::fma(a, w0[1], v1);
+    El<T>::fma(a, w0[2], v2);
+    El<T>::fma(a, w0[3], v3);
+    El<T>::fma(b, w1[0], v0);
+    El<T>::fma(b, w1[1], v1);
+    El<T>::fma(b, w1[2], v2);
+    El<T>::fma(b, w1[3], v3);
+    Pair<T>::st(V + (long)ix * NST + base, a, b);
+  }
 }
 
 // Per-image accumulator slots
@@ -733,10 +787,11 @@ k_casc_hess_fwd(const T* __restrict__ c, const float* __restrict__ pos, const fl
     const RowGeo<1> rg(D, m0, r.x, ty);
     if (valid) {
       const float* const w[2] = {rg.py, rg.dpy};
-      // sets: (c, py) (c, dpy) (c_y, py) (c_y, dpy) [(c_z, py) (c_z, dpy)]
-      vrows<T, 2>(V, D.nobj, c + coff, rg.yy, w, t, TT);
-      vrows<T, 2>(V + 2 * D.nobj, D.nobj, c0 + coff, rg.yy, w, t, TT);
-      if (NDIR == 2) vrows<T, 2>(V + 4 * D.nobj, D.nobj, c1 + coff, rg.yy, w, t, TT);
+      // sets, interleaved per object column (V[ix * NS + set]):
+      // (c, py) (c, dpy) (c_y, py) (c_y, dpy) [(c_z, py) (c_z, dpy)]
+      vrows_pair<T, NS>(V, 0, D.nobj, c + coff, rg.yy, w[0], w[1], t, TT);
+      vrows_pair<T, NS>(V, 2, D.nobj, c0 + coff, rg.yy, w[0], w[1], t, TT);
+      if (NDIR == 2) vrows_pair<T, NS>(V, 4, D.nobj, c1 + coff, rg.yy, w[0], w[1], t, TT);
     }
   }
   __syncthreads();
@@ -746,22 +801,29 @@ k_casc_hess_fwd(const T* __restrict__ c, const float* __restrict__ pos, const fl
     float2 v0 = make_float2(0.f, 0.f), v1 = make_float2(0.f, 0.f);
     if (valid) {
       const ColGeo<1> cg(D, m0, r.y, tx);
-      T v[4];
-      vrow4(V, cg.xx, v);
-      const T x22 = dot4(cg.px, v), dxc = dot4(cg.dpx, v);
-      vrow4(V + D.nobj, cg.xx, v);
-      const T dyc = dot4(cg.px, v);
-      vrow4(V + 2 * D.nobj, cg.xx, v);
-      const T s0 = dot4(cg.px, v), ax0 = dot4(cg.dpx, v);
-      vrow4(V + 3 * D.nobj, cg.xx, v);
-      const T ay0 = dot4(cg.px, v);
+      // the horizontal taps: every set of one tap's column in NS / 2 vector loads
+      T x22 = El<T>::zero(), dxc = El<T>::zero(), dyc = El<T>::zero();
+      T s0 = El<T>::zero(), ax0 = El<T>::zero(), ay0 = El<T>::zero();
       T s1 = El<T>::zero(), ax1 = El<T>::zero(), ay1 = El<T>::zero();
-      if (NDIR == 2) {
-        vrow4(V + 4 * D.nobj, cg.xx, v);
-        s1 = dot4(cg.px, v);
-        ax1 = dot4(cg.dpx, v);
-        vrow4(V + 5 * D.nobj, cg.xx, v);
-        ay1 = dot4(cg.px, v);
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const T* col = V + (long)cg.xx[j] * NS;
+        T a0, a1, a2, a3;
+        Pair<T>::ld(col, a0, a1);
+        Pair<T>::ld(col + 2, a2, a3);
+        El<T>::fma(x22, cg.px[j], a0);
+        El<T>::fma(dxc, cg.dpx[j], a0);
+        El<T>::fma(dyc, cg.px[j], a1);
+        El<T>::fma(s0, cg.px[j], a2);
+        El<T>::fma(ax0, cg.dpx[j], a2);
+        El<T>::fma(ay0, cg.px[j], a3);
+        if (NDIR == 2) {
+          T a4, a5;
+          Pair<T>::ld(col + 4, a4, a5);
+          El<T>::fma(s1, cg.px[j], a4);
+          El<T>::fma(ax1, cg.dpx[j], a4);
+          El<T>::fma(ay1, cg.px[j], a5);
+        }
       }
       // dS (rec_mpi.py:757; cuda_kernels.py:600-609): sum phi phi c_d - (dphi_x phi_y r_dx + phi_x dphi_y r_dy) c
       T y0 = s0, y1 = s1;
