@@ -560,9 +560,40 @@ __device__ __forceinline__ void cand_range_r(float rm0, float C0, int i, int nha
 // column of its stencil (int) and its four tap weights (float): 20 bytes, kept
 // where the vertically reduced rows were once those are consumed.  Elements of
 // T per detector row of that shared area:
+// The vertical rows themselves: set 0 as nobj elements, then sets 1 and 2
+// as nobj pairs from an even offset (so that a pair loads as one vector).
 constexpr int kAdjTabBytes = 20;
+__host__ __device__ constexpr int adj_pair_off(int nobj) { return (nobj + 1) / 2 * 2; }
 __host__ __device__ constexpr int adj_line_elems(int nobj, int n, int elem) {
-  return (3 * nobj * elem >= kAdjTabBytes * n) ? 3 * nobj : (kAdjTabBytes * n + elem - 1) / elem;
+  return ((adj_pair_off(nobj) + 2 * nobj) * elem >= kAdjTabBytes * n)
+             ? adj_pair_off(nobj) + 2 * nobj
+             : ((kAdjTabBytes * n + elem - 1) / elem + 1) / 2 * 2;
+}
+
+// vrows for the adjoint's three weight sets: set 0 to V0[ix], sets 1 and 2 to
+// the pair V12[2 ix], V12[2 ix + 1] (the sums and their order as in vrows)
+template <class T>
+__device__ __forceinline__ void vrows_adj(T* __restrict__ V0, T* __restrict__ V12, int nobj,
+                                          const T* __restrict__ cb, const int (&yy)[4],
+                                          const float* const (&w)[3], int t, int TT) {
+  const T* r0 = cb + (long)yy[0] * nobj;
+  const T* r1 = cb + (long)yy[1] * nobj;
+  const T* r2 = cb + (long)yy[2] * nobj;
+  const T* r3 = cb + (long)yy[3] * nobj;
+  for (int ix = t; ix < nobj; ix += TT) {
+    const T v0 = __ldg(&r0[ix]), v1 = __ldg(&r1[ix]), v2 = __ldg(&r2[ix]), v3 = __ldg(&r3[ix]);
+    T a[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      a[k] = El<T>::zero();
+      El<T>::fma(a[k], w[k][0], v0);
+      El<T>::fma(a[k], w[k][1], v1);
+      El<T>::fma(a[k], w[k][2], v2);
+      El<T>::fma(a[k], w[k][3], v3);
+    }
+    V0[ix] = a[0];
+    Pair<T>::st(V12 + 2 * ix, a[1], a[2]);
+  }
 }
 
 // ============================================== adjoint row pass
@@ -596,12 +627,11 @@ k_casc_adj(const float2* __restrict__ tmp, float2* __restrict__ Pc, T* __restric
   const RowGeo<2> rg(D, m0, r.x, ty);
   if (valid) {
     const float* const w[3] = {rg.py, rg.dpy, rg.d2py};
-    vrows<T, 3>(V, D.nobj, c + th * (long)D.nzobj * D.nobj, rg.yy, w, t, TT);
+    vrows_adj<T>(V, V + adj_pair_off(D.nobj), D.nobj, c + th * (long)D.nzobj * D.nobj, rg.yy, w, t, TT);
   }
   dct3_start<N, TT>(sm, t, tw4, tmp + row * N, valid);  // ends with a barrier: V is complete
   const T* V0 = V;
-  const T* V1 = V + D.nobj;
-  const T* V2 = V + 2 * D.nobj;
+  const T* V12 = V + adj_pair_off(D.nobj);
   float s[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
   float2 Yr[E];
 #pragma unroll
@@ -611,13 +641,20 @@ k_casc_adj(const float2* __restrict__ tmp, float2* __restrict__ Pc, T* __restric
     if (!valid) continue;
     const float2 G = sm.ld(dct_perm(tx, N));
     const ColGeo<2> cg(D, m0, r.y, tx);
-    T v[4];
-    vrow4(V0, cg.xx, v);
-    const T x22 = dot4(cg.px, v), ax = dot4(cg.dpx, v), hxx = dot4(cg.d2px, v);
-    vrow4(V1, cg.xx, v);
-    const T ay = dot4(cg.px, v), hxy = dot4(cg.dpx, v);
-    vrow4(V2, cg.xx, v);
-    const T hyy = dot4(cg.px, v);
+    T x22 = El<T>::zero(), ax = El<T>::zero(), hxx = El<T>::zero();
+    T ay = El<T>::zero(), hxy = El<T>::zero(), hyy = El<T>::zero();
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const T a0 = V0[cg.xx[j]];
+      T a1, a2;
+      Pair<T>::ld(V12 + 2 * cg.xx[j], a1, a2);
+      El<T>::fma(x22, cg.px[j], a0);
+      El<T>::fma(ax, cg.dpx[j], a0);
+      El<T>::fma(hxx, cg.d2px[j], a0);
+      El<T>::fma(ay, cg.px[j], a1);
+      El<T>::fma(hxy, cg.dpx[j], a1);
+      El<T>::fma(hyy, cg.px[j], a2);
+    }
     const float2 x12 = cexp_i(El<T>::cplx(x22));
     const float2 P = cmulc(G, x12);
     Pc[row * N + tx] = P;
