@@ -820,6 +820,10 @@ k_casc_hess_fwd(const T* __restrict__ c, const float* __restrict__ pos, const fl
   const float2 r = valid ? ld_pos(pos, img) : make_float2(0.f, 0.f);
   const float2 rd0 = valid ? ld_pos(pos0, img) : make_float2(0.f, 0.f);
   const float2 rd1 = (valid && NDIR == 2) ? ld_pos(pos1, img) : make_float2(0.f, 0.f);
+  // P streams from DRAM: each pixel's value is loaded one pixel ahead (the
+  // first before the vertical pass), so its latency overlaps other work
+  const float2* Prow = Pc + row * N;
+  float2 Pnext = valid ? Prow[t] : make_float2(0.f, 0.f);
   {
     const RowGeo<1> rg(D, m0, r.x, ty);
     if (valid) {
@@ -836,6 +840,8 @@ k_casc_hess_fwd(const T* __restrict__ c, const float* __restrict__ pos, const fl
   float s[10] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
   for (int tx = t; tx < N; tx += TT) {
     float2 v0 = make_float2(0.f, 0.f), v1 = make_float2(0.f, 0.f);
+    const float2 P = Pnext;
+    if (valid && tx + TT < N) Pnext = Prow[tx + TT];
     if (valid) {
       const ColGeo<1> cg(D, m0, r.y, tx);
       // the horizontal taps: every set of one tap's column in NS / 2 vector loads
@@ -873,7 +879,6 @@ k_casc_hess_fwd(const T* __restrict__ c, const float* __restrict__ pos, const fl
       const float2 x12 = cexp_i(El<T>::cplx(x22));
       const long p = ((long)k * D.nz + ty) * N + tx;
       const float2 pr = prb[p];
-      const float2 P = Pc[row * N + tx];
       const T Y = El<T>::proj(rot<false>(cmulc(P, pr)));
       const float2 Y0 = El<T>::cplx(y0), Y1 = El<T>::cplx(y1);
       const float2 q0 = prb0[p];
