@@ -541,12 +541,12 @@ KERNEL_BYTES = {
 _CASE_512_96 = types.SimpleNamespace(n=512, nz=512, nobj=512, nzobj=512, ntheta=96, ndist=4)
 _CASE_256_448 = types.SimpleNamespace(n=256, nz=256, nobj=256, nzobj=256, ntheta=448, ndist=4)
 NCU_CAPTURE = {
-    "k_casc_fwd": (1.122054e9, 1792, _CASE_256_448),
-    "k_casc_resid": (2.761909e9, 384, _CASE_512_96),
-    "k_casc_adj": (2.661818e9, 384, _CASE_512_96),
-    "k_casc_hess_fwd": (3.384108e9, 2 * 384, _CASE_512_96),
-    "k_casc_hess_q": (2.827706e9, 2 * 384, _CASE_512_96),
-    "k_dct_cols": (1.569498e9, 384, _CASE_512_96),
+    "k_casc_fwd": (0.967394e9, 384, _CASE_512_96),
+    "k_casc_resid": (2.769351e9, 384, _CASE_512_96),
+    "k_casc_adj": (2.659368e9, 384, _CASE_512_96),
+    "k_casc_hess_fwd": (3.426991e9, 2 * 384, _CASE_512_96),
+    "k_casc_hess_q": (2.828069e9, 2 * 384, _CASE_512_96),
+    "k_dct_cols": (1.569036e9, 384, _CASE_512_96),
     "k_tgather": (0.651061e9, 256, _CASE_256_448),
     "k_tcell": (0.797557e9, 256, _CASE_256_448),   # the pair lists come from DRAM once (group-major block order)
 }
@@ -600,7 +600,7 @@ def roofline(kt):
             "frac": d["frac"], "traffic": d["traffic"], "peak_source": "measured" if peaks else "fallback",
             "launch_ms": d["launch_ms"],
             "traffic_source": "ncu dram bytes / algorithmic bytes of one captured launch (512^3 x 96 angles; "
-                              "256^3 x 448 angles for the Radon kernels and k_casc_fwd), times the "
+                              "256^3 x 448 angles for the Radon kernels), times the "
                               "algorithmic bytes of this launch",
             "kernels": rows}
 
