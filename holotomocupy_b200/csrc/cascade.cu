@@ -168,12 +168,6 @@ struct ColGeo {
   }
 };
 
-// the four samples of one object row under a pixel's horizontal stencil
-template <class T>
-__device__ __forceinline__ void row4(const T* __restrict__ rowp, const int (&xx)[4], T (&v)[4]) {
-#pragma unroll
-  for (int j = 0; j < 4; ++j) v[j] = __ldg(&rowp[xx[j]]);
-}
 template <class T>
 __device__ __forceinline__ T dot4(const float (&w)[4], const T (&v)[4]) {
   T a = El<T>::zero();

@@ -93,20 +93,6 @@ __device__ __forceinline__ float wy_tap(const GatherGeom& G, const Window& w, in
   return G.coeff0 * __expf(G.coeff1 * w1 * w1);
 }
 
-// acc[l] += w * p[l] for Z complex samples read as Z/2 float4
-template <int Z>
-__device__ __forceinline__ void zload_fma(float2 (&acc)[Z], float w, const float2* __restrict__ p) {
-  const float4* q = reinterpret_cast<const float4*>(p);
-#pragma unroll
-  for (int i = 0; i < Z / 2; ++i) {
-    const float4 v = __ldg(&q[i]);
-    acc[2 * i].x += w * v.x;
-    acc[2 * i].y += w * v.y;
-    acc[2 * i + 1].x += w * v.z;
-    acc[2 * i + 1].y += w * v.w;
-  }
-}
-
 // ------------------------------------------------------ 1: rows (R)
 // obj [nz, n, n] -> fa [zb][n][2n][Z];  grid (n, nzb)
 template <int N2>
