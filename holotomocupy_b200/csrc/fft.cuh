@@ -14,6 +14,8 @@
 #pragma once
 #include "common.cuh"
 
+#include <type_traits>
+
 namespace ht {
 
 // ------------------------------------------------------- small DFT kernels
@@ -88,6 +90,10 @@ struct SmRow {
   static __host__ __device__ constexpr int padded(int n) { return n + (n >> 4); }
   __device__ __forceinline__ float2 ld(int k) const { return p[k + (k >> 4)]; }
   __device__ __forceinline__ void st(int k, float2 v) const { p[k + (k >> 4)] = v; }
+  // sample k + 16 m sits 17 m slots after sample k: a stage whose strides are
+  // multiples of 16 forms one padded index per butterfly and adds constants
+  __device__ __forceinline__ float2 ld_pad(int pk) const { return p[pk]; }
+  __device__ __forceinline__ void st_pad(int pk, float2 v) const { p[pk] = v; }
 };
 
 // Column line inside a [N][C] tile (row-major, C columns side by side).  For
@@ -219,8 +225,14 @@ __device__ __forceinline__ void fft_stage(float2 (&v)[E], const SM& sm, int t,
 #pragma unroll
   for (int s = 0; s < NB; ++s) {
     const int b = t + s * T;
+    if constexpr (std::is_same<SM, SmRow>::value && NR % 16 == 0) {
+      const int pb = b + (b >> 4);
 #pragma unroll
-    for (int j = 0; j < R; ++j) v[s * R + j] = sm.ld(b + j * NR);
+      for (int j = 0; j < R; ++j) v[s * R + j] = sm.ld_pad(pb + j * (NR + NR / 16));
+    } else {
+#pragma unroll
+      for (int j = 0; j < R; ++j) v[s * R + j] = sm.ld(b + j * NR);
+    }
   }
 #pragma unroll
   for (int s = 0; s < NB; ++s) {
@@ -239,8 +251,15 @@ __device__ __forceinline__ void fft_stage(float2 (&v)[E], const SM& sm, int t,
   for (int s = 0; s < NB; ++s) {
     const int b = t + s * T;
     const int i = (P > 1) ? (b % P) : 0;
+    if constexpr (std::is_same<SM, SmRow>::value && P % 16 == 0) {
+      const int k0 = (b - i) * R + i;
+      const int pk = k0 + (k0 >> 4);
 #pragma unroll
-    for (int j = 0; j < R; ++j) sm.st((b - i) * R + i + j * P, v[s * R + j]);
+      for (int j = 0; j < R; ++j) sm.st_pad(pk + j * (P + P / 16), v[s * R + j]);
+    } else {
+#pragma unroll
+      for (int j = 0; j < R; ++j) sm.st((b - i) * R + i + j * P, v[s * R + j]);
+    }
   }
   if constexpr (SYNC_END) sync();
 }
