@@ -21,9 +21,17 @@ time through the plain path, with p50/p99 per-iteration latencies.
 
 `--impl reference` times the reference algorithm's CPU implementation (the
 NumPy port in oracle/, FP32, all host cores) on a bounded sample of the same
-workload: the per-angle BH cascades (one gradient and three Hessian cascades,
-as rec_mpi.py runs them) for one angle and R + R^T for one slice, scaled to
-900 angles and 512 slices.
+workload: each step runs the per-angle BH cascades (one gradient and three
+Hessian cascades, as rec_mpi.py runs them) for a block of angles -- the steps
+walk through distinct angles spread over [0, pi) -- and R + R^T for one slice,
+scaled to 900 angles and 512 slices (`ms_per_step` is that extrapolation; the
+measured seconds are reported beside it).  It also runs one whole BH
+iteration of the small chain (128^3, 180 angles, 4 distances) end to end,
+unscaled.
+
+`--prop` compares the library's propagator with the padded-grid path on
+torch's cuFFT (the reference's CuPy branch) at 1024^2 x 4 images (the
+reference test script's size), 512^2 and 2048^2.
 """
 import argparse
 import gc
@@ -45,6 +53,13 @@ UNIT = "BH iterations/s"
 DIST = np.array([3e-3, 4e-3, 5e-3, 6e-3])
 WAVELENGTH = 7.3e-11
 VOXEL = 20e-9
+
+
+def bench_config(n, ntheta, ndist, world):
+    """The workload description both arms print (the same dict)."""
+    return {"workload": f"one BH iteration, {n}^3 object, {ntheta} angles, {ndist} distances, {n}^2 detector",
+            "n": n, "ntheta": ntheta, "ndist": ndist, "parallelism": f"replicas x{world}",
+            "l2": "inputs larger than L2 (state ~60 GB)"}
 
 
 def workload_args(n, ntheta, ndist, niter=10 ** 6):
@@ -105,25 +120,37 @@ class ClockSampler:
 
 
 # ----------------------------------------------------------- CPU (oracle)
-def cpu_sample(n, ntheta, ndist, threads):
-    """Seconds per BH iteration of the reference algorithm on the host, from a
-    one-angle cascade sample and a one-slice R/RT sample (scaled)."""
+def _oracle(threads):
     os.environ["HOLO_ORACLE_WORKERS"] = str(threads)
     from oracle import holo_oracle as O
     O._WORKERS = threads
+    return O
+
+
+def cpu_sample(n, ntheta, ndist, threads, angles=None):
+    """Seconds per BH iteration of the reference algorithm on the host: the
+    per-angle cascades (1 gradient + 3 Hessian, as rec_mpi.py runs them) of the
+    given angles (indices into the ntheta angles; default the first) and R, R^T
+    of one slice, scaled linearly to ntheta angles and n slices.  Returns
+    (seconds per iteration, measured seconds, description)."""
+    O = _oracle(threads)
     rng = np.random.default_rng(0)
-    a = workload_args(n, 1, ndist)
-    a.theta = a.theta[:1]
+    th_all = workload_args(n, ntheta, ndist).theta
+    idx = np.asarray([0] if angles is None else angles)
+    na = len(idx)
+    a = workload_args(n, na, ndist)
+    a.theta = th_all[idx]
     rec = O.Rec(a, "complex64")
     rec.eff_demagnifications[:] = 1
     rec.data[:] = 1.0
-    v = {"prb": np.ones((ndist, n, n), "complex64"), "proj": (0.01 * rng.standard_normal((1, n, n))).astype("complex64"),
-         "pos": rng.uniform(-2, 2, (1, ndist, 2)).astype("float32")}
+    v = {"prb": np.ones((ndist, n, n), "complex64"),
+         "proj": (0.01 * rng.standard_normal((na, n, n))).astype("complex64"),
+         "pos": rng.uniform(-2, 2, (na, ndist, 2)).astype("float32")}
     g = {"prb": (0.01 * rng.standard_normal((ndist, n, n))).astype("complex64"),
-         "proj": (0.01 * rng.standard_normal((1, n, n))).astype("complex64"),
-         "pos": rng.uniform(-1, 1, (1, ndist, 2)).astype("float32")}
+         "proj": (0.01 * rng.standard_normal((na, n, n))).astype("complex64"),
+         "pos": rng.uniform(-1, 1, (na, ndist, 2)).astype("float32")}
     e = {k: x.copy() for k, x in g.items()}
-    tomo = O.Tomo(n, 1, workload_args(n, ntheta, ndist).theta, 0, "complex64")
+    tomo = O.Tomo(n, 1, th_all, 0, "complex64")
     x = (0.01 * rng.standard_normal((1, n, n))).astype("complex64")
     t0 = time.perf_counter()
     rec.gradients_cascade(v, g)
@@ -134,32 +161,73 @@ def cpu_sample(n, ntheta, ndist, threads):
     y = tomo.R(x)
     tomo.RT(y)
     t2 = time.perf_counter()
-    per_iter = (t1 - t0) * ntheta + (t2 - t1) * n
-    sample = (f"reference-structure BH cascades (1 gradient + 3 Hessian) for 1 of {ntheta} angles at "
+    per_iter = (t1 - t0) * ntheta / na + (t2 - t1) * n
+    sample = (f"reference-structure BH cascades (1 gradient + 3 Hessian) for {na} of {ntheta} angles at "
               f"{n}x{n}x{ndist}, plus R and R^T of 1 of {n} slices, scaled linearly; FP32 NumPy/SciPy oracle")
     return per_iter, t2 - t0, sample
 
 
-def run_reference(a, rank):
+def cpu_small_chain_iteration(threads, n=128, ntheta=180, ndist=4):
+    """Two whole BH iterations of the small chain (n^3, ntheta angles, ndist
+    distances) on the host, unscaled: gradient with R^T, R of the gradient,
+    the Hessian forms for the step sizes, the updates (the FP32 oracle's BH,
+    rec_mpi.py:163-227).  Returns measured seconds."""
+    O = _oracle(threads)
+    from holotomocupy_b200.synthetic import ellipsoid_phantom
+    args = workload_args(n, ntheta, ndist, niter=2)
+    rec = O.Rec(args, "complex64")
+    rng = np.random.default_rng(1)
+    rec.eff_demagnifications[:] = 1
+    rec.vars["obj"][:] = ellipsoid_phantom(n, 20, 11, device="cpu").numpy()
+    rec.vars["prb"][:] = 1
+    rec.vars["pos"][:] = rng.uniform(-2, 2, (ntheta, ndist, 2))
+    rec.gen_sqrt_data(rec.vars, rec.data)
+    rec.eff_demagnifications[:] = 0
+    rec.vars["obj"][:] = 0
+    t0 = time.perf_counter()
+    rec.BH(niter=2)          # the first iteration (no beta) and one steady-state iteration
+    t1 = time.perf_counter()
+    return {"two_iterations_s": t1 - t0}
+
+
+def run_reference(a, rank, budget_s=100.0):
+    """The reference arm: rank 0 alone (other ranks exit without work)."""
     if rank != 0:
         return
     threads = os.cpu_count() or 1
     n, ntheta, ndist = a.size, a.ntheta, 4
-    for _ in range(a.warmup):
-        cpu_sample(n, ntheta, ndist, threads)
-    per = []
-    for _ in range(a.steps):
-        p, _, sample = cpu_sample(n, ntheta, ndist, threads)
-        per.append(p)
+    # one angle first, to size the per-step angle block within the time budget
+    t_cal = cpu_sample(n, ntheta, ndist, threads)[1]
+    steps = a.warmup + a.steps
+    per_angle = max(t_cal, 1e-3)
+    na = int(max(1, min(90, budget_s / steps / per_angle)))
+    # the steps walk through distinct angles spread over the 900
+    order = np.random.default_rng(0).permutation(ntheta)
+    blocks = [np.sort(order[(k * na) % ntheta: (k * na) % ntheta + na]) for k in range(steps)]
+    per, measured = [], []
+    for k in range(steps):
+        p, w, sample = cpu_sample(n, ntheta, ndist, threads, blocks[k])
+        if k >= a.warmup:
+            per.append(p)
+            measured.append(w)
+    c1 = None if a.no_small_chain else cpu_small_chain_iteration(threads)
     ms = float(np.mean(per)) * 1e3
     value = 1e3 / ms
+    distinct = len(np.unique(np.concatenate(blocks[a.warmup:])))
+    sample = (f"per step: the BH cascades (1 gradient + 3 Hessian, rec_mpi.py's structure) of {na} of {ntheta} "
+              f"angles and R + R^T of 1 of {n} slices at {n}^2 x {ndist} distances, scaled linearly to the whole "
+              f"iteration; the {a.steps} timed steps cover {distinct} distinct angles; FP32 NumPy/SciPy oracle")
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup,
-            "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c64",
-            "data": "synthetic", "impl": "reference",
-            "config": {"workload": f"one BH iteration, {n}^3 object, {ntheta} angles, {ndist} distances, {n}^2 detector",
-                       "n": n, "ntheta": ntheta, "ndist": ndist},
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
-            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "ms_per_step": ms, "ms_per_step_is": "extrapolated from the sampled angles and slice",
+            "measured_s_per_step": float(np.mean(measured)), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "c64", "data": "synthetic", "impl": "reference",
+            "config": bench_config(n, ntheta, ndist, a.gpus),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample,
+                             "angles_per_step": na, "distinct_angles_timed": distinct},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "small_chain_measured": None if c1 is None else {
+                "workload": "two whole BH iterations at 128^3, 180 angles, 4 distances, unscaled (the first and "
+                            "one steady-state iteration)", **c1, "iters_per_s": 2.0 / c1["two_iterations_s"]}}
     print(json.dumps(line), flush=True)
 
 
@@ -226,6 +294,11 @@ def main():
     ap.add_argument("--c5", action="store_true",
                     help="the 2048^3 x 1800 x 4 operator measurement (D, R, R^T on a 256-slice sub-volume) "
                          "instead of the BH line")
+    ap.add_argument("--prop", action="store_true",
+                    help="the propagator against the padded-grid path on torch's cuFFT (1024^2 x 4, 512^2, 2048^2) "
+                         "instead of the BH line")
+    ap.add_argument("--no-small-chain", action="store_true",
+                    help="reference arm: skip the unscaled small-chain BH iterations")
     ap.add_argument("--profile", action="store_true",
                     help="time the device iterations only (no roofline, e2e or CPU legs): for ncu launch lists")
     a = ap.parse_args()
@@ -240,6 +313,9 @@ def main():
         return
     if a.c5:
         run_c5(a)
+        return
+    if a.prop:
+        run_prop(a)
         return
 
     import torch
@@ -346,11 +422,9 @@ def main():
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
         "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c64",
         "data": "synthetic (seeded ellipsoid phantom, random probe and positions, Poisson noise at 1e4 photons)",
-        "config": {"workload": f"one BH iteration, {n}^3 object, {ntheta} angles, {ndist} distances, {n}^2 detector",
-                   "n": n, "ntheta": ntheta, "ndist": ndist, "parallelism": f"replicas x{world}",
-                   "form": "served: device step sizes, iteration replayed from a CUDA graph",
-                   "l2": "inputs larger than L2 (state ~60 GB)", "latency_ms_p50": float(np.percentile(per_lat, 50)),
-                   "latency_ms_p99": float(np.percentile(per_lat, 99))},
+        "config": bench_config(n, ntheta, ndist, world),
+        "form": "served: device step sizes, iteration replayed from a CUDA graph",
+        "latency_ms_p50": float(np.percentile(per_lat, 50)), "latency_ms_p99": float(np.percentile(per_lat, 99)),
         "plain": {"value": replica_value(ms_plain, world), "unit": UNIT, "ms_per_step": ms_plain,
                   "latency_ms_p50": float(np.percentile(lat_plain, 50)),
                   "latency_ms_p99": float(np.percentile(lat_plain, 99)),
@@ -433,6 +507,67 @@ def run_c5(a, n=2048, ntheta=1800, ndist=4, nz_sub=256, nimg_chunk=256):
             "config": {"workload": "D over 256-image chunks of 2048^2; R, R^T of a 256-slice 2048^2 sub-volume at "
                                    "1800 angles", "n": n, "ntheta": ntheta, "ndist": ndist},
             "operators": out}
+    print(json.dumps(line), flush=True)
+
+
+def run_prop(a):
+    """The library's propagator (DCT form, ht_prop_D / ht_prop_DT) against the
+    padded-grid path on torch's cuFFT -- the reference's CuPy branch
+    (propagation.py:77-86, 98-110), the stand-in for its cuFFTDx path -- and the
+    library's own padded-grid convolution (ht_conv2d_run, the surface of the
+    cuFFTDx conv2d_run).  CUDA events around `steps` back-to-back calls after
+    `warmup` calls; algorithmic bytes of D: 16 B n nz + 32 B n nz (table)."""
+    import torch
+    from holotomocupy_b200 import Propagation
+    dev = torch.device("cuda", 0)
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    peak = float(peaks.get("hbm_gbs", 6650.0))
+    g = torch.Generator(device=dev).manual_seed(6)
+
+    def timed(fn):
+        for _ in range(a.warmup):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(a.steps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / a.steps
+
+    rows = []
+    for n, batch in ((1024, 4), (512, 64), (1024, 32), (2048, 16)):
+        cl = Propagation(n, n, batch, 4, WAVELENGTH, VOXEL, DIST)
+        ref = Propagation(n, n, batch, 4, WAVELENGTH, VOXEL, DIST)
+        ref._use_cufftdx = False
+        x = torch.randn(batch, n, n, dtype=torch.complex64, device=dev, generator=g)
+        err = float(torch.abs(cl.D(x, 0) - ref.D(x, 0)).max() / torch.abs(ref.D(x, 0)).max())
+        pad = torch.empty(batch, 2 * n, 2 * n, dtype=torch.complex64, device=dev)
+        cl._fwd_pad(x, pad)
+        ybuf = torch.empty_like(pad)
+        r = {"n": n, "images": batch,
+             "D_ms": timed(lambda: cl.D(x, 0)), "DT_ms": timed(lambda: cl.DT(x, 0)),
+             "cufft_D_ms": timed(lambda: ref.D(x, 0)), "cufft_DT_ms": timed(lambda: ref.DT(x, 0)),
+             "conv2d_run_ms": timed(lambda: cl._conv2d.run(pad, cl.fker[0], ybuf)),
+             "max_rel_diff_D": err}
+        alg = 16.0 * batch * n * n + 32.0 * n * n
+        r["D_achieved_gbs"] = alg / (r["D_ms"] * 1e-3) / 1e9
+        r["D_frac"] = r["D_achieved_gbs"] / peak
+        r["speedup_D"] = r["cufft_D_ms"] / r["D_ms"]
+        r["speedup_DT"] = r["cufft_DT_ms"] / r["DT_ms"]
+        rows.append(r)
+        del cl, ref, x, pad, ybuf
+        torch.cuda.empty_cache()
+    line = {"metric": "Fresnel propagator D / D^T time: library vs padded-grid torch cuFFT", "unit": "ms",
+            "value": rows[0]["D_ms"], "higher_is_better": False, "steps": a.steps, "warmup": a.warmup,
+            "n_gpus": 1, "dtype": "c64", "data": "synthetic (seeded normal complex64)", "peak_gbs": peak,
+            "peak_source": "measured" if peaks else "fallback",
+            "config": {"workload": "D and D^T at distance 3 mm, 7.3e-11 m, 20 nm pixels"}, "rows": rows}
     print(json.dumps(line), flush=True)
 
 

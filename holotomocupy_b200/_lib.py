@@ -25,18 +25,23 @@ SIGNATURES = {
     "ht_prop_destroy": [_vp],
     "ht_prop_D": [_vp, _vp, _vp, _c_long, _c_int, _vp],
     "ht_prop_DT": [_vp, _vp, _vp, _c_long, _c_int, _vp],
+    "ht_conv2d_create": [_c_int, _c_int, ctypes.POINTER(_vp)],
+    "ht_conv2d_destroy": [_vp],
+    "ht_conv2d_run": [_vp, _vp, _vp, _vp, _c_long, _vp],
+    "ht_pad_mirror": [_vp, _vp, _c_long, _c_int, _c_int, _vp],
+    "ht_pad_fold": [_vp, _vp, _c_long, _c_int, _c_int, _vp],
     "ht_tomo_create": [_c_int, _c_int, _c_int, _vp, _vp, ctypes.POINTER(_vp)],
     "ht_tomo_destroy": [_vp],
     "ht_tomo_R": [_vp, _vp, _vp, _c_int, _vp],
     "ht_tomo_RT": [_vp, _vp, _vp, _c_int, _vp],
     "ht_tomo_R_coeffx": [_vp, _vp, _vp, _c_int, _vp],
-    "ht_tomo_RT_coeffx": [_vp, _vp, _vp, _c_int, _vp],
+    "ht_tomo_RT_coeffx": [_vp, _vp, _vp, _c_int, _c_float, _vp],
     "ht_shift_create": [_c_int, _c_int, _c_int, _c_int, _c_int, ctypes.POINTER(_vp)],
     "ht_shift_destroy": [_vp],
     "ht_shift_coeff": [_vp, _vp, _vp, _c_long, _vp],
     "ht_shift_filter": [_vp, _vp, _vp, _c_long, _vp, _vp, _vp],
     "ht_shift_Sback": [_vp, _vp, _vp, _vp, ctypes.c_int, _vp, _c_long, _vp],
-    "ht_shift_coeff_z": [_vp, _vp, _c_long, _vp],
+    "ht_shift_coeff_z": [_vp, _vp, _vp, _c_long, _vp],
     "ht_shift_S": [_vp, _vp, _vp, _vp, _vp, _c_long, _vp],
     "ht_shift_Sadj": [_vp, _vp, _vp, _vp, _vp, _c_long, _vp],
     "ht_shift_dS": [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _c_long, _vp],
@@ -59,7 +64,7 @@ SIGNATURES = {
     "ht_rec_create": [_c_int, _c_int, _c_int, _c_int, _c_int, _c_int, _c_int, _vp, ctypes.POINTER(_vp)],
     "ht_rec_destroy": [_vp],
     "ht_rec_forward": [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
-    "ht_rec_gradient": [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
+    "ht_rec_gradient": [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _c_float, _c_float, _vp],
     "ht_rec_objective_noalloc": [_vp, _c_int, _c_int, _c_int, _c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
     "ht_rec_hessian": [_vp, _vp, _vp, _vp, _vp, _vp, _c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
 }
@@ -104,6 +109,11 @@ def stream_ptr(device=None):
 
 
 def ptr(t):
+    """Device address of a tensor's storage.  A lazily conjugated or negated
+    view (torch's conj/neg bits) would hand the kernel the unconjugated data,
+    so such views are refused: resolve_conj() / resolve_neg() them first."""
+    if t.is_conj() or t.is_neg():
+        raise ValueError("lazily conjugated/negated tensor: call resolve_conj()/resolve_neg() before passing it")
     return _vp(t.data_ptr())
 
 

@@ -6,10 +6,10 @@ streams.  ``gpu_batch(axis_out, axis_inp, nout, inp_pad)`` decorates a
 function ``f(cl, out1, ..., inp1, ...)`` written for device arrays so that it
 also takes host (NumPy) arrays larger than the device: the arrays whose
 ``shape[axis]`` equals the chunked size ("proper" arguments, outputs first)
-are streamed through the pool ``chunk`` rows at a time -- host-to-device copy
-of chunk k, compute of chunk k-1 and device-to-host copy of chunk k-2 on
-three streams at once, double-buffered -- while the other arguments are
-passed whole (NumPy ones copied to the device once).  With ``inp_pad`` the
+are streamed through the pool ``chunk`` rows at a time -- the host-to-device
+copies, the compute and the device-to-host copies of consecutive chunks
+overlap on three streams, double-buffered and ordered by events only -- while
+the other arguments are passed whole (NumPy ones copied to the device once).  With ``inp_pad`` the
 first input holds ``size + inp_pad`` rows and every chunk receives
 ``chunk + inp_pad`` of them (a halo).  Without any host array the function
 runs directly.  These are the reference's argument rules (chunking.py:12-98).
@@ -153,7 +153,7 @@ class Chunking:
     # --------------------------------------------------------------- run
     def run(self, cl, out, inp, proper_inp, nonproper_inp, proper_out, nonproper_out, axis_out, axis_inp, func,
             inp_pad=0):
-        """chunking.py:100-200: the three-stage pipeline over the chunks."""
+        """The pipeline over the chunks (the work of chunking.py:100-200)."""
         size = inp[0].shape[axis_inp] - inp_pad
         nchunk = (size + self.chunk - 1) // self.chunk
         out_gpu, off = self._buffers(out[:proper_out], axis_out, 0, self.chunk)
@@ -197,25 +197,44 @@ class Chunking:
             func(cl, *oc, *out[proper_out:], *ic, *inp[proper_inp:proper_inp + nonproper_inp],
                  *inp[proper_inp + nonproper_inp:])
 
+        # The chunks flow through three streams -- copy in, compute, copy out --
+        # ordered only by events, so the host issues every chunk's work in one
+        # pass and waits once, at the end.  Buffer set b = k % 2 is reused by
+        # chunk k + 2: its copy-in waits until chunk k's compute has read the
+        # inputs, its compute until chunk k's copy-out has drained the outputs.
+        s_in, s_comp, s_out = self.stream
         cur = torch.cuda.current_stream(self.device)
-        for s in self.stream:
-            s.wait_stream(cur)   # device inputs written before the call are visible
+        for st in self.stream:
+            st.wait_stream(cur)   # device inputs written before the call are visible
+        ev = lambda: torch.cuda.Event()
+        loaded, computed, drained = [None] * nchunk, [None] * nchunk, [None] * nchunk
         try:
-            for k in range(nchunk + 2):
-                if k < nchunk:
-                    with torch.cuda.stream(self.stream[k % 3]):
-                        p2g(k % 2, k)
-                if 0 < k < nchunk + 1:
-                    with torch.cuda.stream(self.stream[(k - 1) % 3]):
-                        compute((k - 1) % 2, k - 1)
-                if k > 1:
-                    with torch.cuda.stream(self.stream[(k - 2) % 3]):
-                        g2p((k - 2) % 2, k - 2)
-                for s in self.stream:
-                    s.synchronize()
+            for k in range(nchunk):
+                b = k % 2
+                with torch.cuda.stream(s_in):
+                    if k >= 2:
+                        s_in.wait_event(computed[k - 2])
+                    p2g(b, k)
+                    loaded[k] = ev()
+                    loaded[k].record(s_in)
+                with torch.cuda.stream(s_comp):
+                    s_comp.wait_event(loaded[k])
+                    if k >= 2:
+                        s_comp.wait_event(drained[k - 2])
+                    compute(b, k)
+                    computed[k] = ev()
+                    computed[k].record(s_comp)
+                with torch.cuda.stream(s_out):
+                    s_out.wait_event(computed[k])
+                    g2p(b, k)
+                    drained[k] = ev()
+                    drained[k].record(s_out)
         finally:
-            for s in self.stream:
-                s.synchronize()
+            # host outputs must be complete before the call returns (and before
+            # the host pages are unlocked); device outputs follow on `cur`
+            for st in self.stream:
+                st.synchronize()
+            cur.wait_stream(s_comp)
             pin.close()
 
     # ------------------------------------------- batched BLAS-1 (chunking.py:233-290)

@@ -77,12 +77,14 @@ __global__ void __launch_bounds__(kBlasThreads) k_axpby_dev(float* __restrict__ 
 //   top = -(dots[0]/rho_obj + dots[1]/rho_pos + dots[2]/rho_prb),
 //   bottom = first ? H[0] : beta^2 H[2] - 2 beta H[3] + H[0];
 //   (alpha, beta) is appended to hist[*count] while *count < cap.
-__global__ void k_bh_scalars(const double* __restrict__ H, const double* __restrict__ dots, int first, int phase,
+__global__ void k_bh_scalars(const double* __restrict__ H, double* __restrict__ dots, int first, int phase,
                              double rho_obj, double rho_pos, double rho_prb, double* __restrict__ scal,
                              double* __restrict__ hist, int cap, int* __restrict__ count) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   if (phase == 0) {
     scal[0] = first ? 0.0 : H[1] / H[2];
+    if (dots)  // the direction updates that follow accumulate into them
+      for (int i = 0; i < 3; ++i) dots[i] = 0.0;
     return;
   }
   const double beta = scal[0];
@@ -169,7 +171,7 @@ extern "C" int ht_axpby_dev(void* x, const void* y, const double* A, float sa, c
   return kOk;
 }
 
-extern "C" int ht_bh_scalars(const double* H, const double* dots, int first, int phase, double rho_obj,
+extern "C" int ht_bh_scalars(const double* H, double* dots, int first, int phase, double rho_obj,
                              double rho_pos, double rho_prb, double* scal, double* hist, int cap, int* count,
                              void* stream) {
   using namespace ht;

@@ -708,7 +708,7 @@ k_casc_adj(const float2* __restrict__ tmp, float2* __restrict__ Pc, T* __restric
 // ================================================= probe gradient
 // gprb[k, p] = sum_theta P[theta, k, p]  (gF1, rec_mpi.py:641)
 __global__ void k_sum_theta(const float2* __restrict__ Pc, float2* __restrict__ gprb, long ntheta, int ndist,
-                            long npix) {
+                            long npix, float scale) {
   const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;  // k * npix + p
   if (i >= (long)ndist * npix) return;
   const int k = (int)(i / npix);
@@ -719,7 +719,8 @@ __global__ void k_sum_theta(const float2* __restrict__ Pc, float2* __restrict__ 
     sx += v.x;
     sy += v.y;
   }
-  gprb[i] = make_float2((float)sx, (float)sy);
+  // the float sum times the variable scaling (rec_mpi.py:345: y[0] * rho_sq['prb'])
+  gprb[i] = make_float2((float)sx * scale, (float)sy * scale);
 }
 
 // ================================================= object gradient
@@ -773,11 +774,12 @@ k_casc_vsum(T* __restrict__ gc, const T* __restrict__ hbuf, const float* __restr
 }
 
 // gpos[img] = (-Ay, -Ax)  (dsadj, cuda_kernels.py:744-761 with redot)
-__global__ void k_casc_gpos(const double* __restrict__ acc_img, float* __restrict__ gpos, long nimg) {
+// times the variable scaling (rec_mpi.py:347: y[2] * rho_sq['pos'])
+__global__ void k_casc_gpos(const double* __restrict__ acc_img, float* __restrict__ gpos, long nimg, float scale) {
   const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nimg) return;
-  gpos[2 * i + 0] = (float)(-acc_img[i * kNAcc + kAy]);
-  gpos[2 * i + 1] = (float)(-acc_img[i * kNAcc + kAx]);
+  gpos[2 * i + 0] = (float)(-acc_img[i * kNAcc + kAy]) * scale;
+  gpos[2 * i + 1] = (float)(-acc_img[i * kNAcc + kAx]) * scale;
 }
 
 // ================================================ Hessian row pass
@@ -1250,7 +1252,8 @@ static cudaError_t resid_pass(ht_rec_s* r, const float* data, float* amp, float 
 
 template <int N, class T>
 static cudaError_t grad_impl(ht_rec_s* r, const void* c, const float* pos, const float* mag, const float2* prb,
-                             const float* data, void* gc, float* gpos, float2* gprb, float scale, cudaStream_t st) {
+                             const float* data, void* gc, float* gpos, float2* gprb, float scale, float spos,
+                             float sprb, cudaStream_t st) {
   const float2 *hw, *twn, *twz;
   prop_tables(r->prop, &hw, &twn, &twz);
   cudaError_t e = fwd_pass<N, T>(r, c, pos, mag, prb, hw, twn, twz, st);
@@ -1277,10 +1280,13 @@ static cudaError_t grad_impl(ht_rec_s* r, const void* c, const float* pos, const
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   if ((e = reduce_rows(r, 5, kAx, 0, 5, 0, 0, st)) != cudaSuccess) return e;
   const long npix = (long)r->D.nz * N;
-  k_sum_theta<<<(unsigned)((r->D.ndist * npix + 255) / 256), 256, 0, st>>>(r->P, gprb, r->ntheta, r->D.ndist, npix); ::ht::count_launch();
+  k_sum_theta<<<(unsigned)((r->D.ndist * npix + 255) / 256), 256, 0, st>>>(r->P, gprb, r->ntheta, r->D.ndist, npix,
+                                                                             sprb);
+  ::ht::count_launch();
   dim3 g2((r->D.nobj + 31) / 32, (r->D.nzobj + 8 * kVRows - 1) / (8 * kVRows), r->ntheta);
   k_casc_vsum<T><<<g2, dim3(32, 8), 0, st>>>((T*)gc, hbuf, pos, mag, r->D); ::ht::count_launch();
-  k_casc_gpos<<<(unsigned)((r->D.nimg + 255) / 256), 256, 0, st>>>(r->acc_img, gpos, r->D.nimg); ::ht::count_launch();
+  k_casc_gpos<<<(unsigned)((r->D.nimg + 255) / 256), 256, 0, st>>>(r->acc_img, gpos, r->D.nimg, spos);
+  ::ht::count_launch();
   return cudaGetLastError();
 }
 
@@ -1356,7 +1362,8 @@ extern "C" int ht_rec_forward(ht_rec_s* r, const void* c, const float* pos, cons
 }
 
 extern "C" int ht_rec_gradient(ht_rec_s* r, const void* c, const float* pos, const float* mag, const void* prb,
-                               const float* data, void* gc, float* gpos, void* gprb, double* fval, void* stream) {
+                               const float* data, void* gc, float* gpos, void* gprb, double* fval, float scale_pos,
+                               float scale_prb, void* stream) {
   using namespace ht;
   HT_REQUIRE(r && c && pos && mag && prb && data && gc && gpos && gprb, "ht_rec_gradient: null pointer");
   cudaStream_t st = static_cast<cudaStream_t>(stream);
@@ -1369,9 +1376,9 @@ extern "C" int ht_rec_gradient(ht_rec_s* r, const void* c, const float* pos, con
 #define X(S)                                                                                                     \
   case S:                                                                                                        \
     e = r->is_complex ? grad_impl<S, float2>(r, c, pos, mag, (const float2*)prb, data, gc, gpos, (float2*)gprb,    \
-                                             scale, st)                                                          \
+                                             scale, scale_pos, scale_prb, st)                                    \
                       : grad_impl<S, float>(r, c, pos, mag, (const float2*)prb, data, gc, gpos, (float2*)gprb,     \
-                                            scale, st);                                                          \
+                                            scale, scale_pos, scale_prb, st);                                    \
     break;
     HT_REC_SIZES(X)
 #undef X
@@ -1459,12 +1466,15 @@ unsigned char* noalloc_scratch(int device) {
 template <int N, class T>
 static cudaError_t noalloc_chunks(const ht_prop_s* prop, int nz, int nobj, int nzobj, int ndist, int ntheta,
                                   int per_chunk, const T* c, const float* pos, const float* mag, const float2* prb,
-                                  const float* data, double* acc, float2* tmp, cudaStream_t st) {
+                                  const float* data, double* acc, float2* tmp, double* rows, double* imgs,
+                                  cudaStream_t st) {
   const float2 *hw, *twn, *twz;
   prop_tables(prop, &hw, &twn, &twz);
   using CF = RowCfg<N>;
-  const int smr = CF::SMEM + CF::THREADS * (int)sizeof(double);
-  cudaError_t e = allow_smem(k_casc_resid<N, 1>, smr);
+  const int smr = CF::SMEM + red_doubles<CF::T>(1, CF::THREADS) * (int)sizeof(double);
+  cudaError_t e = N == kR512 ? cudaSuccess : allow_smem(k_casc_resid<N, 1>, smr);
+  // chunks in angle order, each chunk's per-row sums reduced in a fixed order:
+  // the objective is the same bit for bit on every call
   for (int th0 = 0; th0 < ntheta && e == cudaSuccess; th0 += per_chunk) {
     const int nt = std::min(per_chunk, ntheta - th0);
     const CascDims D{N, nz, nobj, nzobj, ndist, (long)nt * ndist};
@@ -1473,8 +1483,19 @@ static cudaError_t noalloc_chunks(const ht_prop_s* prop, int nz, int nobj, int n
                          tmp, twn, st);
     if (e != cudaSuccess) break;
     if ((e = dct_cols(nz, false, tmp, D.nimg, N, hw, ndist, twz, st)) != cudaSuccess) break;
-    k_casc_resid<N, 1><<<HT_ROWS_GRID(N, nrows), CF::THREADS, smr, st>>>(
-        tmp, nullptr, data + (long)th0 * ndist * nz * N, nullptr, acc, nullptr, 0.f, D, twn);
+    const float* dch = data + (long)th0 * ndist * nz * N;
+    if constexpr (N == kR512) {
+      k_casc_resid512<1><<<(unsigned)((nrows + kR512Lines - 1) / kR512Lines), 32 * kR512Lines, 0, st>>>(
+          tmp, nullptr, dch, nullptr, acc, rows, 0.f, D, twn);
+    } else {
+      k_casc_resid<N, 1><<<HT_ROWS_GRID(N, nrows), CF::THREADS, smr, st>>>(tmp, nullptr, dch, nullptr, acc, rows,
+                                                                             0.f, D, twn);
+    }
+    count_launch();
+    if ((e = cudaGetLastError()) != cudaSuccess) break;
+    k_rows_img<<<(unsigned)D.nimg, kRedThreads, 0, st>>>(rows, 1, nz, imgs, nullptr, 0, 0, 0);
+    count_launch();
+    k_imgs_glob<<<1, kRedThreads, 0, st>>>(imgs, 1, D.nimg, acc, kF);
     count_launch();
     e = cudaGetLastError();
   }
@@ -1498,11 +1519,13 @@ extern "C" int ht_rec_objective_noalloc(ht_prop_s* prop, int nobj, int nzobj, in
     set_error("ht_rec_objective_noalloc: n must be one of 32, 64, 128, 256, 384, 512, 768, 1024, 2048");
     return kUnsupported;
   }
-  const size_t per_angle = sizeof(float2) * (size_t)ndist * nz * n;
+  // per angle: its images (ndist*nz*n complex64), their per-row sums
+  // (ndist*nz doubles) and per-image sums (ndist doubles)
+  const size_t per_angle = sizeof(float2) * (size_t)ndist * nz * n + sizeof(double) * (size_t)ndist * (nz + 1);
   const size_t room = kNoAllocBytes - kNoAllocAccBytes;
   if (per_angle > room) {
     set_error("ht_rec_objective_noalloc: one angle needs " + std::to_string(per_angle) +
-              " bytes of scratch (ndist*nz*n*8); the fixed scratch holds " + std::to_string(room) +
+              " bytes of scratch (ndist*nz*n*8 + ndist*(nz+1)*8); the fixed scratch holds " + std::to_string(room) +
               " bytes (32 MiB minus 256)");
     return kBadArgument;
   }
@@ -1510,9 +1533,11 @@ extern "C" int ht_rec_objective_noalloc(ht_prop_s* prop, int nobj, int nzobj, in
   HT_CHECK_CUDA(cudaGetDevice(&device));
   unsigned char* base = noalloc_scratch(device);
   if (!base) return kCudaError;
+  const int per_chunk = (int)std::min<size_t>(room / per_angle, (size_t)ntheta);
   double* acc = reinterpret_cast<double*>(base);
   float2* tmp = reinterpret_cast<float2*>(base + kNoAllocAccBytes);
-  const int per_chunk = (int)std::min<size_t>(room / per_angle, (size_t)ntheta);
+  double* rows = reinterpret_cast<double*>(tmp + (size_t)per_chunk * ndist * nz * n);
+  double* imgs = rows + (size_t)per_chunk * ndist * nz;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   // the array keeps the previous call's contents: clear the accumulators
   HT_CHECK_CUDA(cudaMemsetAsync(acc, 0, kNoAllocAccBytes, st));
@@ -1521,9 +1546,9 @@ extern "C" int ht_rec_objective_noalloc(ht_prop_s* prop, int nobj, int nzobj, in
 #define X(S)                                                                                                      \
   case S:                                                                                                         \
     e = is_complex ? noalloc_chunks<S, float2>(prop, nz, nobj, nzobj, ndist, ntheta, per_chunk, (const float2*)c, \
-                                               pos, mag, (const float2*)prb, data, acc, tmp, st)                  \
+                                               pos, mag, (const float2*)prb, data, acc, tmp, rows, imgs, st)     \
                    : noalloc_chunks<S, float>(prop, nz, nobj, nzobj, ndist, ntheta, per_chunk, (const float*)c,   \
-                                              pos, mag, (const float2*)prb, data, acc, tmp, st);                  \
+                                              pos, mag, (const float2*)prb, data, acc, tmp, rows, imgs, st);     \
     break;
     HT_REC_SIZES(X)
 #undef X

@@ -17,6 +17,6 @@ void prop_tables(const ht_prop_s* p, const float2** hw, const float2** twn, cons
 namespace ht {
 cudaError_t symbol_rows(int N, const float2* in, float2* out, long nrows, const float* sym, const float2* tw,
                         cudaStream_t st);
-cudaError_t symbol_cols(int N, float2* data, long nimg, int ncols, const float* sym, const float2* tw,
-                        cudaStream_t st);
+cudaError_t symbol_cols(int N, const float2* in, float2* out, long nimg, int ncols, const float* sym,
+                        const float2* tw, cudaStream_t st);
 }  // namespace ht

@@ -40,6 +40,24 @@ inline cudaError_t allow_smem(K kernel, int bytes) {
   return e;
 }
 
+// A column of a [rows, ncols] image in global memory, as a line view for the
+// first (GColIn) or last (GColOut) stage of a column transform; an invalid
+// column (past the image's edge) reads zeros and stores nothing.
+struct GColIn {
+  const float2* p;  // row 0 of the column
+  int ncols;
+  bool valid;
+  __device__ __forceinline__ float2 ld(int k) const { return valid ? p[(long)k * ncols] : make_float2(0.f, 0.f); }
+};
+struct GColOut {
+  float2* p;
+  int ncols;
+  bool valid;
+  __device__ __forceinline__ void st(int k, float2 v) const {
+    if (valid) p[(long)k * ncols] = v;
+  }
+};
+
 // Position of input sample g after the even/odd-reversed reordering used by
 // the DCT-II (v[m] = f[2m], v[N-1-m] = f[2m+1]).
 __device__ __forceinline__ int dct_perm_inv(int g, int N) { return (g & 1) ? (N - 1 - (g >> 1)) : (g >> 1); }

@@ -277,13 +277,21 @@ k_shift_dpos(double* __restrict__ acc, const T* __restrict__ c, const T* __restr
 }
 
 // ------------------------------------------- back-projection shift
-// Sback (shift.py:138-148; cuda_kernels.py:294-370, dir = 1): every detector
-// pixel (tx, ty) of image b adds g * phi((dx - jx) / m) phi((dy - jy) / m) to
-// the coefficient cell (iy + jy, ix + jx), the B-spline stretched by the
-// image's magnification m.  The taps run over jx in [ceil(dx - 2m),
-// (int)(dx + 2m)) and likewise jy, as in the reference (whose upper bound
-// drops the last tap of non-zero weight when dx + 2m is not an integer).
-// Cells outside the grid are skipped; contributions meet in float atomics.
+// Sback (shift.py:138-148; cuda_kernels.py:294-370, dir = 1): the detector
+// image g is spread onto the coefficient grid with the B-spline stretched by
+// the image's magnification m.  Pixel (tx, ty) sits at
+// x = (m (tx - n/2) - r_x + (m - 1)/2) + npsi/2 (y likewise), ix = floor(x),
+// dx = x - ix, and reaches the cells ix + jx for jx in [ceil(dx - 2m),
+// (int)(dx + 2m)) with weight phi((dx - jx) / m) (and the same in y; the upper
+// bound drops the last tap of non-zero weight when dx + 2m is not an integer,
+// as the reference has it).
+//
+// Here the transpose is a gather: one thread per coefficient cell finds the
+// pixels whose tap windows contain it -- a window of about 4 + 2/m pixels
+// around the cell's preimage, each tested with the exact membership rule
+// above -- and sums their contributions in a fixed order (rows, then pixels
+// within a row), so the result does not depend on scheduling and every cell
+// is written once (no clearing pass, no atomics).
 __device__ __forceinline__ float sback_phi(float t, float m) {
   t /= m;
   const float a = fabsf(t);
@@ -293,35 +301,61 @@ __device__ __forceinline__ float sback_phi(float t, float m) {
   return 0.f;
 }
 
+// Pixel p's position on the coefficient axis (the reference's float
+// arithmetic) and whether its window reaches cell `cell`; *w is the tap weight.
+__device__ __forceinline__ bool sback_tap(int p, int npix, int ncell, float shift, float m0, int cell, float* w) {
+  const float half = (m0 - 1.0f) / 2.0f;
+  const float x = (m0 * (float)(p - npix / 2) - shift + half) + (float)(ncell / 2);
+  const int ix = (int)floorf(x);
+  const float dx = x - (float)ix;
+  const float span = 2.0f * m0;
+  const int j = cell - ix;
+  if (j < (int)ceilf(dx - span) || j >= (int)(dx + span)) return false;
+  *w = sback_phi(dx - (float)j, m0);
+  return true;
+}
+
+// The pixels whose windows can reach `cell`, padded by two on each side
+// (membership is decided by sback_tap).
+__device__ __forceinline__ void sback_range(int cell, int npix, int ncell, float shift, float m0, int* p0, int* p1) {
+  const float c = -shift + (m0 - 1.0f) / 2.0f + (float)(ncell / 2);
+  const float lo = ((float)cell - 2.0f * m0 - 2.0f - c) / m0 + (float)(npix / 2);
+  const float hi = ((float)cell + 2.0f * m0 + 2.0f - c) / m0 + (float)(npix / 2);
+  *p0 = max(0, (int)floorf(fmaxf(lo, -1.0f)) - 2);
+  *p1 = min(npix - 1, (int)ceilf(fminf(hi, (float)npix)) + 2);
+}
+
 __global__ void k_sback(const float2* __restrict__ g, float2* __restrict__ f, const float* __restrict__ r,
                         const float* __restrict__ mag, int nmag, ShiftDims S, long batch) {
-  const int tx = blockIdx.x * blockDim.x + threadIdx.x;
-  const int ty = blockIdx.y * blockDim.y + threadIdx.y;
+  const int xx = blockIdx.x * blockDim.x + threadIdx.x;
+  const int yy = blockIdx.y * blockDim.y + threadIdx.y;
   const long b = blockIdx.z;
-  if (tx >= S.n || ty >= S.nz || b >= batch) return;
+  if (xx >= S.npsi || yy >= S.nzpsi || b >= batch) return;
   const float m0 = mag[nmag == 1 ? 0 : b];
-  const float half = (m0 - 1.0f) / 2.0f;
-  const float x = (m0 * (float)(tx - S.n / 2) - r[2 * b + 1] + half) + (float)(S.npsi / 2);
-  const float y = (m0 * (float)(ty - S.nz / 2) - r[2 * b + 0] + half) + (float)(S.nzpsi / 2);
-  const int ix = (int)floorf(x), iy = (int)floorf(y);
-  const float dx = x - (float)ix, dy = y - (float)iy;
-  const float span = 2.0f * m0;
-  const float2 v = g[(b * S.nz + ty) * S.n + tx];
-  float2* fb = f + b * (long)S.nzpsi * S.npsi;
-  const int jx0 = (int)ceilf(dx - span), jx1 = (int)(dx + span);
-  for (int jy = (int)ceilf(dy - span); jy < (int)(dy + span); ++jy) {
-    const int yy = iy + jy;
-    if (yy < 0 || yy >= S.nzpsi) continue;
-    const float wy = sback_phi(dy - (float)jy, m0);
-    for (int jx = jx0; jx < jx1; ++jx) {
-      const int xx = ix + jx;
-      if (xx < 0 || xx >= S.npsi) continue;
-      const float w = sback_phi(dx - (float)jx, m0) * wy;
-      float2* cell = fb + (long)yy * S.npsi + xx;
-      atomicAdd(&cell->x, w * v.x);
-      atomicAdd(&cell->y, w * v.y);
+  float2 acc = make_float2(0.f, 0.f);
+  if (m0 > 0.f) {   // m <= 0: the reference's tap ranges are empty
+    const float ry = r[2 * b + 0], rx = r[2 * b + 1];
+    int tx0, tx1, ty0, ty1;
+    sback_range(xx, S.n, S.npsi, rx, m0, &tx0, &tx1);
+    sback_range(yy, S.nz, S.nzpsi, ry, m0, &ty0, &ty1);
+    const float2* gb = g + b * (long)S.nz * S.n;
+    for (int ty = ty0; ty <= ty1; ++ty) {
+      float wy;
+      if (!sback_tap(ty, S.nz, S.nzpsi, ry, m0, yy, &wy)) continue;
+      const float2* grow = gb + (long)ty * S.n;
+      float2 row = make_float2(0.f, 0.f);
+      for (int tx = tx0; tx <= tx1; ++tx) {
+        float wx;
+        if (!sback_tap(tx, S.n, S.npsi, rx, m0, xx, &wx)) continue;
+        const float2 v = __ldg(&grow[tx]);
+        row.x += wx * v.x;
+        row.y += wx * v.y;
+      }
+      acc.x += wy * row.x;
+      acc.y += wy * row.y;
     }
   }
+  f[(b * S.nzpsi + yy) * (long)S.npsi + xx] = acc;
 }
 
 // -------------------------------------------------- prefilter passes
@@ -351,38 +385,21 @@ k_symbol_rows(const float2* in, float2* out, long nrows, const float* __restrict
 // FFT's last stage stores them back (a warp covers 32 / C rows of C adjacent
 // columns per access); the tile passes shared memory only between stages.
 template <int N>
-struct SymColIn {
-  const float2* p;  // row 0 of the column
-  int ncols;
-  bool valid;
-  __device__ __forceinline__ float2 ld(int k) const {
-    return valid ? p[(long)k * ncols] : make_float2(0.f, 0.f);
-  }
-};
-struct SymColOut {
-  float2* p;
-  int ncols;
-  bool valid;
-  __device__ __forceinline__ void st(int k, float2 v) const {
-    if (valid) p[(long)k * ncols] = v;
-  }
-};
-
-template <int N>
 __global__ void __launch_bounds__(ColCfg<N>::THREADS)
-k_symbol_cols(float2* data, int ncols, const float* __restrict__ sym, const float2* __restrict__ tw4) {
+k_symbol_cols(const float2* in, float2* out, int ncols, const float* __restrict__ sym,
+              const float2* __restrict__ tw4) {
   constexpr int C = ColCfg<N>::C;
   constexpr int T = ColCfg<N>::T;
   extern __shared__ float2 tile[];
   const int c = threadIdx.x % C, t = threadIdx.x / C;
   const bool valid = blockIdx.x * C + c < ncols;
   const int col = min((int)blockIdx.x * C + c, ncols - 1);
-  float2* img = data + (long)blockIdx.y * N * ncols + col;
+  const long off = (long)blockIdx.y * N * ncols + col;
   SmCol<C> sm{tile + c};
-  fft_line_from<N, false>(SymColIn<N>{img, ncols, valid}, sm, t, tw4);
+  fft_line_from<N, false>(GColIn{in + off, ncols, valid}, sm, t, tw4);
   for (int k = t; k < N; k += T) sm.st(k, cscale(sm.ld(k), __ldg(&sym[k])));
   __syncthreads();
-  fft_line_to<N, true>(sm, SymColOut{img, ncols, valid}, t, tw4);
+  fft_line_to<N, true>(sm, GColOut{out + off, ncols, valid}, t, tw4);
 }
 
 template <int N>
@@ -397,13 +414,14 @@ static cudaError_t l_symbol_rows(const float2* in, float2* out, long nrows, cons
 }
 
 template <int N>
-static cudaError_t l_symbol_cols(float2* data, long nimg, int ncols, const float* sym, const float2* tw,
-                                 cudaStream_t st) {
+static cudaError_t l_symbol_cols(const float2* in, float2* out, long nimg, int ncols, const float* sym,
+                                 const float2* tw, cudaStream_t st) {
   using CF = ColCfg<N>;
   cudaError_t e = allow_smem(k_symbol_cols<N>, CF::SMEM);
   if (e != cudaSuccess) return e;
-  k_symbol_cols<N><<<dim3((ncols + CF::C - 1) / CF::C, (unsigned)nimg), CF::THREADS, CF::SMEM, st>>>(data, ncols,
-                                                                                                   sym, tw); ::ht::count_launch();
+  k_symbol_cols<N><<<dim3((ncols + CF::C - 1) / CF::C, (unsigned)nimg), CF::THREADS, CF::SMEM, st>>>(in, out, ncols,
+                                                                                                   sym, tw);
+  ::ht::count_launch();
   return cudaGetLastError();
 }
 
@@ -420,12 +438,12 @@ cudaError_t symbol_rows(int N, const float2* in, float2* out, long nrows, const 
   }
 }
 
-cudaError_t symbol_cols(int N, float2* data, long nimg, int ncols, const float* sym, const float2* tw,
-                        cudaStream_t st) {
+cudaError_t symbol_cols(int N, const float2* in, float2* out, long nimg, int ncols, const float* sym,
+                        const float2* tw, cudaStream_t st) {
   switch (N) {
 #define X(S) \
   case S:    \
-    return l_symbol_cols<S>(data, nimg, ncols, sym, tw, st);
+    return l_symbol_cols<S>(in, out, nimg, ncols, sym, tw, st);
     HT_SIZE_CASES(X)
 #undef X
     default:
@@ -502,13 +520,14 @@ extern "C" int ht_shift_coeff(ht_shift_s* s, const void* psi, void* out, long ba
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   HT_CHECK_CUDA(symbol_rows(s->npsi, static_cast<const float2*>(psi), static_cast<float2*>(out),
                             batch * s->nzpsi, s->symx, s->tw_x, st));
-  HT_CHECK_CUDA(symbol_cols(s->nzpsi, static_cast<float2*>(out), batch, s->npsi, s->symy, s->tw_y, st));
+  HT_CHECK_CUDA(symbol_cols(s->nzpsi, static_cast<float2*>(out), static_cast<float2*>(out), batch, s->npsi, s->symy,
+                            s->tw_y, st));
   return kOk;
 }
 
-extern "C" int ht_shift_coeff_z(ht_shift_s* s, void* data, long ncols, void* stream) {
+extern "C" int ht_shift_coeff_z(ht_shift_s* s, const void* in, void* out, long ncols, void* stream) {
   using namespace ht;
-  HT_REQUIRE(s && data, "ht_shift_coeff_z: null pointer");
+  HT_REQUIRE(s && in && out, "ht_shift_coeff_z: null pointer");
   HT_REQUIRE(ncols >= 0, "ht_shift_coeff_z: ncols must be non-negative");
   if (!fft_size_supported(s->nzpsi)) {
     set_error("ht_shift_coeff_z: nzpsi must be a supported FFT length");
@@ -516,8 +535,8 @@ extern "C" int ht_shift_coeff_z(ht_shift_s* s, void* data, long ncols, void* str
   }
   if (ncols == 0) return kOk;
   HT_REQUIRE(ncols <= 0x7fffffffL, "ht_shift_coeff_z: ncols too large");
-  HT_CHECK_CUDA(symbol_cols(s->nzpsi, static_cast<float2*>(data), 1, (int)ncols, s->symy, s->tw_y,
-                            static_cast<cudaStream_t>(stream)));
+  HT_CHECK_CUDA(symbol_cols(s->nzpsi, static_cast<const float2*>(in), static_cast<float2*>(out), 1, (int)ncols,
+                            s->symy, s->tw_y, static_cast<cudaStream_t>(stream)));
   return kOk;
 }
 
@@ -534,7 +553,8 @@ extern "C" int ht_shift_filter(ht_shift_s* s, const void* psi, void* out, long b
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   HT_CHECK_CUDA(symbol_rows(s->npsi, static_cast<const float2*>(psi), static_cast<float2*>(out), batch * s->nzpsi,
                             symx, s->tw_x, st));
-  HT_CHECK_CUDA(symbol_cols(s->nzpsi, static_cast<float2*>(out), batch, s->npsi, symy, s->tw_y, st));
+  HT_CHECK_CUDA(symbol_cols(s->nzpsi, static_cast<float2*>(out), static_cast<float2*>(out), batch, s->npsi, symy,
+                            s->tw_y, st));
   return kOk;
 }
 
@@ -546,9 +566,8 @@ extern "C" int ht_shift_Sback(ht_shift_s* s, const void* g, const float* r, cons
   HT_REQUIRE(batch >= 0 && batch <= 65535, "ht_shift_Sback: batch must be in [0, 65535]");
   if (batch == 0) return kOk;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  HT_CHECK_CUDA(cudaMemsetAsync(out, 0, sizeof(float2) * batch * s->nzpsi * s->npsi, st));
-  k_sback<<<out_grid(s, batch), kBlock, 0, st>>>(static_cast<const float2*>(g), static_cast<float2*>(out), r, mag,
-                                                 nmag, dims(s), batch);
+  k_sback<<<coef_grid(s, batch), kBlock, 0, st>>>(static_cast<const float2*>(g), static_cast<float2*>(out), r, mag,
+                                                  nmag, dims(s), batch);
   count_launch();
   HT_CHECK_CUDA(cudaGetLastError());
   return kOk;

@@ -244,7 +244,7 @@ k_tgather(const float2* __restrict__ fde, float2* __restrict__ sino, GatherGeom 
 template <int N>
 __global__ void __launch_bounds__(ZCfg<N, TZ<2 * N>::Z>::THREADS)
 k_tsino_fft(const float2* __restrict__ sino, float2* __restrict__ gs, int ntheta, int nz,
-            const float2* __restrict__ tw4, const float* __restrict__ symx) {
+            const float2* __restrict__ tw4, const float* __restrict__ symx, float scale) {
   constexpr int Z = TZ<2 * N>::Z;
   constexpr int T = ZCfg<N, Z>::T;
   extern __shared__ float2 smem[];
@@ -264,7 +264,7 @@ k_tsino_fft(const float2* __restrict__ sino, float2* __restrict__ gs, int ntheta
   for (int idx = threadIdx.x; idx < N * Z; idx += blockDim.x) {
     const int tx = idx / Z, ll = idx % Z;
     float2 v = zline<N, Z>(smem, ll).ld(tx);
-    float sg = (tx & 1) ? -1.f : 1.f;
+    float sg = (tx & 1) ? -scale : scale;  // the caller's scale folded into the sign
     if (symx) sg *= __ldg(&symx[(tx + N / 2) % N]);  // detector-axis filter (see k_tgather)
     dst[idx] = cscale(v, sg);
   }
@@ -582,7 +582,7 @@ struct CellLists {
 template <int N2>
 static cudaError_t tomo_RT_sized(const float2* sino, float2* obj, const float* phi, float2* fab, float2* fde,
                                  float2* gs, const GatherGeom& G, const CellLists& L, int nz, const float2* tw_n,
-                                 const float2* tw_2n, const float* symx, cudaStream_t st) {
+                                 const float2* tw_2n, const float* symx, float scale, cudaStream_t st) {
   constexpr int n = N2 / 2;
   constexpr int Z = TZ<N2>::Z;
   using C2 = ZCfg<N2, Z>;
@@ -592,7 +592,7 @@ static cudaError_t tomo_RT_sized(const float2* sino, float2* obj, const float* p
   if ((e = allow_smem(k_tsino_fft<n>, C1::SMEM)) != cudaSuccess) return e;
   if ((e = allow_smem(k_tcol_adj<N2>, C2::SMEM)) != cudaSuccess) return e;
   if ((e = allow_smem(k_trow_adj<N2>, C2::SMEM)) != cudaSuccess) return e;
-  k_tsino_fft<n><<<dim3(G.ntheta, nzb), C1::THREADS, C1::SMEM, st>>>(sino, gs, G.ntheta, nz, tw_n, symx);
+  k_tsino_fft<n><<<dim3(G.ntheta, nzb), C1::THREADS, C1::SMEM, st>>>(sino, gs, G.ntheta, nz, tw_n, symx, scale);
   count_launch();
   {
     KTimer kt("k_tcell", st, (double)nz);
@@ -834,7 +834,7 @@ static int tomo_R(ht_tomo_s* t, const void* obj, void* sino, int nz, bool filt, 
   return kOk;
 }
 
-static int tomo_RT(ht_tomo_s* t, const void* sino, void* obj, int nz, bool filt, void* stream) {
+static int tomo_RT(ht_tomo_s* t, const void* sino, void* obj, int nz, bool filt, float scale, void* stream) {
   HT_REQUIRE(t && obj && sino, "ht_tomo_RT: null pointer");
   HT_REQUIRE(nz >= 0 && nz <= t->nz, "ht_tomo_RT: nz exceeds the handle's slice capacity");
   if (nz == 0) return kOk;
@@ -846,7 +846,8 @@ static int tomo_RT(ht_tomo_s* t, const void* sino, void* obj, int nz, bool filt,
 #define X(A, B)                                                                                                 \
   case A:                                                                                                       \
     e = tomo_RT_sized<B>(static_cast<const float2*>(sino), static_cast<float2*>(obj), t->phi, t->fab, t->fde,    \
-                         t->gs, G, CellLists{t->cl_len, t->cl_off, t->cl_ent}, nz, t->tw_n, t->tw_2n, symx, st); \
+                         t->gs, G, CellLists{t->cl_len, t->cl_off, t->cl_ent}, nz, t->tw_n, t->tw_2n, symx,      \
+                         scale, st);                                                                                \
     break;
     HT_TOMO_SIZES(X)
 #undef X
@@ -863,13 +864,13 @@ extern "C" int ht_tomo_R(ht_tomo_s* t, const void* obj, void* sino, int nz, void
 }
 
 extern "C" int ht_tomo_RT(ht_tomo_s* t, const void* sino, void* obj, int nz, void* stream) {
-  return ht::tomo_RT(t, sino, obj, nz, false, stream);
+  return ht::tomo_RT(t, sino, obj, nz, false, 1.0f, stream);
 }
 
 extern "C" int ht_tomo_R_coeffx(ht_tomo_s* t, const void* obj, void* sino, int nz, void* stream) {
   return ht::tomo_R(t, obj, sino, nz, true, stream);
 }
 
-extern "C" int ht_tomo_RT_coeffx(ht_tomo_s* t, const void* sino, void* obj, int nz, void* stream) {
-  return ht::tomo_RT(t, sino, obj, nz, true, stream);
+extern "C" int ht_tomo_RT_coeffx(ht_tomo_s* t, const void* sino, void* obj, int nz, float scale, void* stream) {
+  return ht::tomo_RT(t, sino, obj, nz, true, scale, stream);
 }

@@ -196,18 +196,20 @@ class Rec:
                   _lib.ptr(dot) if dot is not None else None, _lib.stream_ptr())
 
     # -------------------------------------------------- fused cascade
-    def _gradient_pass(self, c, pos, prb, persistent=False):
+    def _gradient_pass(self, c, pos, prb, persistent=False, gpos=None, gprb=None, scale_pos=1.0, scale_prb=1.0):
         """Fused gF0..gF3 (rec_mpi.py:327-353): returns (sum_k S^T Y22, gpos, gprb), F in _scal[0].
-        persistent=True writes into the Rec's own output arrays (no allocation)."""
-        if persistent:
-            gc, gpos, gprb = self._gc, self._gpos, self._gprb
-        else:
-            gc = torch.empty_like(c)
-            gpos = torch.empty(self.ntheta, self.ndist, 2, dtype=torch.float32, device=self.device)
-            gprb = torch.empty(self.ndist, self.nz, self.n, dtype=torch.complex64, device=self.device)
+        persistent=True writes gc into the Rec's own array (no allocation);
+        gpos / gprb given: written there, times scale_pos / scale_prb."""
+        gc = self._gc if persistent else torch.empty_like(c)
+        if gpos is None:
+            gpos = self._gpos if persistent else torch.empty(self.ntheta, self.ndist, 2, dtype=torch.float32,
+                                                             device=self.device)
+        if gprb is None:
+            gprb = self._gprb if persistent else torch.empty(self.ndist, self.nz, self.n, dtype=torch.complex64,
+                                                             device=self.device)
         _lib.call("ht_rec_gradient", self._h, _lib.ptr(c), _lib.ptr(pos), _lib.ptr(self.eff_demagnifications),
                   _lib.ptr(prb), _lib.ptr(self.data), _lib.ptr(gc), _lib.ptr(gpos), _lib.ptr(gprb),
-                  _lib.ptr(self._scal), _lib.stream_ptr())
+                  _lib.ptr(self._scal), float(scale_pos), float(scale_prb), _lib.stream_ptr())
         return gc, gpos, gprb
 
     def _hessian_pass(self, c, pos, prb, y, z=None, out=None):
@@ -436,20 +438,19 @@ class Rec:
         rho = self.rho_sq
         dots = self._dots
         first = i == self.start_iter
-        # ---- gradients (rec_mpi.py:305-325)
-        gc, gpos, gprb = self._gradient_pass(C["vars"], vars["pos"], vars["prb"], persistent=True)
-        torch.mul(gprb, rho["prb"], out=grads["prb"])
-        torch.mul(gpos, rho["pos"], out=grads["pos"])
+        # ---- gradients (rec_mpi.py:305-325); the variable scalings rho are
+        # applied inside the library passes, so no separate elementwise pass runs
+        gc, _, _ = self._gradient_pass(C["vars"], vars["pos"], vars["prb"], persistent=True, gpos=grads["pos"],
+                                       gprb=grads["prb"], scale_pos=rho["pos"], scale_prb=rho["prb"])
         if self._fold:
             # grads obj = rho R^T coeff(gc) = rho Cz R^T Cx gc;  C grads = coeff(R grads obj) = Cx R Cz grads obj
             st, nc = _lib.stream_ptr(), self.nobj * self.nobj
-            _lib.call("ht_tomo_RT_coeffx", self.cl_tomo._h, _lib.ptr(gc), _lib.ptr(grads["obj"]), self.nzobj, st)
-            _lib.call("ht_shift_coeff_z", self.cl_shift._hc, _lib.ptr(grads["obj"]), nc, st)
-            grads["obj"] *= rho["obj"]
+            _lib.call("ht_tomo_RT_coeffx", self.cl_tomo._h, _lib.ptr(gc), _lib.ptr(grads["obj"]), self.nzobj,
+                      float(rho["obj"]), st)
+            _lib.call("ht_shift_coeff_z", self.cl_shift._hc, _lib.ptr(grads["obj"]), _lib.ptr(grads["obj"]), nc, st)
             self.gradient_laplacian(grads["obj"])
             self.gradient_prbfit(grads["prb"], vars["prb"])
-            self._vol.copy_(grads["obj"])
-            _lib.call("ht_shift_coeff_z", self.cl_shift._hc, _lib.ptr(self._vol), nc, st)
+            _lib.call("ht_shift_coeff_z", self.cl_shift._hc, _lib.ptr(grads["obj"]), _lib.ptr(self._vol), nc, st)
             _lib.call("ht_tomo_R_coeffx", self.cl_tomo._h, _lib.ptr(self._vol), _lib.ptr(C["grads"]), self.nzobj, st)
         else:
             self._coeff_into(gc, grads["proj"])
@@ -478,9 +479,9 @@ class Rec:
         st = _lib.stream_ptr()
         bh = self._bh
         rr = (float(rho["obj"]), float(rho["pos"]), float(rho["prb"]))
-        _lib.call("ht_bh_scalars", _lib.ptr(H), None, int(first), 0, *rr, _lib.ptr(bh), None, 0, None, st)
+        # phase 0: beta, and the dots cleared for the direction updates below
+        _lib.call("ht_bh_scalars", _lib.ptr(H), _lib.ptr(dots), int(first), 0, *rr, _lib.ptr(bh), None, 0, None, st)
         beta = _lib.ptr(bh)
-        dots.zero_()
         for k, v in enumerate(("obj", "pos", "prb")):
             self._axpby_dev(etas[v], grads[v], beta, 1.0, None, -1.0, dots[k:k + 1])
         if not self._fold:

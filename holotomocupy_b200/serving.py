@@ -191,7 +191,7 @@ class Server:
                     # once the active requests have made room
                     self._streams.append(slot.stream)
                     pending.insert(0, r)
-                    self._release()
+                    used -= self._release()
                     if not active or "out of memory" not in str(err):
                         raise
                     break

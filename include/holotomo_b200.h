@@ -61,6 +61,33 @@ int ht_prop_D(ht_prop_s* p, const void* in, void* out, long batch, int j, void* 
 int ht_prop_DT(ht_prop_s* p, const void* in, void* out, long batch, int j, void* stream);
 
 /* ------------------------------------------------------------------------
+ * Padded-grid convolution and mirror padding, for callers that work on the
+ * reference's 2nz x 2n grid directly (its tests time and compare these steps).
+ * Replaces the cuFFTDx convolution conv2d_create / conv2d_run /
+ * conv2d_destroy (src/holotomocupy/cuda/conv2d.cu:117-159, bound in
+ * conv2d_cufftdx.py:150-196) and the pad_fwd / pad_adj kernels
+ * (src/holotomocupy/cuda_kernels.py:78-127, Propagation._fwd_pad/_adj_pad,
+ * propagation.py:46-68).  ht_prop_D/DT do not use them.
+ * --------------------------------------------------------------------- */
+typedef struct ht_conv2d_s ht_conv2d_s;
+
+/* A convolution of [rows, cols] complex64 images; rows, cols: 2^a 3^b from
+ * 18 to 4096.  The handle holds only shared twiddle tables (no workspace). */
+int ht_conv2d_create(int rows, int cols, ht_conv2d_s** out);
+int ht_conv2d_destroy(ht_conv2d_s* h);
+/* y[b] = IFFT2(FFT2(x[b]) * H) for b < batch, the inverse unnormalised
+ * (rows*cols times the normalised one, as conv2d_run); x, y [batch, rows,
+ * cols], H [rows, cols] complex64; y may alias x. */
+int ht_conv2d_run(ht_conv2d_s* h, const void* x, const void* H, void* y, long batch, void* stream);
+
+/* fpad[batch, 2nz, 2n] = the half-sample-symmetric (mirror) extension of
+ * f[batch, nz, n] centred on the padded grid (pad_fwd); n, nz even. */
+int ht_pad_mirror(const void* f, void* fpad, long batch, int nz, int n, void* stream);
+/* f[batch, nz, n] = the adjoint of ht_pad_mirror: each sample sums the four
+ * padded samples that copy it (pad_adj). */
+int ht_pad_fold(const void* fpad, void* f, long batch, int nz, int n, void* stream);
+
+/* ------------------------------------------------------------------------
  * USFFT Radon transform.  Replaces Tomo.__init__/R/RT
  * (src/holotomocupy/tomo.py:12-54, 56-86, 88-116) and the gather kernel
  * (src/holotomocupy/cuda_kernels.py:3-76).
@@ -87,7 +114,9 @@ int ht_tomo_RT(ht_tomo_s* t, const void* sino, void* obj, int nz, void* stream);
  * ht_shift_coeff_z on the volume they give coeff(R obj) = Cx R Cz obj and
  * R^T coeff(sino) = Cz R^T Cx sino (the z factor commutes with R). */
 int ht_tomo_R_coeffx(ht_tomo_s* t, const void* obj, void* sino, int nz, void* stream);
-int ht_tomo_RT_coeffx(ht_tomo_s* t, const void* sino, void* obj, int nz, void* stream);
+/* ... and obj = scale * R^T(Cx sino): the BH variable scaling rho of the
+ * object gradient (rec_mpi.py:345) applied in the same pass. */
+int ht_tomo_RT_coeffx(ht_tomo_s* t, const void* sino, void* obj, int nz, float scale, void* stream);
 
 /* ------------------------------------------------------------------------
  * Cubic B-spline shift family.  Replaces Shift.__init__/coeff/S/Sadj/
@@ -106,10 +135,10 @@ int ht_shift_destroy(ht_shift_s* s);
 /* out = ifft2(fft2(psi) / B3): the B-spline prefilter (shift.py:74-82);
  * complex64 [batch, nzpsi, npsi]; out may alias psi. */
 int ht_shift_coeff(ht_shift_s* s, const void* psi, void* out, long batch, void* stream);
-/* The z-axis half of the prefilter (the column factor of shift.py:74-82),
- * in place on data [nzpsi, ncols] complex64 (a volume [nzpsi, ny, nx] has
- * ncols = ny nx). */
-int ht_shift_coeff_z(ht_shift_s* s, void* data, long ncols, void* stream);
+/* The z-axis half of the prefilter (the column factor of shift.py:74-82):
+ * out = Cz in for in, out [nzpsi, ncols] complex64 (a volume [nzpsi, ny, nx]
+ * has ncols = ny nx); out may alias in. */
+int ht_shift_coeff_z(ht_shift_s* s, const void* in, void* out, long ncols, void* stream);
 
 /* out = ifft2(fft2(psi) * (symy (x) symx)): a separable periodic filter with
  * caller-given device symbols symx [npsi], symy [nzpsi] in FFT order, each
@@ -123,7 +152,7 @@ int ht_shift_filter(ht_shift_s* s, const void* psi, void* out, long batch, const
  * the back-projection of detector images g [batch, nz, n] complex64 onto the
  * coefficient grid [batch, nzpsi, npsi] complex64 with the B-spline stretched
  * by mag (nmag = 1: one magnification for every image; nmag = batch: one
- * each); out is zeroed first. */
+ * each); every cell of out is written (a deterministic gather, no atomics). */
 int ht_shift_Sback(ht_shift_s* s, const void* g, const float* r, const float* mag, int nmag, void* out, long batch,
                    void* stream);
 
@@ -176,12 +205,15 @@ int ht_rec_destroy(ht_rec_s* r);
 int ht_rec_forward(ht_rec_s* r, const void* c, const float* pos, const float* mag, const void* prb, const float* data,
                    float* amp, double* fval, void* stream);
 
-/* Gradient of the data term (gF0..gF3, rec_mpi.py:327-353, 562-813), unscaled:
- * gc [ntheta, nzobj, nobj] = sum_k S_k^T(Y22) (apply coeff() for the proj
- * gradient), gpos [ntheta, ndist, 2] float32, gprb [ndist, nz, n] complex64,
- * *fval (device double) = sum (|x0| - data)^2 at the same point. */
+/* Gradient of the data term (gF0..gF3, rec_mpi.py:327-353, 562-813):
+ * gc [ntheta, nzobj, nobj] = sum_k S_k^T(Y22) (unscaled; apply coeff() for
+ * the proj gradient), gpos [ntheta, ndist, 2] float32 times scale_pos,
+ * gprb [ndist, nz, n] complex64 times scale_prb (the variable scalings
+ * rho_sq of rec_mpi.py:345-347; 1 for the plain gradient), *fval (device
+ * double) = sum (|x0| - data)^2 at the same point. */
 int ht_rec_gradient(ht_rec_s* r, const void* c, const float* pos, const float* mag, const void* prb,
-                    const float* data, void* gc, float* gpos, void* gprb, double* fval, void* stream);
+                    const float* data, void* gc, float* gpos, void* gprb, double* fval, float scale_pos,
+                    float scale_prb, void* stream);
 
 /* Hessian forms at the state of the last ht_rec_gradient call
  * (hessian_cascade, rec_mpi.py:250-303) for directions y (and z when
@@ -211,12 +243,13 @@ int ht_axpby_dev(void* x, const void* y, const double* A, float sa, const double
                  void* stream);
 /* BH step sizes on the device (rec_mpi.py:180-218, with the forms of
  * ht_rec_hessian in H[4] and dots[3] = <eta,grad> of obj, pos, prb).
- * phase 0: scal[0] = beta = first ? 0 : H[1]/H[2].
+ * phase 0: scal[0] = beta = first ? 0 : H[1]/H[2]; dots[0..2] = 0 if dots
+ *          != NULL (the direction updates then accumulate into them).
  * phase 1: scal[1] = alpha = -(dots[0]/rho_obj + dots[1]/rho_pos + dots[2]/rho_prb)
  *          / (first ? H[0] : beta^2 H[2] - 2 beta H[3] + H[0]);
  *          if hist: (alpha, beta) goes to hist[2*(*count)] while *count < cap,
  *          and *count is incremented (device int). */
-int ht_bh_scalars(const double* H, const double* dots, int first, int phase, double rho_obj, double rho_pos,
+int ht_bh_scalars(const double* H, double* dots, int first, int phase, double rho_obj, double rho_pos,
                   double rho_prb, double* scal, double* hist, int cap, int* count, void* stream);
 
 /* The objective sum (|x0| - data)^2 of ht_rec_forward, without allocating.
@@ -226,7 +259,8 @@ int ht_bh_scalars(const double* H, const double* dots, int first, int phase, dou
  * the propagator handle (created once at set-up) and the inputs, and works
  * in one fixed 32 MiB device array that every GPU loading the library holds
  * until exit.  Angles are processed in chunks that fit it; one angle needs
- * ndist*nz*n*8 bytes, and larger sizes are rejected (status 1).  The first
+ * ndist*nz*n*8 + ndist*(nz+1)*8 bytes, and larger sizes are rejected
+ * (status 1).  The sum is reduced in a fixed order (bitwise reproducible).  The first
  * call on a device looks up the array's device address: make it before any
  * stream capture.  All calls share the array, so calls that overlap on the
  * GPU race; run them in one stream. */

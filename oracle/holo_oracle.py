@@ -149,6 +149,25 @@ class Tomo:
         norm_const = np.sqrt(self.n / self.ntheta)
         return self.RT(self.filter_sino(data, filter_name)) * norm_const
 
+    def rec_tomo(self, d, niter=1):
+        """tomo.py:185-210: conjugate gradients on ||R u - d||^2 from u = 0."""
+        u = np.zeros((d.shape[1], self.n, self.n), dtype=d.dtype)
+        Ru = self.R(u)
+        eta = Reta = None
+        for k in range(niter):
+            grad = self.RT(2 * (Ru - d))
+            Rgrad = self.R(grad)
+            if k == 0:
+                eta, Reta = -grad, -Rgrad
+            else:
+                beta = redot(Rgrad, Reta) / redot(Reta, Reta)
+                eta = beta * eta - grad
+                Reta = beta * Reta - Rgrad
+            alpha = -redot(grad, eta) / (2 * redot(Reta, Reta))
+            u = u + alpha * eta
+            Ru = Ru + alpha * Reta
+        return u
+
 
 class Shift:
     """Cubic B-spline shift (shift.py:15-221)."""

@@ -283,15 +283,183 @@ def lap_cases(ns):
     np.savez_compressed(os.path.join(HERE, "lap.npz"), **out)
 
 
+def _unit_mag_rec(ns, n, ntheta, ndist, nobj, distance, wavelength=7.3e-11, voxelsize=20e-9, niter=1):
+    """The reference's Rec with the propagation geometry given directly and unit
+    magnification: its constructor derives both from z1 and the focus distance
+    (rec_mpi.py:55-60), so the propagator is replaced after construction."""
+    args = rec_args(n, ntheta, ndist, nobj, niter)
+    rec = ns.rec_mpi.Rec(args)
+    rec.cl_prop = ns.propagation.Propagation(n, n, rec.nchunk, ndist, wavelength, voxelsize, distance)
+    rec.norm_magnifications = np.ones(ndist)
+    rec.eff_demagnifications[:] = 1
+    return rec
+
+
+def c1_data(ntheta, ndist, n):
+    """Deterministic amplitudes for the adjoint chain of the small plain chain:
+    0.8 + 0.1 k/17 with k = (7y + 13x + 5 angle + 3 distance) mod 17 (the
+    residual against them is well away from zero, so the gradient carries no
+    FP32 cancellation)."""
+    a = np.arange(ntheta)[:, None, None, None]
+    j = np.arange(ndist)[None, :, None, None]
+    y = np.arange(n)[None, None, :, None]
+    x = np.arange(n)[None, None, None, :]
+    k = (7 * y + 13 * x + 5 * a + 3 * j) % 17
+    return (0.8 + 0.1 * (k / 17)).astype("float32")
+
+
+def c1_cases(ns):
+    """The small plain chain at its full size: 128^3 ellipsoid phantom (20
+    ellipsoids, k dx (-delta + i beta)), 180 angles, distances 3/4/5/6 mm at
+    7.3e-11 m and 20 nm pixels, flat unit probe, positions uniform in +-2 px.
+    Forward: proj = R(obj / norm_const) -> S(coeff(proj)) -> exp(i .) -> D(prb .)
+    -> |.| (gen_sqrt_data, rec_mpi.py:882-897).  Adjoint: the full gradient
+    (gF0..gF4, rec_mpi.py:305-353) at a perturbed state (object x 0.8, positions
+    moved by up to 0.5 px) against the deterministic amplitudes of c1_data, so
+    the test needs no stored data.  Full outputs are 20-50 MB each,
+    so the fixture keeps an angle block (every 30th angle) of proj and the
+    amplitudes, four slices of the object gradient, the probe and position
+    gradients whole, and float64 checksums of every full array: its squared norm
+    and its inner product with seeded unit normal weights over its float32 view
+    (regenerated by the test from the seed 1000 + len(name))."""
+    from holotomocupy_b200.synthetic import ellipsoid_phantom
+    n, ntheta, ndist = 128, 180, 4
+    distance = np.array([3e-3, 4e-3, 5e-3, 6e-3])
+    obj = ellipsoid_phantom(n, 20, 11, device="cpu").numpy()
+    rng = np.random.default_rng(12)
+    pos = rng.uniform(-2, 2, (ntheta, ndist, 2)).astype("float32")
+    pos_err = rng.uniform(-0.5, 0.5, (ntheta, ndist, 2)).astype("float32")
+    prb = np.ones((ndist, n, n), "complex64")
+    rec = _unit_mag_rec(ns, n, ntheta, ndist, n, distance)
+    rec.vars["obj"][:] = obj
+    rec.vars["prb"][:] = ns.cp.array(prb)
+    rec.vars["pos"][:] = ns.cp.array(pos)
+    amp = np.zeros((ntheta, ndist, n, n), "float32")
+    rec.gen_sqrt_data(rec.vars, amp)
+    proj = np.array(rec.vars["proj"])
+    rec.data[:] = c1_data(ntheta, ndist, n)
+    # the perturbed state, normalised as BH() has it (rec_mpi.py:149-158)
+    rec.vars["obj"][:] = obj * np.float32(0.8) / rec.norm_const
+    rec.vars["pos"][:] = ns.cp.array(pos + pos_err)
+    rec.fwd_tomo(rec.vars["obj"], out=rec.proj_tmp)
+    rec.vars["proj"][:] = rec.proj_tmp
+    rec.gradients(rec.vars, rec.grads)
+    blk = np.arange(0, ntheta, 30)
+    sl = np.array([16, 63, 64, 100])
+    out = {"dims": np.array([n, ntheta, ndist]), "distance": distance, "obj": obj, "pos": pos,
+           "pos_err": pos_err, "blk": blk, "slices": sl, "proj_blk": proj[blk], "amp_blk": amp[blk],
+           "grad_prb": np.asarray(rec.grads["prb"]), "grad_pos": np.asarray(rec.grads["pos"]),
+           "grad_obj_sl": np.array(rec.grads["obj"])[sl], "grad_proj_blk": np.array(rec.grads["proj"])[blk]}
+    full = {"proj": proj, "amp": amp, "grad_obj": np.array(rec.grads["obj"]),
+            "grad_proj": np.array(rec.grads["proj"])}
+    for k, v in full.items():
+        vv = np.ascontiguousarray(v).view("float32").astype("float64")
+        w = np.random.default_rng(1000 + len(k)).standard_normal(vv.shape)
+        out[f"{k}_sq"] = np.array(np.sum(vv ** 2))
+        out[f"{k}_wdot"] = np.array(np.sum(vv * w))
+    np.savez_compressed(os.path.join(HERE, "c1.npz"), **out)
+
+
+def prbfit_cases(ns):
+    """The probe-fit regulariser lam_prbfit |||D prb| - ref||^2 (rec_mpi.py:365-398,
+    815-835) at lam_prbfit = 2e-3: the full gradient, the Hessian form and the
+    objective at one point, and a 4-iteration BH run, 32^3 x 12 angles x 2
+    distances with ref = |D prb_true| (gen_sqrt_ref, rec_mpi.py:899-902)."""
+    out = {}
+    n, ntheta, ndist, nobj = 32, 6, 2, 32
+    rng = np.random.default_rng(52)
+    args = rec_args(n, ntheta, ndist, nobj)
+    args.lam_prbfit = 2e-3
+    rec = ns.rec_mpi.Rec(args)
+    prb_true = (1 + 0.2 * crand(rng, (ndist, n, n))).astype("complex64")
+    rec.gen_sqrt_ref(ns.cp.array(prb_true), rec.ref)
+    prb = (prb_true + 0.1 * crand(rng, (ndist, n, n))).astype("complex64")
+    obj = crand(rng, (nobj, nobj, nobj), 0.02)
+    pos = frand(rng, (ntheta, ndist, 2), 0.8)
+    data = (np.abs(frand(rng, (ntheta, ndist, n, n))) + 0.5).astype("float32")
+    rec.data[:] = data
+    rec.eff_demagnifications[:] = (1 + rec.shrink_nd) / ns.cp.array(rec.norm_magnifications[None, :])
+    rec.vars["obj"][:] = obj
+    rec.vars["prb"][:] = ns.cp.array(prb)
+    rec.vars["pos"][:] = ns.cp.array(pos)
+    rec.fwd_tomo(rec.vars["obj"], out=rec.proj_tmp)
+    rec.vars["proj"][:] = rec.proj_tmp
+    d1 = crand(rng, (ndist, n, n), 0.1)
+    d2 = crand(rng, (ndist, n, n), 0.1)
+    F = float(rec.min(rec.vars["prb"], rec.vars["obj"], rec.vars["pos"], rec.vars["proj"]))
+    h12 = float(rec.hessian_prbfit(rec.vars["prb"], ns.cp.array(d1), ns.cp.array(d2)))
+    h11 = float(rec.hessian_prbfit(rec.vars["prb"], ns.cp.array(d1), ns.cp.array(d1)))
+    gp = ns.cp.zeros((ndist, n, n), "complex64")
+    rec.gradient_prbfit(gp, rec.vars["prb"])
+    rec.gradients(rec.vars, rec.grads)
+    out.update({"p_dims": np.array([n, ntheta, ndist, nobj]), "p_lam": np.array(args.lam_prbfit),
+                "p_prb_true": prb_true, "p_ref": np.asarray(rec.ref), "p_prb": prb, "p_obj": obj, "p_pos": pos,
+                "p_data": data, "p_d1": d1, "p_d2": d2, "p_F": np.array(F), "p_h12": np.array(h12),
+                "p_h11": np.array(h11), "p_gprb_fit": np.asarray(gp),
+                "p_grad_prb": np.asarray(rec.grads["prb"]), "p_grad_obj": np.array(rec.grads["obj"]),
+                "p_grad_pos": np.asarray(rec.grads["pos"])})
+    # BH with the probe-fit term, from the golden BH problem of rec_cases
+    n, ntheta, ndist, nobj, niter = 32, 12, 2, 32, 4
+    rng = np.random.default_rng(7)
+    args = rec_args(n, ntheta, ndist, nobj, niter)
+    args.lam_prbfit = 2e-3
+    rec = ns.rec_mpi.Rec(args)
+    obj = phantom(nobj, rng)
+    prb = (1 + 0.1 * crand(rng, (ndist, n, n))).astype("complex64")
+    pos = frand(rng, (ntheta, ndist, 2), 1.0)
+    pos_err = frand(rng, (ntheta, ndist, 2), 0.2)
+    rec.vars["obj"][:] = obj
+    rec.vars["prb"][:] = ns.cp.array(prb)
+    rec.vars["pos"][:] = ns.cp.array(pos)
+    rec.gen_sqrt_data(rec.vars, rec.data)
+    rec.gen_sqrt_ref(ns.cp.array(prb), rec.ref)
+    rec.vars["obj"][:] = 0
+    rec.vars["prb"][:] = ns.cp.array(1)
+    rec.vars["pos"][:] = ns.cp.array(pos + pos_err)
+    pairs = []
+    orig = rec.allreduce2
+    rec.allreduce2 = lambda a, b: (pairs.append((float(a), float(b))), orig(a, b))[1]
+    rec.BH()
+    out.update({
+        "pbh_dims": np.array([n, ntheta, ndist, nobj, niter]), "pbh_lam": np.array(args.lam_prbfit),
+        "pbh_ref": np.asarray(rec.ref),
+        "pbh_obj": np.array(rec.vars["obj"]), "pbh_prb": np.asarray(rec.vars["prb"]),
+        "pbh_pos": np.asarray(rec.vars["pos"]), "pbh_proj": np.array(rec.vars["proj"]),
+        "pbh_topbottom": np.array(pairs, dtype="float64"),
+    })
+    np.savez_compressed(os.path.join(HERE, "prbfit.npz"), **out)
+
+
+def rectomo_cases(ns):
+    """Tomo.rec_tomo (tomo.py:185-210), the conjugate-gradient initial guess,
+    on a sinogram of the small ellipsoid phantom: 1 and 6 iterations, complex
+    and real data."""
+    out = {}
+    for (n, nz, ntheta, niter, dt, tag) in [(32, 4, 40, 6, "complex64", "a"), (48, 3, 64, 6, "float32", "b")]:
+        rng = np.random.default_rng(900 + n)
+        theta = np.linspace(0, np.pi, ntheta, endpoint=False).astype("float32")
+        t = ns.tomo.Tomo(n, nz, theta, 1)
+        obj = phantom(n, rng)[n // 2 - nz // 2: n // 2 - nz // 2 + nz]
+        obj = obj if dt == "complex64" else obj.real.astype("float32").copy()
+        d = t.R(ns.cp.array(obj)).get()
+        d = (d + 0.01 * np.abs(d).max() * (crand(rng, d.shape) if dt == "complex64" else frand(rng, d.shape))
+             ).astype(dt)
+        u = t.rec_tomo(ns.cp.array(d), niter).get()
+        u1 = t.rec_tomo(ns.cp.array(d), 1).get()
+        out.update({f"{tag}_dims": np.array([n, nz, ntheta, niter]), f"{tag}_theta": theta, f"{tag}_d": d,
+                    f"{tag}_u": u, f"{tag}_u1": u1})
+    np.savez_compressed(os.path.join(HERE, "rectomo.npz"), **out)
+
+
 def main():
     src = sys.argv[1] if len(sys.argv) > 1 else None
     if src is None:
         raise SystemExit("usage: make_golden.py <reference src dir>")
     ns = load_reference(src)
-    which = sys.argv[2:] or ["tomo", "prop", "shift", "rec", "lap", "sback"]
+    which = sys.argv[2:] or ["tomo", "prop", "shift", "rec", "lap", "sback", "c1", "prbfit", "rectomo"]
     for w in which:
         {"tomo": tomo_cases, "prop": prop_cases, "shift": shift_cases, "rec": rec_cases, "lap": lap_cases,
-         "sback": sback_cases}[w](ns)
+         "sback": sback_cases, "c1": c1_cases, "prbfit": prbfit_cases, "rectomo": rectomo_cases}[w](ns)
         print("wrote", w)
 
 

@@ -1,0 +1,93 @@
+"""The small plain chain at its full size against the reference's own operators.
+
+128^3 ellipsoid phantom, 180 angles, 4 distances (3-6 mm, 7.3e-11 m, 20 nm
+pixels), flat unit probe, positions uniform in +-2 px, unit magnification.
+Forward: R -> B-spline shift S -> exp(i .) -> Fresnel D -> |.|; adjoint: the
+full gradient (gF0..gF4 and R^T) at a perturbed state against deterministic
+amplitudes.  The fixture
+(tests/golden/c1.npz, from the reference's rec_mpi.py run under the CPU shim)
+holds an angle block and a few slices of the outputs plus float64 checksums of
+every full array.  Bound: rel L2 <= 1e-5 on every stored block, and the
+checksums within 1e-5 of the full arrays' scale."""
+import numpy as np
+import pytest
+import torch
+
+from conftest import rel_l2
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-5
+
+
+def c1_data(ntheta, ndist, n):
+    """The fixture generator's deterministic amplitudes (make_golden.c1_data):
+    0.8 + 0.1 k/17, k = (7y + 13x + 5 angle + 3 distance) mod 17."""
+    a = np.arange(ntheta)[:, None, None, None]
+    j = np.arange(ndist)[None, :, None, None]
+    y = np.arange(n)[None, None, :, None]
+    x = np.arange(n)[None, None, None, :]
+    k = (7 * y + 13 * x + 5 * a + 3 * j) % 17
+    return (0.8 + 0.1 * (k / 17)).astype("float32")
+
+
+def _checksums(t, name):
+    """(sum of squares, inner product with the fixture's seeded weights) of the
+    float32 view of a full array, in float64 (the generator's recipe)."""
+    v = t.detach().contiguous().view(torch.float32).double()
+    w = torch.from_numpy(np.random.default_rng(1000 + len(name)).standard_normal(tuple(v.shape))).to(v.device)
+    return float((v * v).sum()), float((v * w).sum())
+
+
+def _check_full(t, g, name):
+    sq, wd = _checksums(t, name)
+    ref_sq, ref_wd = float(g[f"{name}_sq"]), float(g[f"{name}_wdot"])
+    assert abs(sq / ref_sq - 1) < 2 * TOL, (name, sq, ref_sq)
+    # the weighted sum of N unit-normal weights has spread sqrt(sum of squares)
+    assert abs(wd - ref_wd) < TOL * np.sqrt(ref_sq), (name, wd, ref_wd)
+
+
+@pytest.fixture(scope="module")
+def c1(golden):
+    from holotomocupy_b200.rec import Rec
+    from holotomocupy_b200.synthetic import workload_args
+    g = golden("c1")
+    n, ntheta, ndist = [int(v) for v in g["dims"]]
+    rec = Rec(workload_args(n, ntheta, ndist, niter=1, distances=tuple(g["distance"])))
+    return g, rec
+
+
+def test_c1_forward_chain(c1):
+    g, rec = c1
+    rec.eff_demagnifications[:] = 1
+    v = rec.vars
+    v["obj"][:] = torch.from_numpy(g["obj"]).cuda()
+    v["prb"][:] = 1
+    v["pos"][:] = torch.from_numpy(g["pos"]).cuda()
+    amp = torch.empty_like(rec.data)
+    rec.gen_sqrt_data(v, amp)
+    blk = torch.from_numpy(g["blk"]).cuda()
+    assert rel_l2(v["proj"][blk].cpu().numpy(), g["proj_blk"]) < TOL
+    assert rel_l2(amp[blk].cpu().numpy(), g["amp_blk"]) < TOL
+    _check_full(v["proj"], g, "proj")
+    _check_full(amp, g, "amp")
+
+
+def test_c1_adjoint_chain(c1):
+    g, rec = c1
+    rec.eff_demagnifications[:] = 1
+    v, gr = rec.vars, rec.grads
+    n, ntheta, ndist = [int(q) for q in g["dims"]]
+    rec.data[:] = torch.from_numpy(c1_data(ntheta, ndist, n)).cuda()
+    v["obj"][:] = torch.from_numpy(g["obj"]).cuda() * 0.8 / rec.norm_const
+    v["prb"][:] = 1
+    v["pos"][:] = torch.from_numpy(g["pos"] + g["pos_err"]).cuda()
+    rec.fwd_tomo(v["obj"], out=v["proj"])
+    rec.gradients(v, gr)
+    blk = torch.from_numpy(g["blk"]).cuda()
+    sl = torch.from_numpy(g["slices"]).cuda()
+    assert rel_l2(gr["prb"].cpu().numpy(), g["grad_prb"]) < TOL
+    assert rel_l2(gr["pos"].cpu().numpy(), g["grad_pos"]) < TOL
+    assert rel_l2(gr["obj"][sl].cpu().numpy(), g["grad_obj_sl"]) < TOL
+    assert rel_l2(gr["proj"][blk].cpu().numpy(), g["grad_proj_blk"]) < TOL
+    _check_full(gr["obj"], g, "grad_obj")
+    _check_full(gr["proj"], g, "grad_proj")

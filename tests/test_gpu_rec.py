@@ -298,3 +298,113 @@ def test_bh_with_laplacian_matches_reference(golden, mode):
         assert abs(a / ra - 1) < 1e-4, (i, a, ra)
     for k in ("obj", "prb", "pos", "proj"):
         assert rel_l2(rec.vars[k].cpu().numpy(), g[f"lbh_{k}"]) < TOL, k
+
+
+def _prbfit_rec(g, niter=1):
+    from holotomocupy_b200.rec import Rec
+    n, ntheta, ndist, nobj = [int(v) for v in g["p_dims"]]
+    args = rec_args(n, ntheta, ndist, nobj, niter)
+    args.lam_prbfit = float(g["p_lam"])
+    return Rec(args)
+
+
+def test_prbfit_terms_match_reference(golden):
+    """The probe-fit regulariser's gradient, Hessian form and objective, and the
+    full gradient with it, against the reference's rec_mpi.py at lam_prbfit =
+    2e-3 (rec_mpi.py:365-398, 305-325, 815-835)."""
+    g = golden("prbfit")
+    rec = _prbfit_rec(g)
+    rec.ref[:] = cuda(g["p_ref"])
+    rec.data[:] = cuda(g["p_data"])
+    rec.eff_demagnifications[:] = (1 + rec.shrink_nd) / cuda(rec.norm_magnifications[None, :].astype("float32"))
+    v = rec.vars
+    v["obj"][:] = cuda(g["p_obj"])
+    v["prb"][:] = cuda(g["p_prb"])
+    v["pos"][:] = cuda(g["p_pos"])
+    rec.fwd_tomo(v["obj"], out=v["proj"])
+    gp = torch.zeros_like(v["prb"])
+    rec.gradient_prbfit(gp, v["prb"])
+    assert rel_l2(gp.cpu().numpy(), g["p_gprb_fit"]) < TOL
+    h11, h12, _ = rec._prbfit_forms(v["prb"], cuda(g["p_d1"]), cuda(g["p_d2"]))
+    assert abs(h12 / float(g["p_h12"]) - 1) < TOL
+    assert abs(h11 / float(g["p_h11"]) - 1) < TOL
+    assert abs(rec.min(v["prb"], v["obj"], v["pos"], v["proj"]) / float(g["p_F"]) - 1) < TOL
+    rec.gradients(v, rec.grads)
+    for k in ("prb", "obj", "pos"):
+        assert rel_l2(rec.grads[k].cpu().numpy(), g[f"p_grad_{k}"]) < TOL, k
+
+
+def test_bh_with_prbfit_matches_reference(golden):
+    """4 BH iterations with lam_prbfit = 2e-3 (host step sizes) against the
+    reference's run: state and step sizes."""
+    gr = golden("rec")
+    g = golden("prbfit")
+    from holotomocupy_b200.rec import Rec
+    n, ntheta, ndist, nobj, niter = [int(v) for v in g["pbh_dims"]]
+    args = rec_args(n, ntheta, ndist, nobj, niter)
+    args.lam_prbfit = float(g["pbh_lam"])
+    rec = Rec(args)
+    rec.vars["obj"][:] = cuda(gr["bh_obj_true"])
+    rec.vars["prb"][:] = cuda(gr["bh_prb_true"])
+    rec.vars["pos"][:] = cuda(gr["bh_pos_true"])
+    rec.gen_sqrt_data(rec.vars, rec.data)
+    rec.gen_sqrt_ref(rec.vars["prb"], rec.ref)
+    assert rel_l2(rec.ref.cpu().numpy(), g["pbh_ref"]) < TOL
+    rec.vars["obj"][:] = 0
+    rec.vars["prb"][:] = 1
+    rec.vars["pos"][:] = cuda(gr["bh_pos_true"] + gr["bh_pos_err"])
+    record = []
+    rec.BH(record=record)
+    tb = g["pbh_topbottom"]
+    ref_alpha = [tb[0, 0] / tb[0, 1]] + [tb[2 * i, 0] / tb[2 * i, 1] for i in range(1, niter)]
+    ref_beta = [0.0] + [tb[2 * i - 1, 0] / tb[2 * i - 1, 1] for i in range(1, niter)]
+    for (i, a, b), ra, rb in zip(record, ref_alpha, ref_beta):
+        assert abs(a / ra - 1) < 1e-4, (i, a, ra)
+        if rb:
+            assert abs(b / rb - 1) < 1e-4, (i, b, rb)
+    for k in ("obj", "prb", "pos", "proj"):
+        assert rel_l2(rec.vars[k].cpu().numpy(), g[f"pbh_{k}"]) < TOL, k
+
+
+@pytest.fixture(scope="module")
+def bh64_oracle():
+    """32 BH iterations of the FP64 oracle at 64^3, 32 angles, 4 distances
+    (3-6 mm, unit magnification), seeded ellipsoid phantom, random probe,
+    positions +-2 px (0.5 px initial error), noise-free amplitudes."""
+    from oracle import holo_oracle as O
+    from holotomocupy_b200.synthetic import ellipsoid_phantom, random_positions, random_probe, workload_args
+    n, ntheta, ndist, niter = 64, 32, 4, 32
+    args = workload_args(n, ntheta, ndist, niter=niter)
+    obj = ellipsoid_phantom(n, 20, 21, device="cpu").numpy()
+    prb = random_probe(ndist, n, n, 22, device="cpu").numpy()
+    pos = random_positions(ntheta, ndist, 2.0, 23, device="cpu").numpy()
+    pos0 = pos + np.random.default_rng(24).uniform(-0.5, 0.5, pos.shape).astype("float32")
+    orc = O.Rec(args, "complex128")
+    orc.eff_demagnifications[:] = 1
+    orc.vars["obj"][:] = obj
+    orc.vars["prb"][:] = prb
+    orc.vars["pos"][:] = pos
+    orc.gen_sqrt_data(orc.vars, orc.data)
+    orc.eff_demagnifications[:] = 0          # shrink_nd is the same array (rec_mpi.py:135-136)
+    data = orc.data.astype("float32")
+    orc.data[:] = data
+    orc.vars["obj"][:] = 0
+    orc.vars["prb"][:] = 1
+    orc.vars["pos"][:] = pos0
+    orc.BH()
+    return args, data, pos0, {k: orc.vars[k].copy() for k in ("obj", "prb", "pos")}
+
+
+@pytest.mark.parametrize("mode", ["host", "graph"])
+def test_bh_32_iterations_64cubed_4dist_against_fp64_oracle(bh64_oracle, mode):
+    """The 32-iteration bound at 64^3 x 32 angles x 4 distances: the FP32-bulk,
+    FP64-reduction BH stays within rel L2 1e-4 of the FP64 oracle's BH."""
+    from holotomocupy_b200.rec import Rec
+    args, data, pos0, ref = bh64_oracle
+    rec = Rec(args)
+    rec.data[:] = cuda(data)
+    rec.vars["prb"][:] = 1
+    rec.vars["pos"][:] = cuda(pos0)
+    rec.BH(mode=mode)
+    for k in ("obj", "prb", "pos"):
+        assert rel_l2(rec.vars[k].cpu().numpy(), ref[k]) < 1e-4, k

@@ -99,13 +99,40 @@ def test_prefilter_folded_into_R_and_RT(n, ntheta, nz):
     # forward
     ref = sh.coeff(t.R(x))
     xz = x.clone()
-    _lib.call("ht_shift_coeff_z", sh._hc, _lib.ptr(xz), n * n, st)
+    _lib.call("ht_shift_coeff_z", sh._hc, _lib.ptr(xz), _lib.ptr(xz), n * n, st)
     got = torch.empty(ntheta, nz, n, dtype=torch.complex64, device="cuda")
     _lib.call("ht_tomo_R_coeffx", t._h, _lib.ptr(xz), _lib.ptr(got), nz, st)
     assert rel_l2(got.cpu().numpy(), ref.cpu().numpy()) < 1e-5
     # adjoint
     ref = t.RT(sh.coeff(y))
     got = torch.empty(nz, n, n, dtype=torch.complex64, device="cuda")
-    _lib.call("ht_tomo_RT_coeffx", t._h, _lib.ptr(y), _lib.ptr(got), nz, st)
-    _lib.call("ht_shift_coeff_z", sh._hc, _lib.ptr(got), n * n, st)
+    _lib.call("ht_tomo_RT_coeffx", t._h, _lib.ptr(y), _lib.ptr(got), nz, 1.0, st)
+    _lib.call("ht_shift_coeff_z", sh._hc, _lib.ptr(got), _lib.ptr(got), n * n, st)
     assert rel_l2(got.cpu().numpy(), ref.cpu().numpy()) < 1e-5
+    # the scaled adjoint and the out-of-place z prefilter (the BH gradient's form)
+    scaled = torch.empty_like(got)
+    _lib.call("ht_tomo_RT_coeffx", t._h, _lib.ptr(y), _lib.ptr(scaled), nz, 0.37, st)
+    out = torch.empty_like(got)
+    _lib.call("ht_shift_coeff_z", sh._hc, _lib.ptr(scaled), _lib.ptr(out), n * n, st)
+    assert rel_l2(out.cpu().numpy(), 0.37 * ref.cpu().numpy()) < 1e-5
+
+
+@pytest.mark.parametrize("tag", ["a", "b"])
+def test_rec_tomo_matches_reference(golden, tag):
+    """Tomo.rec_tomo (tomo.py:185-210), the CG initial guess, on a noisy phantom
+    sinogram, complex and real.  One iteration matches the reference's run to
+    1e-5.  The reference accumulates CG's inner products in FP32 (utils.redot
+    through cp.vdot), these are FP64, and CG amplifies the difference: after 6
+    iterations the bound is 1e-5 against the FP64 oracle's CG and 2e-4 against
+    the reference's run (measured 8-10e-5)."""
+    from holotomocupy_b200 import Tomo
+    g = golden("rectomo")
+    n, nz, ntheta, niter = [int(v) for v in g[f"{tag}_dims"]]
+    t = Tomo(n, nz, g[f"{tag}_theta"], 1)
+    d = torch.from_numpy(g[f"{tag}_d"]).cuda()
+    assert rel_l2(t.rec_tomo(d, 1).cpu().numpy(), g[f"{tag}_u1"]) < 1e-5
+    u = t.rec_tomo(d, niter).cpu().numpy()
+    o = O.Tomo(n, nz, g[f"{tag}_theta"], 1, "complex128")
+    ref64 = o.rec_tomo(g[f"{tag}_d"].astype("complex128" if tag == "a" else "float64"), niter)
+    assert rel_l2(u, ref64) < 1e-5
+    assert rel_l2(u, g[f"{tag}_u"]) < 2e-4

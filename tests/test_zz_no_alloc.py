@@ -58,6 +58,10 @@ def test_noalloc_objective_matches_the_allocating_entry_point():
         assert st == 0, _lib.lib().ht_last_error()
         r, v = float(ref), float(out)
         assert np.isfinite(v) and abs(v / r - 1) < 1e-6, (call, v, r)
+    # the sums are reduced in a fixed order: the same inputs give the same bits
+    st, again = _noalloc(rec.cl_prop._h, n, ntheta, c, pos, mag, prb, data)
+    torch.cuda.synchronize()
+    assert st == 0 and float(again) == v
 
 
 def test_noalloc_rejects_sizes_beyond_its_scratch():
