@@ -419,7 +419,12 @@ def main():
         served = served_vs_plain(a.serve_requests, a.serve_iters, 4321 + rank)
 
     line = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
+        "metric": METRIC, "value": value, "unit": UNIT,
+        "served_over_plain": {
+            "single_512_job": ms_plain / ms,
+            "poisson_stream": served["poisson_2_per_s"]["served_over_plain"] if served else None,
+            "saturated_stream": served["saturated"]["served_over_plain"] if served else None},
+        "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
         "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c64",
         "data": "synthetic (seeded ellipsoid phantom, random probe and positions, Poisson noise at 1e4 photons)",
         "config": bench_config(n, ntheta, ndist, world),
@@ -610,7 +615,11 @@ def host_streamed_D(a, n, ndist, nimg=512, chunk=64):
 
 
 def served_vs_plain(nreq, niter, seed):
-    """The mixed request stream through the server and one at a time."""
+    """The mixed request stream through the server and one at a time, twice:
+    with the Poisson arrivals (2/s) and saturated (every request present at
+    t = 0).  Reported per variant: aggregate BH iterations/s, p50/p99
+    per-iteration latency and p50/p99 per-request completion latency (arrival
+    to result on the host)."""
     import torch
     from holotomocupy_b200.serving import Request, Server, run_plain
     from holotomocupy_b200.synthetic import make_problem
@@ -626,23 +635,37 @@ def served_vs_plain(nreq, niter, seed):
         torch.cuda.synchronize()
         torch.cuda.empty_cache()
     total = nreq * niter
-    wall_p, lat_p, _ = run_plain(reqs, realtime=True)
-    torch.cuda.empty_cache()
-    for r in reqs:
-        r.latencies_ms = []
-    srv = Server(max_active=8)
-    for r in reqs:
-        srv.submit(r)
-    srv.run(realtime=True)
-    st = Server.latency_stats(reqs)
-    return {"workload": f"{nreq} requests, n from {{128,256,384,512}} (p 0.4/0.3/0.2/0.1), 1.75 n angles, "
-                        f"4 distances, Poisson arrivals at 2/s, {niter} BH iterations each",
-            "sizes": [int(x) for x in sizes], "iterations": total,
+    out = {"workload": f"{nreq} requests, n from {{128,256,384,512}} (p 0.4/0.3/0.2/0.1), 1.75 n angles, "
+                       f"4 distances, {niter} BH iterations each", "sizes": [int(x) for x in sizes],
+           "iterations": total}
+    for variant, realtime in (("poisson_2_per_s", True), ("saturated", False)):
+        done_plain = []
+        wall_p, lat_p, _ = run_plain(reqs, realtime=realtime, done_times=done_plain)
+        order = sorted(reqs, key=lambda q: q.arrival)
+        comp_p = np.array([d - (q.arrival if realtime else 0.0) for d, q in zip(done_plain, order)])
+        torch.cuda.empty_cache()
+        for r in reqs:
+            r.latencies_ms, r.result, r.t_admit, r.t_done = [], None, None, None
+        srv = Server(max_active=8)
+        for r in reqs:
+            srv.submit(r)
+        srv.run(realtime=realtime)
+        st = Server.latency_stats(reqs)
+        cs = Server.completion_stats(reqs, realtime)
+        out[variant] = {
             "served_iters_per_s": total / srv.wall, "plain_iters_per_s": total / wall_p,
-            "served_wall_s": srv.wall, "plain_wall_s": wall_p,
+            "served_over_plain": wall_p / srv.wall, "served_wall_s": srv.wall, "plain_wall_s": wall_p,
             "served_p50_ms": st["p50_ms"], "served_p99_ms": st["p99_ms"],
             "plain_p50_ms": float(np.percentile(lat_p, 50)), "plain_p99_ms": float(np.percentile(lat_p, 99)),
+            "served_completion_p50_s": cs["p50_s"], "served_completion_p99_s": cs["p99_s"],
+            "plain_completion_p50_s": float(np.percentile(comp_p, 50)),
+            "plain_completion_p99_s": float(np.percentile(comp_p, 99)),
             "max_concurrent": srv.max_concurrent, "peak_bytes_admitted": srv.peak_bytes}
+        for r in reqs:
+            r.latencies_ms, r.result, r.t_admit, r.t_done = [], None, None, None
+        gc.collect()
+        torch.cuda.empty_cache()
+    return out
 
 
 # Algorithmic HBM bytes per work unit of each timed kernel (inputs read once,

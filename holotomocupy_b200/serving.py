@@ -98,6 +98,7 @@ class Server:
         self.done = []
         self.peak_bytes = 0
         self.max_concurrent = 0
+        self.used_bytes = 0       # estimated bytes of the active and not yet released requests
         # one stream per slot, reused by the requests that follow so that the
         # caching allocator hands their freed blocks to the next request
         self._streams = [torch.cuda.Stream(device=self.device) for _ in range(max_active)]
@@ -169,16 +170,16 @@ class Server:
         pending = sorted(self.queue, key=lambda q: q.arrival)
         self.queue = []
         active = []
-        used = 0
+        self.used_bytes = 0
         self._retired = []
         t0 = time.perf_counter()
         while pending or active:
             now = time.perf_counter() - t0
             while pending and len(active) < self.max_active and (not realtime or pending[0].arrival <= now):
                 need = estimate_bytes(pending[0].args)
-                if used + need > self.budget and self._retired:
-                    used -= self._release()
-                if active and used + need > self.budget:
+                if self.used_bytes + need > self.budget and self._retired:
+                    self.used_bytes -= self._release()
+                if active and self.used_bytes + need > self.budget:
                     break
                 r = pending.pop(0)
                 slot = _Slot(r, self._streams.pop())
@@ -191,13 +192,13 @@ class Server:
                     # once the active requests have made room
                     self._streams.append(slot.stream)
                     pending.insert(0, r)
-                    used -= self._release()
+                    self.used_bytes -= self._release()
                     if not active or "out of memory" not in str(err):
                         raise
                     break
                 active.append(slot)
-                used += slot.bytes
-                self.peak_bytes = max(self.peak_bytes, used)
+                self.used_bytes += slot.bytes
+                self.peak_bytes = max(self.peak_bytes, self.used_bytes)
                 self.max_concurrent = max(self.max_concurrent, len(active))
             progressed = False
             for slot in list(active):
@@ -221,8 +222,15 @@ class Server:
                 else:
                     time.sleep(20e-6)
         self.wall = time.perf_counter() - t0
-        self._release()
+        self.used_bytes -= self._release()
         return self.done
+
+    @staticmethod
+    def completion_stats(reqs, realtime=True):
+        """p50/p99 of the per-request completion latency: arrival (or the
+        start of the run when arrivals are ignored) to the result on the host."""
+        lat = np.array([r.t_done - (r.arrival if realtime else 0.0) for r in reqs if r.t_done is not None] or [0.0])
+        return {"p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99))}
 
     @staticmethod
     def latency_stats(reqs):
@@ -233,11 +241,12 @@ class Server:
                 "iterations": int(sum(len(r.latencies_ms) for r in reqs))}
 
 
-def run_plain(reqs, realtime=False):
+def run_plain(reqs, realtime=False, done_times=None):
     """The same requests one at a time through Rec.BH's host-synchronised
     iteration (no graphs, no overlap), in arrival order; realtime=True waits
     for each arrival.  Returns (wall seconds, per-iteration latencies in ms,
-    results)."""
+    results); done_times (a list) receives each request's completion time in
+    seconds from the start."""
     lat = []
     results = []
     t0 = time.perf_counter()
@@ -260,6 +269,8 @@ def run_plain(reqs, realtime=False):
             lat.append(e0.elapsed_time(e1))
         rec.bh_finish()
         results.append({k: rec.vars[k].cpu() for k in ("obj", "prb", "pos")})
+        if done_times is not None:
+            done_times.append(time.perf_counter() - t0)
         rec.close()
         del rec
     torch.cuda.synchronize()

@@ -344,11 +344,25 @@ def c1_cases(ns):
     rec.fwd_tomo(rec.vars["obj"], out=rec.proj_tmp)
     rec.vars["proj"][:] = rec.proj_tmp
     rec.gradients(rec.vars, rec.grads)
+    # the position gradient is a per-image sum over nz * n pixels, which the
+    # reference reduces in FP32 (3.9e-5 from FP64 here): keep the FP64 oracle's
+    # value beside it
+    from oracle import holo_oracle as O
+    from holotomocupy_b200.synthetic import workload_args
+    orc = O.Rec(workload_args(n, ntheta, ndist, niter=1, distances=tuple(distance)), "complex128")
+    orc.eff_demagnifications[:] = 1
+    orc.data[:] = c1_data(ntheta, ndist, n)
+    v64 = {"obj": obj.astype("complex128") * np.float32(0.8) / np.sqrt(n / ntheta),
+           "prb": np.ones((ndist, n, n), "complex128"), "pos": (pos + pos_err).astype("float64")}
+    v64["proj"] = orc.fwd_tomo(v64["obj"])
+    g64 = {k: np.zeros_like(x) for k, x in v64.items()}
+    orc.gradients(v64, g64)
     blk = np.arange(0, ntheta, 30)
     sl = np.array([16, 63, 64, 100])
     out = {"dims": np.array([n, ntheta, ndist]), "distance": distance, "obj": obj, "pos": pos,
            "pos_err": pos_err, "blk": blk, "slices": sl, "proj_blk": proj[blk], "amp_blk": amp[blk],
            "grad_prb": np.asarray(rec.grads["prb"]), "grad_pos": np.asarray(rec.grads["pos"]),
+           "grad_pos_fp64": g64["pos"],
            "grad_obj_sl": np.array(rec.grads["obj"])[sl], "grad_proj_blk": np.array(rec.grads["proj"])[blk]}
     full = {"proj": proj, "amp": amp, "grad_obj": np.array(rec.grads["obj"]),
             "grad_proj": np.array(rec.grads["proj"])}

@@ -86,7 +86,10 @@ def test_c1_adjoint_chain(c1):
     blk = torch.from_numpy(g["blk"]).cuda()
     sl = torch.from_numpy(g["slices"]).cuda()
     assert rel_l2(gr["prb"].cpu().numpy(), g["grad_prb"]) < TOL
-    assert rel_l2(gr["pos"].cpu().numpy(), g["grad_pos"]) < TOL
+    # the position gradient: per-image sums over nz * n pixels, reduced in FP64
+    # here and in FP32 by the reference (its own value is 3.9e-5 from FP64)
+    assert rel_l2(gr["pos"].cpu().numpy(), g["grad_pos_fp64"]) < TOL
+    assert rel_l2(gr["pos"].cpu().numpy(), g["grad_pos"]) < 6e-5
     assert rel_l2(gr["obj"][sl].cpu().numpy(), g["grad_obj_sl"]) < TOL
     assert rel_l2(gr["proj"][blk].cpu().numpy(), g["grad_proj_blk"]) < TOL
     _check_full(gr["obj"], g, "grad_obj")

@@ -93,3 +93,34 @@ def test_device_scalar_iteration_matches_host_iteration():
         np.testing.assert_allclose(np.array(h), np.array(h0), rtol=1e-9)
         for k in v0:
             assert rel_l2(v[k], v0[k]) < 1e-6
+
+
+def test_out_of_memory_admission_returns_the_released_bytes():
+    """An admission that runs out of device memory while a retired request is
+    still held releases it and takes its bytes off the ledger: after the run
+    the ledger is back at zero and every request finished with the result it
+    has alone.  Two slots for three requests: the small first request retires
+    while the 128^3 one runs, and the third request's first admission attempt
+    fails (injected), with the retired request unreleased."""
+    from holotomocupy_b200.serving import Server, estimate_bytes, run_plain
+    reqs = _requests()
+    _, _, alone = run_plain(reqs)
+    big = max(estimate_bytes(r.args) for r in reqs)
+    srv = Server(budget_bytes=4 * big, max_active=2)
+    admit = srv._admit
+    state = {"injected": False}
+
+    def flaky(slot):
+        if not state["injected"] and srv._retired:
+            state["injected"] = True
+            raise torch.OutOfMemoryError("CUDA out of memory (injected)")
+        return admit(slot)
+
+    srv._admit = flaky
+    for r in reqs:
+        srv.submit(r)
+    done = {r.rid: r for r in srv.run(realtime=False)}
+    assert state["injected"]
+    assert srv.used_bytes == 0
+    for r, ref in zip(reqs, alone):
+        assert rel_l2(done[r.rid].result["obj"].numpy(), ref["obj"].numpy()) < 1e-5
