@@ -36,6 +36,8 @@ SIGNATURES = {
     "ht_tomo_RT": [_vp, _vp, _vp, _c_int, _vp],
     "ht_tomo_R_coeffx": [_vp, _vp, _vp, _c_int, _vp],
     "ht_tomo_RT_coeffx": [_vp, _vp, _vp, _c_int, _c_float, _vp],
+    "ht_tomo_R_slab": [_vp, _vp, _vp, _c_int, _c_int, _c_int, _vp],
+    "ht_tomo_RT_slab": [_vp, _vp, _vp, _c_int, _c_int, _c_int, _c_float, _vp],
     "ht_shift_create": [_c_int, _c_int, _c_int, _c_int, _c_int, ctypes.POINTER(_vp)],
     "ht_shift_destroy": [_vp],
     "ht_shift_coeff": [_vp, _vp, _vp, _c_long, _vp],
@@ -64,9 +66,10 @@ SIGNATURES = {
     "ht_rec_create": [_c_int, _c_int, _c_int, _c_int, _c_int, _c_int, _c_int, _vp, ctypes.POINTER(_vp)],
     "ht_rec_destroy": [_vp],
     "ht_rec_forward": [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
-    "ht_rec_gradient": [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _c_float, _c_float, _vp],
+    "ht_rec_gradient": [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _c_float, _c_float, _c_int, _vp],
+    "ht_rec_set_data_size": [_vp, _c_double],
     "ht_rec_objective_noalloc": [_vp, _c_int, _c_int, _c_int, _c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
-    "ht_rec_hessian": [_vp, _vp, _vp, _vp, _vp, _vp, _c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
+    "ht_rec_hessian": [_vp, _vp, _vp, _vp, _vp, _vp, _c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _c_int, _vp],
 }
 _RESTYPE = {"ht_last_error": ctypes.c_char_p, "ht_launch_count": ctypes.c_long}
 

@@ -708,7 +708,7 @@ k_casc_adj(const float2* __restrict__ tmp, float2* __restrict__ Pc, T* __restric
 // ================================================= probe gradient
 // gprb[k, p] = sum_theta P[theta, k, p]  (gF1, rec_mpi.py:641)
 __global__ void k_sum_theta(const float2* __restrict__ Pc, float2* __restrict__ gprb, long ntheta, int ndist,
-                            long npix, float scale) {
+                            long npix, float scale, int acc) {
   const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;  // k * npix + p
   if (i >= (long)ndist * npix) return;
   const int k = (int)(i / npix);
@@ -720,7 +720,13 @@ __global__ void k_sum_theta(const float2* __restrict__ Pc, float2* __restrict__ 
     sy += v.y;
   }
   // the float sum times the variable scaling (rec_mpi.py:345: y[0] * rho_sq['prb'])
-  gprb[i] = make_float2((float)sx * scale, (float)sy * scale);
+  const float2 g = make_float2((float)sx * scale, (float)sy * scale);
+  gprb[i] = acc ? cadd(gprb[i], g) : g;   // acc: an angle chunk adds to the earlier chunks' sum
+}
+
+// dst[i] += src[i] (the objective and Hessian forms of an angle chunk)
+__global__ void k_dacc(double* __restrict__ dst, const double* __restrict__ src, int n) {
+  if (threadIdx.x < n) dst[threadIdx.x] += src[threadIdx.x];
 }
 
 // ================================================= object gradient
@@ -1048,7 +1054,7 @@ k_imgs_glob(const double* __restrict__ imgs, int K, long nimg, double* __restric
 // out[0] = H(y,y), out[1] = H_ref(y,z), out[2] = H(z,z), out[3] = H_sym(y,z)
 __global__ void k_casc_hess_combine(const double* __restrict__ acc_img, const double* __restrict__ glob,
                                     const float* __restrict__ posy, const float* __restrict__ posz, int ndir,
-                                    long nimg, double qscale, double* __restrict__ out) {
+                                    long nimg, double qscale, int acc, double* __restrict__ out) {
   double b00 = 0, b01 = 0, b11 = 0, ayy = 0, azz = 0, ayz = 0, azy = 0;
   for (long i = threadIdx.x; i < nimg; i += blockDim.x) {
     const double* a = acc_img + i * kNAcc;
@@ -1081,15 +1087,14 @@ __global__ void k_casc_hess_combine(const double* __restrict__ acc_img, const do
     azz = red[4][0];
     ayz = red[5][0];
     azy = red[6][0];
-    out[0] = qscale * glob[kQ0] + glob[kL10] + glob[kL20] + b00 + 2.0 * ayy;
+    double h[4] = {qscale * glob[kQ0] + glob[kL10] + glob[kL20] + b00 + 2.0 * ayy, 0.0, 0.0, 0.0};
     if (ndir == 2) {
       const double common = qscale * glob[kQ1] + glob[kL11] + glob[kL21] + b01;
-      out[1] = common + ayy + azz;
-      out[2] = qscale * glob[kQ2] + glob[kL12] + glob[kL22] + b11 + 2.0 * azz;
-      out[3] = common + ayz + azy;
-    } else {
-      out[1] = out[2] = out[3] = 0.0;
+      h[1] = common + ayy + azz;
+      h[2] = qscale * glob[kQ2] + glob[kL12] + glob[kL22] + b11 + 2.0 * azz;
+      h[3] = common + ayz + azy;
     }
+    for (int i = 0; i < 4; ++i) out[i] = acc ? out[i] + h[i] : h[i];   // acc: an angle chunk
   }
 }
 
@@ -1109,6 +1114,7 @@ struct ht_rec_s {
   double* glob;    // [kNGlob]
   double* rows;    // [nimg * nz, kRowKMax] per-row sums of the row kernels
   double* imgs;    // [nimg, kRowKMax] their per-image sums
+  double ndata;    // N of the objective's 2/N: ntheta*ndist*nz*n, or the whole problem's for an angle chunk
 };
 
 extern "C" int ht_rec_create(int n, int nz, int nobj, int nzobj, int ntheta, int ndist, int is_complex,
@@ -1130,6 +1136,7 @@ extern "C" int ht_rec_create(int n, int nz, int nobj, int nzobj, int ntheta, int
   ht_rec_s* r = new ht_rec_s{};
   r->D = CascDims{n, nz, nobj, nzobj, ndist, (long)ntheta * ndist};
   r->ntheta = ntheta;
+  r->ndata = (double)ntheta * ndist * nz * n;
   r->is_complex = is_complex ? 1 : 0;
   r->prop = prop;
   cudaGetDevice(&r->device);
@@ -1253,7 +1260,7 @@ static cudaError_t resid_pass(ht_rec_s* r, const float* data, float* amp, float 
 template <int N, class T>
 static cudaError_t grad_impl(ht_rec_s* r, const void* c, const float* pos, const float* mag, const float2* prb,
                              const float* data, void* gc, float* gpos, float2* gprb, float scale, float spos,
-                             float sprb, cudaStream_t st) {
+                             float sprb, int acc, cudaStream_t st) {
   const float2 *hw, *twn, *twz;
   prop_tables(r->prop, &hw, &twn, &twz);
   cudaError_t e = fwd_pass<N, T>(r, c, pos, mag, prb, hw, twn, twz, st);
@@ -1281,7 +1288,7 @@ static cudaError_t grad_impl(ht_rec_s* r, const void* c, const float* pos, const
   if ((e = reduce_rows(r, 5, kAx, 0, 5, 0, 0, st)) != cudaSuccess) return e;
   const long npix = (long)r->D.nz * N;
   k_sum_theta<<<(unsigned)((r->D.ndist * npix + 255) / 256), 256, 0, st>>>(r->P, gprb, r->ntheta, r->D.ndist, npix,
-                                                                             sprb);
+                                                                             sprb, acc);
   ::ht::count_launch();
   dim3 g2((r->D.nobj + 31) / 32, (r->D.nzobj + 8 * kVRows - 1) / (8 * kVRows), r->ntheta);
   k_casc_vsum<T><<<g2, dim3(32, 8), 0, st>>>((T*)gc, hbuf, pos, mag, r->D); ::ht::count_launch();
@@ -1361,24 +1368,33 @@ extern "C" int ht_rec_forward(ht_rec_s* r, const void* c, const float* pos, cons
   return kOk;
 }
 
+extern "C" int ht_rec_set_data_size(ht_rec_s* r, double ndata) {
+  using namespace ht;
+  HT_REQUIRE(r, "ht_rec_set_data_size: null pointer");
+  HT_REQUIRE(ndata >= (double)r->ntheta * r->D.ndist * r->D.nz * r->D.n,
+             "ht_rec_set_data_size: N is smaller than the handle's own ntheta*ndist*nz*n");
+  r->ndata = ndata;
+  return kOk;
+}
+
 extern "C" int ht_rec_gradient(ht_rec_s* r, const void* c, const float* pos, const float* mag, const void* prb,
                                const float* data, void* gc, float* gpos, void* gprb, double* fval, float scale_pos,
-                               float scale_prb, void* stream) {
+                               float scale_prb, int accumulate, void* stream) {
   using namespace ht;
   HT_REQUIRE(r && c && pos && mag && prb && data && gc && gpos && gprb, "ht_rec_gradient: null pointer");
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   HT_CHECK_CUDA(cudaMemsetAsync(r->glob, 0, sizeof(double) * kNGlob, st));
   HT_CHECK_CUDA(cudaMemsetAsync(r->acc_img, 0, sizeof(double) * r->D.nimg * kNAcc, st));
   // rec_mpi.py:569: np.float32(2 / data_size)
-  const float scale = (float)(2.0 / ((double)r->ntheta * r->D.ndist * r->D.nz * r->D.n));
+  const float scale = (float)(2.0 / r->ndata);
   cudaError_t e = cudaErrorInvalidValue;
   switch (r->D.n) {
 #define X(S)                                                                                                     \
   case S:                                                                                                        \
     e = r->is_complex ? grad_impl<S, float2>(r, c, pos, mag, (const float2*)prb, data, gc, gpos, (float2*)gprb,    \
-                                             scale, scale_pos, scale_prb, st)                                    \
+                                             scale, scale_pos, scale_prb, accumulate, st)                        \
                       : grad_impl<S, float>(r, c, pos, mag, (const float2*)prb, data, gc, gpos, (float2*)gprb,     \
-                                            scale, scale_pos, scale_prb, st);                                    \
+                                            scale, scale_pos, scale_prb, accumulate, st);                        \
     break;
     HT_REC_SIZES(X)
 #undef X
@@ -1386,13 +1402,20 @@ extern "C" int ht_rec_gradient(ht_rec_s* r, const void* c, const float* pos, con
       break;
   }
   HT_CHECK_CUDA(e);
-  if (fval) HT_CHECK_CUDA(cudaMemcpyAsync(fval, r->glob + kF, sizeof(double), cudaMemcpyDeviceToDevice, st));
+  if (fval && accumulate) {
+    k_dacc<<<1, 32, 0, st>>>(fval, r->glob + kF, 1);
+    ::ht::count_launch();
+    HT_CHECK_CUDA(cudaGetLastError());
+  } else if (fval) {
+    HT_CHECK_CUDA(cudaMemcpyAsync(fval, r->glob + kF, sizeof(double), cudaMemcpyDeviceToDevice, st));
+  }
   return kOk;
 }
 
 extern "C" int ht_rec_hessian(ht_rec_s* r, const void* c, const float* pos, const float* mag, const void* prb,
                               const float* data, int ndir, const void* cy, const float* posy, const void* prby,
-                              const void* cz, const float* posz, const void* prbz, double* out, void* stream) {
+                              const void* cz, const float* posz, const void* prbz, double* out, int accumulate,
+                              void* stream) {
   using namespace ht;
   HT_REQUIRE(r && c && pos && mag && prb && data && cy && posy && prby && out, "ht_rec_hessian: null pointer");
   HT_REQUIRE(ndir == 1 || (ndir == 2 && cz && posz && prbz), "ht_rec_hessian: ndir must be 1, or 2 with z given");
@@ -1418,9 +1441,10 @@ extern "C" int ht_rec_hessian(ht_rec_s* r, const void* c, const float* pos, cons
       break;
   }
   HT_CHECK_CUDA(e);
-  const double qscale = 2.0 / ((double)r->ntheta * r->D.ndist * r->D.nz * r->D.n);
+  const double qscale = 2.0 / r->ndata;
   k_casc_hess_combine<<<1, 256, 0, st>>>(r->acc_img, r->glob, posy, ndir == 2 ? posz : posy, ndir, r->D.nimg, qscale,
-                                         out); ::ht::count_launch();
+                                         accumulate, out);
+  ::ht::count_launch();
   HT_CHECK_CUDA(cudaGetLastError());
   return kOk;
 }

@@ -178,7 +178,7 @@ constexpr int gather_max_regs() {
 
 template <int N, int THREADS = ZCfg<N, TZ<2 * N>::Z>::THREADS>
 __global__ void __maxnreg__(gather_max_regs<THREADS>())
-k_tgather(const float2* __restrict__ fde, float2* __restrict__ sino, GatherGeom G, int nz,
+k_tgather(const float2* __restrict__ fde, float2* __restrict__ sino, GatherGeom G, int nz, int ldz,
           const float2* __restrict__ tw4, const float* __restrict__ symx) {
   constexpr int Z = TZ<2 * N>::Z;
   constexpr int Q = Z / 2;                       // lanes per sample
@@ -231,7 +231,7 @@ k_tgather(const float2* __restrict__ fde, float2* __restrict__ sino, GatherGeom 
   fft_line<N, true>(zline<N, Z>(smem, l), t, tw4, line_sync<T>());
   const int z = zb * Z + l;
   if (z >= nz) return;
-  float2* dst = sino + ((long)th * nz + z) * N;
+  float2* dst = sino + ((long)th * ldz + z) * N;  // ldz: rows per angle of the sinogram
   SmRow sm = zline<N, Z>(smem, l);
   for (int k = t; k < N; k += T) {
     const float s = ((k & 1) ? -1.f : 1.f) / (4.f * (float)N);  // ifft 1/n, (-1)^k, /4
@@ -243,7 +243,7 @@ k_tgather(const float2* __restrict__ fde, float2* __restrict__ sino, GatherGeom 
 // sino [ntheta, nz, n] -> gs [zb][ntheta][n][Z];  grid (ntheta, nzb)
 template <int N>
 __global__ void __launch_bounds__(ZCfg<N, TZ<2 * N>::Z>::THREADS)
-k_tsino_fft(const float2* __restrict__ sino, float2* __restrict__ gs, int ntheta, int nz,
+k_tsino_fft(const float2* __restrict__ sino, float2* __restrict__ gs, int ntheta, int nz, int ldz,
             const float2* __restrict__ tw4, const float* __restrict__ symx, float scale) {
   constexpr int Z = TZ<2 * N>::Z;
   constexpr int T = ZCfg<N, Z>::T;
@@ -253,7 +253,7 @@ k_tsino_fft(const float2* __restrict__ sino, float2* __restrict__ gs, int ntheta
   const int z = zb * Z + l;
   SmRow sm = zline<N, Z>(smem, l);
   for (int k = t; k < N; k += T) {
-    float2 v = (z < nz) ? sino[((long)th * nz + z) * N + k] : make_float2(0.f, 0.f);
+    float2 v = (z < nz) ? sino[((long)th * ldz + z) * N + k] : make_float2(0.f, 0.f);
     if (k & 1) v = make_float2(-v.x, -v.y);
     sm.st(k, v);
   }
@@ -550,7 +550,7 @@ k_trow_adj(const float2* __restrict__ fb, const float* __restrict__ phi, float2*
 // ================================================================ launch
 template <int N2>
 static cudaError_t tomo_R_sized(const float2* obj, float2* sino, const float* phi, float2* fa, float2* fde,
-                                const GatherGeom& G, int nz, const float2* tw_n, const float2* tw_2n,
+                                const GatherGeom& G, int nz, int ldz, const float2* tw_n, const float2* tw_2n,
                                 const float* symx, cudaStream_t st) {
   constexpr int n = N2 / 2;
   constexpr int Z = TZ<N2>::Z;
@@ -567,7 +567,7 @@ static cudaError_t tomo_R_sized(const float2* obj, float2* sino, const float* ph
   count_launch();
   {
     KTimer kt("k_tgather", st, (double)nz);
-    k_tgather<n><<<dim3(G.ntheta, nzb), C1::THREADS, C1::SMEM, st>>>(fde, sino, G, nz, tw_n, symx);
+    k_tgather<n><<<dim3(G.ntheta, nzb), C1::THREADS, C1::SMEM, st>>>(fde, sino, G, nz, ldz, tw_n, symx);
   }
   count_launch();
   return cudaGetLastError();
@@ -581,7 +581,8 @@ struct CellLists {
 
 template <int N2>
 static cudaError_t tomo_RT_sized(const float2* sino, float2* obj, const float* phi, float2* fab, float2* fde,
-                                 float2* gs, const GatherGeom& G, const CellLists& L, int nz, const float2* tw_n,
+                                 float2* gs, const GatherGeom& G, const CellLists& L, int nz, int ldz,
+                                 const float2* tw_n,
                                  const float2* tw_2n, const float* symx, float scale, cudaStream_t st) {
   constexpr int n = N2 / 2;
   constexpr int Z = TZ<N2>::Z;
@@ -592,7 +593,8 @@ static cudaError_t tomo_RT_sized(const float2* sino, float2* obj, const float* p
   if ((e = allow_smem(k_tsino_fft<n>, C1::SMEM)) != cudaSuccess) return e;
   if ((e = allow_smem(k_tcol_adj<N2>, C2::SMEM)) != cudaSuccess) return e;
   if ((e = allow_smem(k_trow_adj<N2>, C2::SMEM)) != cudaSuccess) return e;
-  k_tsino_fft<n><<<dim3(G.ntheta, nzb), C1::THREADS, C1::SMEM, st>>>(sino, gs, G.ntheta, nz, tw_n, symx, scale);
+  k_tsino_fft<n><<<dim3(G.ntheta, nzb), C1::THREADS, C1::SMEM, st>>>(sino, gs, G.ntheta, nz, ldz, tw_n, symx,
+                                                                    scale);
   count_launch();
   {
     KTimer kt("k_tcell", st, (double)nz);
@@ -811,9 +813,10 @@ static cudaError_t build_cell_lists(ht_tomo_s* t) {
 }  // namespace ht
 
 namespace ht {
-static int tomo_R(ht_tomo_s* t, const void* obj, void* sino, int nz, bool filt, void* stream) {
+static int tomo_R(ht_tomo_s* t, const void* obj, void* sino, int nz, int ldz, bool filt, void* stream) {
   HT_REQUIRE(t && obj && sino, "ht_tomo_R: null pointer");
   HT_REQUIRE(nz >= 0 && nz <= t->nz, "ht_tomo_R: nz exceeds the handle's slice capacity");
+  HT_REQUIRE(ldz >= nz, "ht_tomo_R: ldz must be at least nz");
   if (nz == 0) return kOk;
   const GatherGeom G = geom(t);
   cudaStream_t st = static_cast<cudaStream_t>(stream);
@@ -823,7 +826,7 @@ static int tomo_R(ht_tomo_s* t, const void* obj, void* sino, int nz, bool filt, 
 #define X(A, B)                                                                                             \
   case A:                                                                                                   \
     e = tomo_R_sized<B>(static_cast<const float2*>(obj), static_cast<float2*>(sino), t->phi, t->fab, t->fde, G, \
-                        nz, t->tw_n, t->tw_2n, symx, st);                                                   \
+                        nz, ldz, t->tw_n, t->tw_2n, symx, st);                                              \
     break;
     HT_TOMO_SIZES(X)
 #undef X
@@ -834,9 +837,11 @@ static int tomo_R(ht_tomo_s* t, const void* obj, void* sino, int nz, bool filt, 
   return kOk;
 }
 
-static int tomo_RT(ht_tomo_s* t, const void* sino, void* obj, int nz, bool filt, float scale, void* stream) {
+static int tomo_RT(ht_tomo_s* t, const void* sino, void* obj, int nz, int ldz, bool filt, float scale,
+                   void* stream) {
   HT_REQUIRE(t && obj && sino, "ht_tomo_RT: null pointer");
   HT_REQUIRE(nz >= 0 && nz <= t->nz, "ht_tomo_RT: nz exceeds the handle's slice capacity");
+  HT_REQUIRE(ldz >= nz, "ht_tomo_RT: ldz must be at least nz");
   if (nz == 0) return kOk;
   const GatherGeom G = geom(t);
   cudaStream_t st = static_cast<cudaStream_t>(stream);
@@ -846,7 +851,7 @@ static int tomo_RT(ht_tomo_s* t, const void* sino, void* obj, int nz, bool filt,
 #define X(A, B)                                                                                                 \
   case A:                                                                                                       \
     e = tomo_RT_sized<B>(static_cast<const float2*>(sino), static_cast<float2*>(obj), t->phi, t->fab, t->fde,    \
-                         t->gs, G, CellLists{t->cl_len, t->cl_off, t->cl_ent}, nz, t->tw_n, t->tw_2n, symx,      \
+                         t->gs, G, CellLists{t->cl_len, t->cl_off, t->cl_ent}, nz, ldz, t->tw_n, t->tw_2n, symx, \
                          scale, st);                                                                                \
     break;
     HT_TOMO_SIZES(X)
@@ -860,17 +865,26 @@ static int tomo_RT(ht_tomo_s* t, const void* sino, void* obj, int nz, bool filt,
 }  // namespace ht
 
 extern "C" int ht_tomo_R(ht_tomo_s* t, const void* obj, void* sino, int nz, void* stream) {
-  return ht::tomo_R(t, obj, sino, nz, false, stream);
+  return ht::tomo_R(t, obj, sino, nz, nz, false, stream);
 }
 
 extern "C" int ht_tomo_RT(ht_tomo_s* t, const void* sino, void* obj, int nz, void* stream) {
-  return ht::tomo_RT(t, sino, obj, nz, false, 1.0f, stream);
+  return ht::tomo_RT(t, sino, obj, nz, nz, false, 1.0f, stream);
 }
 
 extern "C" int ht_tomo_R_coeffx(ht_tomo_s* t, const void* obj, void* sino, int nz, void* stream) {
-  return ht::tomo_R(t, obj, sino, nz, true, stream);
+  return ht::tomo_R(t, obj, sino, nz, nz, true, stream);
 }
 
 extern "C" int ht_tomo_RT_coeffx(ht_tomo_s* t, const void* sino, void* obj, int nz, float scale, void* stream) {
-  return ht::tomo_RT(t, sino, obj, nz, true, scale, stream);
+  return ht::tomo_RT(t, sino, obj, nz, nz, true, scale, stream);
+}
+
+extern "C" int ht_tomo_R_slab(ht_tomo_s* t, const void* obj, void* sino, int nz, int ldz, int coeffx, void* stream) {
+  return ht::tomo_R(t, obj, sino, nz, ldz, coeffx != 0, stream);
+}
+
+extern "C" int ht_tomo_RT_slab(ht_tomo_s* t, const void* sino, void* obj, int nz, int ldz, int coeffx, float scale,
+                               void* stream) {
+  return ht::tomo_RT(t, sino, obj, nz, ldz, coeffx != 0, scale, stream);
 }

@@ -81,7 +81,12 @@ class Rec:
         self.complex_obj = self.obj_dtype == "complex64"
         self.odt = torch.complex64 if self.complex_obj else torch.float32
         theta = np.asarray(self.theta.cpu() if isinstance(self.theta, torch.Tensor) else self.theta)
-        self.cl_tomo = Tomo(self.nobj, self.nzobj, theta, self.mask)
+        # angle chunks of the fused cascade and object slabs of the Radon
+        # transform (None: all at once); the chunked iteration recomputes each
+        # angle chunk's forward pass before its Hessian pass
+        self.angle_chunk = min(int(getattr(self, "angle_chunk", None) or self.ntheta), self.ntheta)
+        self.slab_chunk = min(int(getattr(self, "slab_chunk", None) or self.nzobj), self.nzobj)
+        self.cl_tomo = Tomo(self.nobj, self.slab_chunk, theta, self.mask)
         self.cl_prop = Propagation(self.n, self.nz, self.ntheta, self.ndist, wavelength, voxelsize, distance)
         self.cl_shift = Shift(self.n, self.nobj, self.nz, self.nzobj, self.obj_dtype)
         self.norm_const = float(np.float32(np.sqrt(self.nobj / self.ntheta)))   # rec_mpi.py:88
@@ -92,9 +97,11 @@ class Rec:
         self.table = []
         self.alloc_arrays()
         h = ctypes.c_void_p()
-        _lib.call("ht_rec_create", self.n, self.nz, self.nobj, self.nzobj, self.ntheta, self.ndist,
+        _lib.call("ht_rec_create", self.n, self.nz, self.nobj, self.nzobj, self.angle_chunk, self.ndist,
                   1 if self.complex_obj else 0, self.cl_prop._h, ctypes.byref(h))
         self._h = h
+        if self.angle_chunk < self.ntheta:
+            _lib.call("ht_rec_set_data_size", h, float(self.data_size))
         self._scal = torch.zeros(8, dtype=torch.float64, device=dev)
 
     # the reference's operator lists (rec_mpi.py:38-45), built on access so
@@ -196,10 +203,35 @@ class Rec:
                   _lib.ptr(dot) if dot is not None else None, _lib.stream_ptr())
 
     # -------------------------------------------------- fused cascade
+    # ---------------------------------------------------- angle chunks
+    def _chunks(self):
+        """(first angle, angles) of each angle chunk of the fused cascade."""
+        for th0 in range(0, self.ntheta, self.angle_chunk):
+            yield th0, min(self.angle_chunk, self.ntheta - th0)
+
+    @staticmethod
+    def _at(t, th0):
+        """Address of angle th0 of an angle-major array (an angle chunk)."""
+        return ctypes.c_void_p(t.data_ptr() + th0 * (t.numel() // t.shape[0]) * t.element_size())
+
+    def _forward(self, c, pos, mag, prb, data=None, amp=None):
+        """ht_rec_forward over the angle chunks: amplitudes into amp, or the
+        objective sum (|x0| - data)^2 returned as a float."""
+        total, st = 0.0, _lib.stream_ptr()
+        for th0, _ in self._chunks():
+            _lib.call("ht_rec_forward", self._h, self._at(c, th0), self._at(pos, th0), self._at(mag, th0),
+                      _lib.ptr(prb), self._at(data, th0) if data is not None else None,
+                      self._at(amp, th0) if amp is not None else None,
+                      _lib.ptr(self._scal) if data is not None else None, st)
+            if data is not None:
+                total += float(self._scal[0])
+        return total
+
     def _gradient_pass(self, c, pos, prb, persistent=False, gpos=None, gprb=None, scale_pos=1.0, scale_prb=1.0):
         """Fused gF0..gF3 (rec_mpi.py:327-353): returns (sum_k S^T Y22, gpos, gprb), F in _scal[0].
         persistent=True writes gc into the Rec's own array (no allocation);
-        gpos / gprb given: written there, times scale_pos / scale_prb."""
+        gpos / gprb given: written there, times scale_pos / scale_prb.  Angle
+        chunks run in turn, the probe gradient and F accumulated."""
         gc = self._gc if persistent else torch.empty_like(c)
         if gpos is None:
             gpos = self._gpos if persistent else torch.empty(self.ntheta, self.ndist, 2, dtype=torch.float32,
@@ -207,22 +239,38 @@ class Rec:
         if gprb is None:
             gprb = self._gprb if persistent else torch.empty(self.ndist, self.nz, self.n, dtype=torch.complex64,
                                                              device=self.device)
-        _lib.call("ht_rec_gradient", self._h, _lib.ptr(c), _lib.ptr(pos), _lib.ptr(self.eff_demagnifications),
-                  _lib.ptr(prb), _lib.ptr(self.data), _lib.ptr(gc), _lib.ptr(gpos), _lib.ptr(gprb),
-                  _lib.ptr(self._scal), float(scale_pos), float(scale_prb), _lib.stream_ptr())
+        mag, st = self.eff_demagnifications, _lib.stream_ptr()
+        for k, (th0, _) in enumerate(self._chunks()):
+            _lib.call("ht_rec_gradient", self._h, self._at(c, th0), self._at(pos, th0), self._at(mag, th0),
+                      _lib.ptr(prb), self._at(self.data, th0), self._at(gc, th0), self._at(gpos, th0), _lib.ptr(gprb),
+                      _lib.ptr(self._scal), float(scale_pos), float(scale_prb), int(k > 0), st)
         return gc, gpos, gprb
 
     def _hessian_pass(self, c, pos, prb, y, z=None, out=None):
         """Fused Hessian forms; y, z = (coefficients, pos, prb) of the directions.
-        Returns float64 tensor [H(y,y), H_ref(y,z), H(z,z), H_sym(y,z)]."""
+        Returns float64 tensor [H(y,y), H_ref(y,z), H(z,z), H_sym(y,z)].  With
+        angle chunks, each chunk's forward and adjoint caches are recomputed
+        (its gradient call, outputs discarded) before its Hessian call."""
         if out is None:
             out = torch.zeros(4, dtype=torch.float64, device=self.device)
         zz = z if z is not None else (None, None, None)
-        _lib.call("ht_rec_hessian", self._h, _lib.ptr(c), _lib.ptr(pos), _lib.ptr(self.eff_demagnifications),
-                  _lib.ptr(prb), _lib.ptr(self.data), 2 if z is not None else 1, _lib.ptr(y[0]), _lib.ptr(y[1]),
-                  _lib.ptr(y[2]), _lib.ptr(zz[0]) if z is not None else None,
-                  _lib.ptr(zz[1]) if z is not None else None, _lib.ptr(zz[2]) if z is not None else None,
-                  _lib.ptr(out), _lib.stream_ptr())
+        mag, st = self.eff_demagnifications, _lib.stream_ptr()
+        chunked = self.angle_chunk < self.ntheta
+        if chunked and getattr(self, "_scratch", None) is None:
+            self._scratch = (torch.empty((self.angle_chunk,) + tuple(c.shape[1:]), dtype=c.dtype, device=self.device),
+                             torch.empty(self.angle_chunk, self.ndist, 2, dtype=torch.float32, device=self.device),
+                             torch.empty(self.ndist, self.nz, self.n, dtype=torch.complex64, device=self.device))
+        at = self._at
+        for k, (th0, _) in enumerate(self._chunks()):
+            if chunked:
+                sc, sp, sq = self._scratch
+                _lib.call("ht_rec_gradient", self._h, at(c, th0), at(pos, th0), at(mag, th0), _lib.ptr(prb),
+                          at(self.data, th0), _lib.ptr(sc), _lib.ptr(sp), _lib.ptr(sq),
+                          ctypes.c_void_p(self._scal.data_ptr() + 8), 1.0, 1.0, 0, st)
+            _lib.call("ht_rec_hessian", self._h, at(c, th0), at(pos, th0), at(mag, th0), _lib.ptr(prb),
+                      at(self.data, th0), 2 if z is not None else 1, at(y[0], th0), at(y[1], th0), _lib.ptr(y[2]),
+                      at(zz[0], th0) if z is not None else None, at(zz[1], th0) if z is not None else None,
+                      _lib.ptr(zz[2]) if z is not None else None, _lib.ptr(out), int(k > 0), st)
         return out
 
     def _contig(self, d):
@@ -328,10 +376,8 @@ class Rec:
         out = 0.0
         if not prbfit_only:
             c = self._coeff_into(proj.contiguous(), torch.empty_like(proj))
-            _lib.call("ht_rec_forward", self._h, _lib.ptr(c), _lib.ptr(pos.contiguous()),
-                      _lib.ptr(self.eff_demagnifications), _lib.ptr(prb.contiguous()), _lib.ptr(self.data), None,
-                      _lib.ptr(self._scal), _lib.stream_ptr())
-            out = float(self._scal[0]) / self.data_size
+            out = self._forward(c, pos.contiguous(), self.eff_demagnifications, prb.contiguous(),
+                                data=self.data) / self.data_size
         if self.lam_prbfit != 0:
             for j in range(self.ndist):
                 Dprb = self.cl_prop.D(prb[j: j + 1].contiguous(), j)[0]
@@ -346,8 +392,7 @@ class Rec:
         vars["obj"] /= self.norm_const
         self.fwd_tomo(vars["obj"], out=vars["proj"])
         c = self._coeff_into(vars["proj"], torch.empty_like(vars["proj"]))
-        _lib.call("ht_rec_forward", self._h, _lib.ptr(c), _lib.ptr(vars["pos"]), _lib.ptr(self.eff_demagnifications),
-                  _lib.ptr(vars["prb"]), None, _lib.ptr(out), None, _lib.stream_ptr())
+        self._forward(c, vars["pos"], self.eff_demagnifications, vars["prb"], amp=out)
         vars["obj"] *= self.norm_const
 
     def forward_amplitudes(self, obj, prb, pos, out=None):
@@ -361,8 +406,7 @@ class Rec:
         del proj
         if out is None:
             out = torch.empty(self.ntheta, self.ndist, self.nz, self.n, dtype=torch.float32, device=self.device)
-        _lib.call("ht_rec_forward", self._h, _lib.ptr(c), _lib.ptr(pos.contiguous()), _lib.ptr(eff),
-                  _lib.ptr(prb.contiguous()), None, _lib.ptr(out), None, _lib.stream_ptr())
+        self._forward(c, pos.contiguous(), eff, prb.contiguous(), amp=out)
         return out
 
     def gen_sqrt_ref(self, prb, out):
@@ -445,13 +489,12 @@ class Rec:
         if self._fold:
             # grads obj = rho R^T coeff(gc) = rho Cz R^T Cx gc;  C grads = coeff(R grads obj) = Cx R Cz grads obj
             st, nc = _lib.stream_ptr(), self.nobj * self.nobj
-            _lib.call("ht_tomo_RT_coeffx", self.cl_tomo._h, _lib.ptr(gc), _lib.ptr(grads["obj"]), self.nzobj,
-                      float(rho["obj"]), st)
+            self.cl_tomo._RT_into(gc, grads["obj"], coeffx=True, scale=rho["obj"])
             _lib.call("ht_shift_coeff_z", self.cl_shift._hc, _lib.ptr(grads["obj"]), _lib.ptr(grads["obj"]), nc, st)
             self.gradient_laplacian(grads["obj"])
             self.gradient_prbfit(grads["prb"], vars["prb"])
             _lib.call("ht_shift_coeff_z", self.cl_shift._hc, _lib.ptr(grads["obj"]), _lib.ptr(self._vol), nc, st)
-            _lib.call("ht_tomo_R_coeffx", self.cl_tomo._h, _lib.ptr(self._vol), _lib.ptr(C["grads"]), self.nzobj, st)
+            self.cl_tomo._R_into(self._vol, C["grads"], coeffx=True)
         else:
             self._coeff_into(gc, grads["proj"])
             grads["proj"] *= rho["obj"]
@@ -571,10 +614,8 @@ class Rec:
         if self.err_step == -1 or i % self.err_step != 0:
             return
         if self._fold and i >= 0:   # proj is not kept up to date inside BH: use its coefficients
-            _lib.call("ht_rec_forward", self._h, _lib.ptr(self._c["vars"]), _lib.ptr(vars["pos"]),
-                      _lib.ptr(self.eff_demagnifications), _lib.ptr(vars["prb"]), _lib.ptr(self.data), None,
-                      _lib.ptr(self._scal), _lib.stream_ptr())
-            err = float(self._scal[0]) / self.data_size + self._lap_energy()
+            err = self._forward(self._c["vars"], vars["pos"], self.eff_demagnifications, vars["prb"],
+                                data=self.data) / self.data_size + self._lap_energy()
             if self.lam_prbfit != 0:
                 err += self.min(vars["prb"], None, vars["pos"], None, prbfit_only=True)
         else:

@@ -85,18 +85,47 @@ class Tomo:
                 pass
             self._h = None
 
+    # ------------------------------------------------ slabs of object slices
+    # The handle's workspace holds `nz` slices (the constructor's nz); a taller
+    # volume is transformed slab by slab, each slab's sinogram rows written in
+    # place inside the full sinogram (row stride ldz = the volume's height).
+    def _slabs(self, nz):
+        for z0 in range(0, nz, self._nz):
+            yield z0, min(self._nz, nz - z0)
+
+    def _R_into(self, x, res, coeffx=False):
+        """res[ntheta, nz, n] = R(x[nz, n, n]) (complex64, contiguous), with the
+        detector-axis B-spline prefilter when coeffx (ht_tomo_R_slab)."""
+        nz, st = x.shape[0], _lib.stream_ptr()
+        row = self.n * 8
+        with torch.cuda.device(x.device):
+            for z0, nzs in self._slabs(nz):
+                _lib.call("ht_tomo_R_slab", self._h, _lib.ptr(x[z0]), ctypes.c_void_p(res.data_ptr() + z0 * row), nzs,
+                          nz, int(coeffx), st)
+        return res
+
+    def _RT_into(self, d, res, coeffx=False, scale=1.0):
+        """res[nz, n, n] = scale R^T(d[ntheta, nz, n]) (complex64, contiguous)."""
+        nz, st = d.shape[1], _lib.stream_ptr()
+        row = self.n * 8
+        with torch.cuda.device(d.device):
+            for z0, nzs in self._slabs(nz):
+                _lib.call("ht_tomo_RT_slab", self._h, ctypes.c_void_p(d.data_ptr() + z0 * row), _lib.ptr(res[z0]),
+                          nzs, nz, int(coeffx), float(scale), st)
+        return res
+
     def R(self, obj, out=None):
-        """Radon transform (tomo.py:56-86): [nz, n, n] -> [ntheta, nz, n]."""
+        """Radon transform (tomo.py:56-86): [nz, n, n] -> [ntheta, nz, n] (any nz:
+        volumes taller than the handle's slab run slab by slab)."""
         _lib.require_cuda(obj, "obj")
         nz = obj.shape[0]
-        if tuple(obj.shape[1:]) != (self.n, self.n) or nz > self._nz:
-            raise ValueError(f"obj must be [<= {self._nz}, {self.n}, {self.n}], got {tuple(obj.shape)}")
+        if tuple(obj.shape[1:]) != (self.n, self.n):
+            raise ValueError(f"obj must be [nz, {self.n}, {self.n}], got {tuple(obj.shape)}")
         real = not obj.is_complex()
         x = obj.to(torch.complex64).contiguous()
         res = out if (out is not None and not real) else torch.empty(self.ntheta, nz, self.n, dtype=torch.complex64,
                                                                      device=x.device)
-        with torch.cuda.device(x.device):
-            _lib.call("ht_tomo_R", self._h, _lib.ptr(x), _lib.ptr(res), nz, _lib.stream_ptr())
+        self._R_into(x, res)
         if real:
             res = res.real.contiguous()
             if out is not None:
@@ -108,14 +137,13 @@ class Tomo:
         """Adjoint Radon transform (tomo.py:88-116): [ntheta, nz, n] -> [nz, n, n]."""
         _lib.require_cuda(data, "data")
         nz = data.shape[1]
-        if data.shape[0] != self.ntheta or data.shape[2] != self.n or nz > self._nz:
-            raise ValueError(f"data must be [{self.ntheta}, <= {self._nz}, {self.n}], got {tuple(data.shape)}")
+        if data.shape[0] != self.ntheta or data.shape[2] != self.n:
+            raise ValueError(f"data must be [{self.ntheta}, nz, {self.n}], got {tuple(data.shape)}")
         real = not data.is_complex()
         x = data.to(torch.complex64).contiguous()
         res = out if (out is not None and not real) else torch.empty(nz, self.n, self.n, dtype=torch.complex64,
                                                                      device=x.device)
-        with torch.cuda.device(x.device):
-            _lib.call("ht_tomo_RT", self._h, _lib.ptr(x), _lib.ptr(res), nz, _lib.stream_ptr())
+        self._RT_into(x, res)
         if real:
             res = res.real.contiguous()
             if out is not None:

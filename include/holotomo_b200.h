@@ -117,6 +117,15 @@ int ht_tomo_R_coeffx(ht_tomo_s* t, const void* obj, void* sino, int nz, void* st
 /* ... and obj = scale * R^T(Cx sino): the BH variable scaling rho of the
  * object gradient (rec_mpi.py:345) applied in the same pass. */
 int ht_tomo_RT_coeffx(ht_tomo_s* t, const void* sino, void* obj, int nz, float scale, void* stream);
+/* R and R^T of a slab of nz object slices inside a taller sinogram (object
+ * slabs processed in turn when the handle's workspace holds fewer slices
+ * than the volume): the slab's row z of angle th is at sino[(th * ldz + z) *
+ * n], sino offset to the slab's first row, ldz >= nz the sinogram's rows per
+ * angle.  coeffx = 1: with the detector-axis prefilter of the _coeffx forms;
+ * scale multiplies R^T's result. */
+int ht_tomo_R_slab(ht_tomo_s* t, const void* obj, void* sino, int nz, int ldz, int coeffx, void* stream);
+int ht_tomo_RT_slab(ht_tomo_s* t, const void* sino, void* obj, int nz, int ldz, int coeffx, float scale,
+                    void* stream);
 
 /* ------------------------------------------------------------------------
  * Cubic B-spline shift family.  Replaces Shift.__init__/coeff/S/Sadj/
@@ -205,25 +214,36 @@ int ht_rec_destroy(ht_rec_s* r);
 int ht_rec_forward(ht_rec_s* r, const void* c, const float* pos, const float* mag, const void* prb, const float* data,
                    float* amp, double* fval, void* stream);
 
+/* A handle created for an angle chunk of a larger problem: N of the
+ * objective's 2/N (rec_mpi.py:569, 91) becomes the whole problem's
+ * ntheta*ndist*nz*n.  With it, ht_rec_gradient / ht_rec_hessian called on the
+ * chunks in turn (pointers offset to the chunk's angles, accumulate = 1 after
+ * the first) give the whole problem's sums.  A chunk's Hessian reads the
+ * caches of that chunk's gradient call, so a chunked Hessian evaluation
+ * repeats each chunk's gradient call before its Hessian call. */
+int ht_rec_set_data_size(ht_rec_s* r, double ndata);
+
 /* Gradient of the data term (gF0..gF3, rec_mpi.py:327-353, 562-813):
  * gc [ntheta, nzobj, nobj] = sum_k S_k^T(Y22) (unscaled; apply coeff() for
  * the proj gradient), gpos [ntheta, ndist, 2] float32 times scale_pos,
  * gprb [ndist, nz, n] complex64 times scale_prb (the variable scalings
  * rho_sq of rec_mpi.py:345-347; 1 for the plain gradient), *fval (device
- * double) = sum (|x0| - data)^2 at the same point. */
+ * double) = sum (|x0| - data)^2 at the same point.  accumulate = 1: gprb and
+ * *fval are added to (an angle chunk after the first; gc and gpos cover only
+ * the chunk's angles and are written). */
 int ht_rec_gradient(ht_rec_s* r, const void* c, const float* pos, const float* mag, const void* prb,
                     const float* data, void* gc, float* gpos, void* gprb, double* fval, float scale_pos,
-                    float scale_prb, void* stream);
+                    float scale_prb, int accumulate, void* stream);
 
 /* Hessian forms at the state of the last ht_rec_gradient call
  * (hessian_cascade, rec_mpi.py:250-303) for directions y (and z when
  * ndir = 2), each given as (coefficients of its proj, its pos, its prb).
  * out (device double[4]) = {H(y,y), H(y,z) as the reference evaluates it
  * (its d2s pairs c_y with r_y and c_z with r_z), H(z,z), the symmetric
- * H(y,z)}. */
+ * H(y,z)}; accumulate = 1 adds to out (an angle chunk after the first). */
 int ht_rec_hessian(ht_rec_s* r, const void* c, const float* pos, const float* mag, const void* prb,
                    const float* data, int ndir, const void* cy, const float* posy, const void* prby, const void* cz,
-                   const float* posz, const void* prbz, double* out, void* stream);
+                   const float* posz, const void* prbz, double* out, int accumulate, void* stream);
 
 /* ------------------------------------------------------------------------
  * BLAS-1 on float32 vectors (complex64 arrays as interleaved pairs, n =

@@ -408,3 +408,32 @@ def test_bh_32_iterations_64cubed_4dist_against_fp64_oracle(bh64_oracle, mode):
     rec.BH(mode=mode)
     for k in ("obj", "prb", "pos"):
         assert rel_l2(rec.vars[k].cpu().numpy(), ref[k]) < 1e-4, k
+
+
+@pytest.mark.parametrize("mode", ["host", "graph"])
+def test_chunked_bh_equals_unchunked(golden, mode):
+    """Angle chunks of the fused cascade (each chunk's forward pass recomputed
+    before its Hessian pass) and object slabs of the Radon transform give the
+    BH iteration of the whole problem: 4 iterations, chunks of 5 of 12 angles
+    and slabs of 12 of 32 slices, against the unchunked run and the
+    reference's."""
+    from holotomocupy_b200.rec import Rec
+    g = golden("rec")
+    n, ntheta, ndist, nobj, niter = [int(v) for v in g["bh_dims"]]
+    out = []
+    for chunk, slab in ((None, None), (5, 12)):
+        args = rec_args(n, ntheta, ndist, nobj, niter)
+        args.angle_chunk, args.slab_chunk = chunk, slab
+        rec = Rec(args)
+        rec.vars["obj"][:] = cuda(g["bh_obj_true"])
+        rec.vars["prb"][:] = cuda(g["bh_prb_true"])
+        rec.vars["pos"][:] = cuda(g["bh_pos_true"])
+        rec.gen_sqrt_data(rec.vars, rec.data)
+        rec.vars["obj"][:] = 0
+        rec.vars["prb"][:] = 1
+        rec.vars["pos"][:] = cuda(g["bh_pos_true"] + g["bh_pos_err"])
+        rec.BH(mode=mode)
+        out.append({k: rec.vars[k].cpu().numpy() for k in ("obj", "prb", "pos", "proj")})
+    for k in out[0]:
+        assert rel_l2(out[1][k], out[0][k]) < 1e-6, k
+        assert rel_l2(out[1][k], g[f"bh_{k}"]) < TOL, k

@@ -137,3 +137,17 @@ def test_rec_tomo_matches_reference(golden, tag):
     ref64 = o.rec_tomo(g[f"{tag}_d"].astype("complex128" if tag == "a" else "float64"), niter)
     assert rel_l2(u, ref64) < 1e-4
     assert rel_l2(u, g[f"{tag}_u"]) < 2e-4
+
+
+def test_R_RT_by_slabs_equal_whole_volume():
+    """A Tomo whose workspace holds 8 slices transforms a 20-slice volume slab by
+    slab into the same sinogram (and back) as one holding all 20."""
+    from holotomocupy_b200 import Tomo
+    n, nz, ntheta = 64, 20, 48
+    rng = np.random.default_rng(9)
+    theta = np.linspace(0, np.pi, ntheta, endpoint=False).astype("float32")
+    cn = lambda *s: torch.from_numpy((rng.standard_normal(s) + 1j * rng.standard_normal(s)).astype("complex64")).cuda()
+    x, y = cn(nz, n, n), cn(ntheta, nz, n)
+    whole, slabs = Tomo(n, nz, theta, 0.9), Tomo(n, 8, theta, 0.9)
+    assert rel_l2(slabs.R(x).cpu().numpy(), whole.R(x).cpu().numpy()) < 1e-7
+    assert rel_l2(slabs.RT(y).cpu().numpy(), whole.RT(y).cpu().numpy()) < 1e-7
