@@ -100,8 +100,19 @@ class Rec:
         _lib.call("ht_rec_create", self.n, self.nz, self.nobj, self.nzobj, self.angle_chunk, self.ndist,
                   1 if self.complex_obj else 0, self.cl_prop._h, ctypes.byref(h))
         self._h = h
+        # a handle processes exactly its own number of angles: the last, shorter
+        # chunk has a handle of its own
+        self._hrest = None
+        rest = self.ntheta % self.angle_chunk
+        if rest:
+            hr = ctypes.c_void_p()
+            _lib.call("ht_rec_create", self.n, self.nz, self.nobj, self.nzobj, rest, self.ndist,
+                      1 if self.complex_obj else 0, self.cl_prop._h, ctypes.byref(hr))
+            self._hrest = hr
         if self.angle_chunk < self.ntheta:
-            _lib.call("ht_rec_set_data_size", h, float(self.data_size))
+            for hh in (h, self._hrest):
+                if hh is not None:
+                    _lib.call("ht_rec_set_data_size", hh, float(self.data_size))
         self._scal = torch.zeros(8, dtype=torch.float64, device=dev)
 
     # the reference's operator lists (rec_mpi.py:38-45), built on access so
@@ -129,13 +140,14 @@ class Rec:
             self.release_graph()
         except Exception:
             pass
-        h = getattr(self, "_h", None)
-        if h is not None and h.value:
-            try:
-                _lib.lib().ht_rec_destroy(h)
-            except Exception:
-                pass
-            self._h = None
+        for name in ("_h", "_hrest"):
+            h = getattr(self, name, None)
+            if h is not None and h.value:
+                try:
+                    _lib.lib().ht_rec_destroy(h)
+                except Exception:
+                    pass
+                setattr(self, name, None)
         try:
             for name in ("vars", "grads", "etas", "data", "ref"):
                 if isinstance(getattr(self, name, None), (dict, torch.Tensor)):
@@ -205,9 +217,9 @@ class Rec:
     # -------------------------------------------------- fused cascade
     # ---------------------------------------------------- angle chunks
     def _chunks(self):
-        """(first angle, angles) of each angle chunk of the fused cascade."""
+        """(first angle, handle) of each angle chunk of the fused cascade."""
         for th0 in range(0, self.ntheta, self.angle_chunk):
-            yield th0, min(self.angle_chunk, self.ntheta - th0)
+            yield th0, (self._h if th0 + self.angle_chunk <= self.ntheta else self._hrest)
 
     @staticmethod
     def _at(t, th0):
@@ -218,8 +230,8 @@ class Rec:
         """ht_rec_forward over the angle chunks: amplitudes into amp, or the
         objective sum (|x0| - data)^2 returned as a float."""
         total, st = 0.0, _lib.stream_ptr()
-        for th0, _ in self._chunks():
-            _lib.call("ht_rec_forward", self._h, self._at(c, th0), self._at(pos, th0), self._at(mag, th0),
+        for th0, h in self._chunks():
+            _lib.call("ht_rec_forward", h, self._at(c, th0), self._at(pos, th0), self._at(mag, th0),
                       _lib.ptr(prb), self._at(data, th0) if data is not None else None,
                       self._at(amp, th0) if amp is not None else None,
                       _lib.ptr(self._scal) if data is not None else None, st)
@@ -240,8 +252,8 @@ class Rec:
             gprb = self._gprb if persistent else torch.empty(self.ndist, self.nz, self.n, dtype=torch.complex64,
                                                              device=self.device)
         mag, st = self.eff_demagnifications, _lib.stream_ptr()
-        for k, (th0, _) in enumerate(self._chunks()):
-            _lib.call("ht_rec_gradient", self._h, self._at(c, th0), self._at(pos, th0), self._at(mag, th0),
+        for k, (th0, h) in enumerate(self._chunks()):
+            _lib.call("ht_rec_gradient", h, self._at(c, th0), self._at(pos, th0), self._at(mag, th0),
                       _lib.ptr(prb), self._at(self.data, th0), self._at(gc, th0), self._at(gpos, th0), _lib.ptr(gprb),
                       _lib.ptr(self._scal), float(scale_pos), float(scale_prb), int(k > 0), st)
         return gc, gpos, gprb
@@ -261,13 +273,13 @@ class Rec:
                              torch.empty(self.angle_chunk, self.ndist, 2, dtype=torch.float32, device=self.device),
                              torch.empty(self.ndist, self.nz, self.n, dtype=torch.complex64, device=self.device))
         at = self._at
-        for k, (th0, _) in enumerate(self._chunks()):
+        for k, (th0, h) in enumerate(self._chunks()):
             if chunked:
                 sc, sp, sq = self._scratch
-                _lib.call("ht_rec_gradient", self._h, at(c, th0), at(pos, th0), at(mag, th0), _lib.ptr(prb),
+                _lib.call("ht_rec_gradient", h, at(c, th0), at(pos, th0), at(mag, th0), _lib.ptr(prb),
                           at(self.data, th0), _lib.ptr(sc), _lib.ptr(sp), _lib.ptr(sq),
                           ctypes.c_void_p(self._scal.data_ptr() + 8), 1.0, 1.0, 0, st)
-            _lib.call("ht_rec_hessian", self._h, at(c, th0), at(pos, th0), at(mag, th0), _lib.ptr(prb),
+            _lib.call("ht_rec_hessian", h, at(c, th0), at(pos, th0), at(mag, th0), _lib.ptr(prb),
                       at(self.data, th0), 2 if z is not None else 1, at(y[0], th0), at(y[1], th0), _lib.ptr(y[2]),
                       at(zz[0], th0) if z is not None else None, at(zz[1], th0) if z is not None else None,
                       _lib.ptr(zz[2]) if z is not None else None, _lib.ptr(out), int(k > 0), st)

@@ -86,9 +86,12 @@ def test_c1_adjoint_chain(c1):
     blk = torch.from_numpy(g["blk"]).cuda()
     sl = torch.from_numpy(g["slices"]).cuda()
     assert rel_l2(gr["prb"].cpu().numpy(), g["grad_prb"]) < TOL
-    # the position gradient: per-image sums over nz * n pixels, reduced in FP64
-    # here and in FP32 by the reference (its own value is 3.9e-5 from FP64)
-    assert rel_l2(gr["pos"].cpu().numpy(), g["grad_pos_fp64"]) < TOL
+    # the position gradient: per-image sums over nz * n = 16384 pixel products
+    # that largely cancel (each image's sum is ~1e-15 against per-pixel terms
+    # many orders larger), so the FP32 rounding of the operators shows in it:
+    # the reference's own value is 3.9e-5 from the FP64 oracle's; here the
+    # products are FP32 and the sums FP64 (measured 3.4e-5 from FP64)
+    assert rel_l2(gr["pos"].cpu().numpy(), g["grad_pos_fp64"]) < 5e-5
     assert rel_l2(gr["pos"].cpu().numpy(), g["grad_pos"]) < 6e-5
     assert rel_l2(gr["obj"][sl].cpu().numpy(), g["grad_obj_sl"]) < TOL
     assert rel_l2(gr["proj"][blk].cpu().numpy(), g["grad_proj_blk"]) < TOL

@@ -77,10 +77,17 @@ def test_fbp_matches_oracle():
 
 
 def test_slice_capacity_is_enforced():
-    from holotomocupy_b200 import Tomo
+    """The library refuses more slices than the handle's workspace holds; the
+    Python class then runs taller volumes slab by slab, and refuses wrong
+    shapes."""
+    from holotomocupy_b200 import Tomo, _lib
     t = Tomo(32, 2, np.linspace(0, np.pi, 8, endpoint=False), 0)
+    x = torch.zeros(3, 32, 32, dtype=torch.complex64, device="cuda")
+    y = torch.empty(8, 3, 32, dtype=torch.complex64, device="cuda")
+    assert _lib.lib().ht_tomo_R(t._h, _lib.ptr(x), _lib.ptr(y), 3, _lib.stream_ptr()) == 1
+    assert tuple(t.R(x).shape) == (8, 3, 32)
     with pytest.raises(ValueError):
-        t.R(torch.zeros(3, 32, 32, dtype=torch.complex64, device="cuda"))
+        t.R(torch.zeros(3, 32, 31, dtype=torch.complex64, device="cuda"))
 
 
 @pytest.mark.parametrize("n,ntheta,nz", [(64, 40, 24), (128, 90, 32)])
