@@ -68,6 +68,7 @@ SIGNATURES = {
     "ht_rec_forward": [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
     "ht_rec_gradient": [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _c_float, _c_float, _c_int, _vp],
     "ht_rec_set_data_size": [_vp, _c_double],
+    "ht_rec_set_shared_coefficients": [_vp, _c_int],
     "ht_rec_objective_noalloc": [_vp, _c_int, _c_int, _c_int, _c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
     "ht_rec_hessian": [_vp, _vp, _vp, _vp, _vp, _vp, _c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _c_int, _vp],
 }

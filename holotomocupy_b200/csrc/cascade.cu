@@ -101,8 +101,14 @@ __device__ __forceinline__ float2 cexp_i(float2 z) {
 
 struct CascDims {
   int n, nz, nobj, nzobj, ndist;
-  long nimg;  // ntheta * ndist
+  long nimg;         // ntheta * ndist
+  int shared_c = 0;  // 1: one coefficient array [nzobj, nobj] for every angle
 };
+
+// Offset of angle th's coefficient array.
+__device__ __forceinline__ long coef_off(const CascDims& D, long th) {
+  return D.shared_c ? 0 : th * (long)D.nzobj * D.nobj;
+}
 
 // Object coordinate of detector column tx / row ty (cuda_kernels.py:177-190):
 // mag * (t - n/2) - shift + (mag - 1)/2 + nobj/2.  Forward and adjoint use
@@ -324,7 +330,7 @@ k_casc_fwd(const T* __restrict__ c, const float* __restrict__ pos, const float* 
   const RowGeo<0> rg(D, m0, r.x, ty);
   if (valid) {
     const float* const w[1] = {rg.py};
-    vrows<T, 1>(V, D.nobj, c + th * (long)D.nzobj * D.nobj, rg.yy, w, t, TT);
+    vrows<T, 1>(V, D.nobj, c + coef_off(D, th), rg.yy, w, t, TT);
   }
   __syncthreads();
   for (int tx = t; tx < N; tx += TT) {
@@ -621,7 +627,7 @@ k_casc_adj(const float2* __restrict__ tmp, float2* __restrict__ Pc, T* __restric
   const RowGeo<2> rg(D, m0, r.x, ty);
   if (valid) {
     const float* const w[3] = {rg.py, rg.dpy, rg.d2py};
-    vrows_adj<T>(V, V + adj_pair_off(D.nobj), D.nobj, c + th * (long)D.nzobj * D.nobj, rg.yy, w, t, TT);
+    vrows_adj<T>(V, V + adj_pair_off(D.nobj), D.nobj, c + coef_off(D, th), rg.yy, w, t, TT);
   }
   dct3_start<N, TT>(sm, t, tw4, tmp + row * N, valid);  // ends with a barrier: V is complete
   const T* V0 = V;
@@ -817,7 +823,7 @@ k_casc_hess_fwd(const T* __restrict__ c, const float* __restrict__ pos, const fl
   const long th = img / D.ndist;
   SmRow sm0{smem + line * SmRow::padded(N)};
   SmRow sm1{smem + (LINES + line) * SmRow::padded(N)};
-  const long coff = th * (long)D.nzobj * D.nobj;
+  const long coff = coef_off(D, th);
   const float m0 = valid ? mag[img] : 1.f;
   const float2 r = valid ? ld_pos(pos, img) : make_float2(0.f, 0.f);
   const float2 rd0 = valid ? ld_pos(pos0, img) : make_float2(0.f, 0.f);
@@ -1290,8 +1296,18 @@ static cudaError_t grad_impl(ht_rec_s* r, const void* c, const float* pos, const
   k_sum_theta<<<(unsigned)((r->D.ndist * npix + 255) / 256), 256, 0, st>>>(r->P, gprb, r->ntheta, r->D.ndist, npix,
                                                                              sprb, acc);
   ::ht::count_launch();
-  dim3 g2((r->D.nobj + 31) / 32, (r->D.nzobj + 8 * kVRows - 1) / (8 * kVRows), r->ntheta);
-  k_casc_vsum<T><<<g2, dim3(32, 8), 0, st>>>((T*)gc, hbuf, pos, mag, r->D); ::ht::count_launch();
+  if (r->D.shared_c) {
+    // one coefficient array for all angles: its gradient sums every image
+    // (all images taken as the distances of a single angle)
+    CascDims all = r->D;
+    all.ndist = (int)r->D.nimg;
+    dim3 g1((r->D.nobj + 31) / 32, (r->D.nzobj + 8 * kVRows - 1) / (8 * kVRows), 1);
+    k_casc_vsum<T><<<g1, dim3(32, 8), 0, st>>>((T*)gc, hbuf, pos, mag, all);
+  } else {
+    dim3 g2((r->D.nobj + 31) / 32, (r->D.nzobj + 8 * kVRows - 1) / (8 * kVRows), r->ntheta);
+    k_casc_vsum<T><<<g2, dim3(32, 8), 0, st>>>((T*)gc, hbuf, pos, mag, r->D);
+  }
+  ::ht::count_launch();
   k_casc_gpos<<<(unsigned)((r->D.nimg + 255) / 256), 256, 0, st>>>(r->acc_img, gpos, r->D.nimg, spos);
   ::ht::count_launch();
   return cudaGetLastError();
@@ -1365,6 +1381,13 @@ extern "C" int ht_rec_forward(ht_rec_s* r, const void* c, const float* pos, cons
   }
   HT_CHECK_CUDA(e);
   if (fval) HT_CHECK_CUDA(cudaMemcpyAsync(fval, r->glob + kF, sizeof(double), cudaMemcpyDeviceToDevice, st));
+  return kOk;
+}
+
+extern "C" int ht_rec_set_shared_coefficients(ht_rec_s* r, int shared) {
+  using namespace ht;
+  HT_REQUIRE(r, "ht_rec_set_shared_coefficients: null pointer");
+  r->D.shared_c = shared ? 1 : 0;
   return kOk;
 }
 

@@ -433,10 +433,14 @@ class Rec:
         mode="host" iterates as the reference does (step sizes on the host).
         mode="graph" keeps the step sizes on the device and replays the
         steady-state iteration from a CUDA graph (same arithmetic; needs
-        lam_prbfit == 0 and no error table)."""
+        lam_prbfit == 0, no error table and no checkpoints).  ``writer``
+        (checkpoint.Writer) saves obj/prb/pos every vis_step iterations
+        (rec_mpi.py:837-860, vis_debug)."""
         self.bh_setup()
         niter = self.niter if niter is None else niter
-        if mode == "graph" and self.lam_prbfit == 0 and self.err_step == -1 and niter > self.start_iter:
+        checkpoints = writer is not None and getattr(self, "vis_step", -1) not in (-1, 0, None)
+        if (mode == "graph" and self.lam_prbfit == 0 and self.err_step == -1 and not checkpoints
+                and niter > self.start_iter):
             cur = torch.cuda.current_stream(self.device)
             side = torch.cuda.Stream(device=self.device)
             side.wait_stream(cur)
@@ -457,6 +461,8 @@ class Rec:
             if record is not None:
                 record.append((i, a, b))
             self.error_debug(self.vars, i)
+            if checkpoints and i % self.vis_step == 0 and i > self.start_iter:
+                writer.write_checkpoint(self.vars, i, self.norm_const)
         return self.bh_finish()
 
     def bh_setup(self):

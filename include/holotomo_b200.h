@@ -223,6 +223,15 @@ int ht_rec_forward(ht_rec_s* r, const void* c, const float* pos, const float* ma
  * repeats each chunk's gradient call before its Hessian call. */
 int ht_rec_set_data_size(ht_rec_s* r, double ndata);
 
+/* shared = 1: the coefficient arguments (c, and cy, cz of ht_rec_hessian) are
+ * one [nzobj, nobj] array for every angle, and ht_rec_gradient's gc is its
+ * gradient summed over all images, [nzobj, nobj].  Near-field ptychography
+ * (RecNFP, src/holotomocupy/rec_nfp_mpi.py:20-469) scans one projection over
+ * ntheta positions at one distance; the reference tiles the coefficients over
+ * the positions (rec_nfp_mpi.py:353-357) and sums the per-position adjoints
+ * (:393-405). */
+int ht_rec_set_shared_coefficients(ht_rec_s* r, int shared);
+
 /* Gradient of the data term (gF0..gF3, rec_mpi.py:327-353, 562-813):
  * gc [ntheta, nzobj, nobj] = sum_k S_k^T(Y22) (unscaled; apply coeff() for
  * the proj gradient), gpos [ntheta, ndist, 2] float32 times scale_pos,

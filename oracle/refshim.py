@@ -2,8 +2,9 @@
 
 The reference (holotomocupy) is CuPy + mpi4py code.  Neither package exists in
 this image, so this module installs small stand-ins in ``sys.modules`` and then
-imports the reference's ``tomo.py``, ``shift.py``, ``propagation.py`` and
-``rec_mpi.py`` UNCHANGED from a source tree given by the caller:
+imports the reference's ``tomo.py``, ``shift.py``, ``propagation.py``,
+``rec_mpi.py`` and ``rec_nfp_mpi.py`` UNCHANGED from a source tree given by
+the caller:
 
 * ``cupy``            -> NumPy, with arrays of a small ndarray subclass that has
                          CuPy's ``.get()``; ``cp.RawKernel`` -> the NumPy kernel
@@ -263,7 +264,7 @@ _LOADED = {}
 def load_reference(src_dir):
     """Import the reference package from ``src_dir`` (the directory holding
     ``holotomocupy/``) with the stand-ins installed.  Returns a namespace with
-    the modules ``tomo``, ``shift``, ``propagation``, ``rec_mpi`` and ``utils``."""
+    the modules ``tomo``, ``shift``, ``propagation``, ``rec_mpi``, ``rec_nfp_mpi`` and ``utils``."""
     if src_dir in _LOADED:
         return _LOADED[src_dir]
     cp, cpfft = _make_cupy()
@@ -291,7 +292,7 @@ def load_reference(src_dir):
     try:
         pkg = importlib.import_module("holotomocupy")
         ns = types.SimpleNamespace()
-        for name in ("utils", "tomo", "shift", "propagation", "chunking", "rec_mpi"):
+        for name in ("utils", "tomo", "shift", "propagation", "chunking", "rec_mpi", "rec_nfp_mpi"):
             setattr(ns, name, importlib.import_module("holotomocupy." + name))
         # Chunking: call the wrapped function directly (chunking.py:39-42 branch)
         ns.chunking.Chunking.__init__ = lambda self, nbytes, chunk: setattr(self, "chunk", chunk)

@@ -465,15 +465,79 @@ def rectomo_cases(ns):
     np.savez_compressed(os.path.join(HERE, "rectomo.npz"), **out)
 
 
+def nfp_args(n, nobj, ntheta, dt, niter=1):
+    return types.SimpleNamespace(
+        energy=17.1, detector_pixelsize=3e-6, focustodetectordistance=1.217, z1=8.245e-3,
+        ntheta=ntheta, nz=n, n=n, nzobj=nobj, nobj=nobj, obj_dtype=dt, rho=[1, 0.5, 0.1],
+        niter=niter, nchunk=ntheta, vis_step=-1, err_step=-1, start_iter=0,
+        comm=sys.modules["mpi4py"].MPI.COMM_WORLD)
+
+
+def nfp_cases(ns):
+    """RecNFP (rec_nfp_mpi.py:20-469), near-field ptychography: one 2-D
+    projection scanned at ntheta positions, one distance.  The gradient and the
+    Hessian forms at one point, and a 4-iteration BH run from a flat probe, a
+    zero projection and perturbed positions; complex and real projections."""
+    out = {}
+    for dt, tag in (("complex64", "c"), ("float32", "f")):
+        n, nobj, ntheta, niter = 32, 48, 8, 4
+        rng = np.random.default_rng(60 + len(dt))
+        rec = ns.rec_nfp_mpi.RecNFP(nfp_args(n, nobj, ntheta, dt, niter))
+        ph = phantom(nobj, rng)[nobj // 2]
+        proj = (ph if dt == "complex64" else ph.real.astype("float32")).copy()
+        prb = (1 + 0.2 * crand(rng, (n, n))).astype("complex64")
+        pos = rng.uniform(-2, 2, (ntheta, 2)).astype("float32")
+        pos_err = rng.uniform(-0.3, 0.3, (ntheta, 2)).astype("float32")
+        C = lambda x: ns.cp.array(x)
+        rec.vars["prb"][:] = C(prb)
+        rec.vars["proj"][:] = C(proj)
+        rec.vars["pos"][:] = C(pos)
+        rec.gen_sqrt_data(rec.vars, rec.data)
+        data = np.array(rec.data)
+        # gradient and Hessian forms at a perturbed point
+        mk = (lambda sh, sc: crand(rng, sh, sc)) if dt == "complex64" else (lambda sh, sc: frand(rng, sh, sc))
+        v = {"prb": C(prb + 0.1 * crand(rng, (n, n))), "proj": C((proj * 0.7).astype(dt)),
+             "pos": C((pos + pos_err).astype("float32"))}
+        g = {"prb": C(0.1 * crand(rng, (n, n))), "proj": C(mk((nobj, nobj), 0.05)),
+             "pos": C(frand(rng, (ntheta, 2), 0.3))}
+        e = {"prb": C(0.1 * crand(rng, (n, n))), "proj": C(mk((nobj, nobj), 0.05)),
+             "pos": C(frand(rng, (ntheta, 2), 0.3))}
+        grads = {"prb": ns.cp.zeros((n, n), "complex64"), "proj": ns.cp.zeros((nobj, nobj), dt),
+                 "pos": ns.cp.zeros((ntheta, 2), "float32")}
+        rec.gradients(v, grads)
+        F = float(rec.min(v["prb"], v["proj"], v["pos"]))
+        h_ge = float(rec.hessian(v, g, e))
+        h_ee = float(rec.hessian(v, e, e))
+        out.update({f"{tag}_dims": np.array([n, nobj, ntheta, niter]), f"{tag}_data": data,
+                    f"{tag}_prb_true": prb, f"{tag}_proj_true": proj, f"{tag}_pos_true": pos,
+                    f"{tag}_pos_err": pos_err, f"{tag}_F": np.array(F), f"{tag}_h_ge": np.array(h_ge),
+                    f"{tag}_h_ee": np.array(h_ee)})
+        for name, d in (("v", v), ("g", g), ("e", e), ("grad", grads)):
+            for k, x in d.items():
+                out[f"{tag}_{name}_{k}"] = np.array(x)
+        # BH from a flat probe and a zero projection
+        rec.vars["prb"][:] = C(np.ones((n, n), "complex64"))
+        rec.vars["proj"][:] = 0
+        rec.vars["pos"][:] = C((pos + pos_err).astype("float32"))
+        pairs = []
+        orig = rec.allreduce2
+        rec.allreduce2 = lambda a, b: (pairs.append((float(a), float(b))), orig(a, b))[1]
+        rec.BH()
+        out.update({f"{tag}_bh_{k}": np.array(rec.vars[k]) for k in ("prb", "proj", "pos")})
+        out[f"{tag}_bh_topbottom"] = np.array(pairs, dtype="float64")
+    np.savez_compressed(os.path.join(HERE, "nfp.npz"), **out)
+
+
 def main():
     src = sys.argv[1] if len(sys.argv) > 1 else None
     if src is None:
         raise SystemExit("usage: make_golden.py <reference src dir>")
     ns = load_reference(src)
-    which = sys.argv[2:] or ["tomo", "prop", "shift", "rec", "lap", "sback", "c1", "prbfit", "rectomo"]
+    which = sys.argv[2:] or ["tomo", "prop", "shift", "rec", "lap", "sback", "c1", "prbfit", "rectomo", "nfp"]
     for w in which:
         {"tomo": tomo_cases, "prop": prop_cases, "shift": shift_cases, "rec": rec_cases, "lap": lap_cases,
-         "sback": sback_cases, "c1": c1_cases, "prbfit": prbfit_cases, "rectomo": rectomo_cases}[w](ns)
+         "sback": sback_cases, "c1": c1_cases, "prbfit": prbfit_cases, "rectomo": rectomo_cases,
+         "nfp": nfp_cases}[w](ns)
         print("wrote", w)
 
 

@@ -437,3 +437,31 @@ def test_chunked_bh_equals_unchunked(golden, mode):
     for k in out[0]:
         assert rel_l2(out[1][k], out[0][k]) < 1e-6, k
         assert rel_l2(out[1][k], g[f"bh_{k}"]) < TOL, k
+
+
+def test_bh_checkpoints_hold_the_iteration_state(golden, tmp_path):
+    """BH with a checkpoint writer (vis_step 2, rec_mpi.py's vis_debug) saves,
+    at iteration 2, the state a 3-iteration run ends with; reading it back
+    gives obj, prb and pos."""
+    from holotomocupy_b200.checkpoint import Writer, read_checkpoint
+    from holotomocupy_b200.rec import Rec
+    g = golden("rec")
+    n, ntheta, ndist, nobj, _ = [int(v) for v in g["bh_dims"]]
+    states = []
+    for niter, writer in ((4, Writer(str(tmp_path), fmt="npz")), (3, None)):
+        args = rec_args(n, ntheta, ndist, nobj, niter)
+        args.vis_step = 2
+        rec = Rec(args)
+        rec.vars["obj"][:] = cuda(g["bh_obj_true"])
+        rec.vars["prb"][:] = cuda(g["bh_prb_true"])
+        rec.vars["pos"][:] = cuda(g["bh_pos_true"])
+        rec.gen_sqrt_data(rec.vars, rec.data)
+        rec.vars["obj"][:] = 0
+        rec.vars["prb"][:] = 1
+        rec.vars["pos"][:] = cuda(g["bh_pos_true"] + g["bh_pos_err"])
+        rec.BH(writer=writer)
+        states.append({k: rec.vars[k].cpu().numpy() for k in ("obj", "prb", "pos")})
+    ck = read_checkpoint(str(tmp_path / "checkpoint_0002.npz"), n, nobj)
+    assert ck["iter"] == 2
+    for k in ("obj", "prb", "pos"):
+        assert rel_l2(ck[k].numpy(), states[1][k]) < 1e-6, k
