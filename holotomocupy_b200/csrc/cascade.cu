@@ -207,6 +207,8 @@ struct StCfg {
   static constexpr int fit(int l) { return (l > 1 && l * PER_LINE > 100 * 1024) ? fit(l / 2) : l; }
   static constexpr int LINES = fit(RowCfg<N>::LINES / NFFT > 0 ? RowCfg<N>::LINES / NFFT : 1);
   static constexpr int THREADS = LINES * TR;
+  // each FFT group of T threads is a line with its own named barrier (1..15)
+  static_assert(T % 32 != 0 || LINES * NFFT <= 15, "at most 15 line barriers per block");
   // dynamic shared memory: FFT lines, then reduction scratch, then the rows
   static constexpr int FFT_BYTES = LINES * NFFT * SmRow::padded(N) * 8;
   static int bytes(int K, int nobj, int elem) {

@@ -12,6 +12,8 @@ struct RowCfg {
   static constexpr int LINES = (T >= 256) ? 1 : (256 / T);
   static constexpr int THREADS = LINES * T;
   static constexpr int SMEM = LINES * SmRow::padded(N) * (int)sizeof(float2);
+  // lines of whole warps synchronise on named barriers 1..15 (LineSync)
+  static_assert(T % 32 != 0 || LINES <= 15, "at most 15 line barriers per block");
 };
 
 // Columns per CTA for a column pass of length N (tile N x C in shared memory;

@@ -58,6 +58,8 @@ struct ZCfg {
   static constexpr int THREADS = Z * T;
   static constexpr int LS = SmRow::padded(N) + 1;
   static constexpr int SMEM = Z * LS * (int)sizeof(float2);
+  // lines of whole warps synchronise on named barriers 1..15 (LineSync)
+  static_assert(T % 32 != 0 || Z <= 15, "at most 15 line barriers per block");
 };
 
 template <int N, int Z>
