@@ -49,7 +49,7 @@ k_conv_rows(const float2* in, float2* out, long nrows, const float2* __restrict_
 // data [nimg, N, ncols] in place along the column axis, times H[k, col]
 // between the forward and inverse column transforms.
 template <int N>
-__global__ void __launch_bounds__(ColCfg<N>::THREADS)
+__global__ void __launch_bounds__(ColCfg<N>::THREADS, ColCfg<N>::MIN_BLOCKS)
 k_conv_cols(float2* data, int ncols, const float2* __restrict__ H, const float2* __restrict__ tw4) {
   constexpr int C = ColCfg<N>::C;
   constexpr int T = ColCfg<N>::T;

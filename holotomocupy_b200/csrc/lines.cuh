@@ -24,6 +24,9 @@ struct ColCfg {
   static constexpr int C = (N >= 2048) ? 4 : ((N >= 256) ? 8 : 16);
   static constexpr int THREADS = C * T;
   static constexpr int SMEM = N * C * (int)sizeof(float2);
+  // two CTAs per SM where that leaves 64 registers a thread (one CTA's block
+  // barriers then overlap the other's work); the 1024-thread tiles keep one
+  static constexpr int MIN_BLOCKS = THREADS <= 512 ? 2 : 1;
 };
 
 // Raise the dynamic shared-memory limit of a kernel (no-op below 48 KB).  The

@@ -114,11 +114,12 @@ struct ColOut {
 // the last one stores them there (a warp covers 32/C rows of C adjacent
 // columns per access), so the column tile passes through shared memory only
 // between stages.
-// Two CTAs per SM (the register cap this sets, 64, spills a little at
-// NZ = 2048): the block barriers of one CTA overlap the other's work
-// (D at 2048^2 x 16 images 1.88 -> 1.67 ms, at 1024^2 x 32 0.80 -> 0.72 ms).
+// Two CTAs per SM up to 512 threads (ColCfg::MIN_BLOCKS; the register cap
+// this sets, 64, spills a little at NZ = 2048): the block barriers of one CTA
+// overlap the other's work (D at 2048^2 x 16 images 1.88 -> 1.67 ms, at
+// 1024^2 x 32 0.80 -> 0.72 ms).
 template <int NZ, bool CONJ>
-__global__ void __launch_bounds__(ColCfg<NZ>::THREADS, 2)
+__global__ void __launch_bounds__(ColCfg<NZ>::THREADS, ColCfg<NZ>::MIN_BLOCKS)
 k_dct_cols(float2* data, int n, const float2* __restrict__ Hall, int ntab, const float2* __restrict__ tw4) {
   // image blockIdx.y uses table (blockIdx.y % ntab) of Hall [ntab, NZ, n]
   const float2* __restrict__ H = Hall + (long)(blockIdx.y % ntab) * NZ * n;

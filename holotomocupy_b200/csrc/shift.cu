@@ -385,7 +385,7 @@ k_symbol_rows(const float2* in, float2* out, long nrows, const float* __restrict
 // FFT's last stage stores them back (a warp covers 32 / C rows of C adjacent
 // columns per access); the tile passes shared memory only between stages.
 template <int N>
-__global__ void __launch_bounds__(ColCfg<N>::THREADS)
+__global__ void __launch_bounds__(ColCfg<N>::THREADS, ColCfg<N>::MIN_BLOCKS)
 k_symbol_cols(const float2* in, float2* out, int ncols, const float* __restrict__ sym,
               const float2* __restrict__ tw4) {
   constexpr int C = ColCfg<N>::C;
