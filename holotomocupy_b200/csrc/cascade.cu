@@ -71,10 +71,13 @@ struct El;
 template <>
 struct El<float2> {
   static __device__ __forceinline__ float2 zero() { return make_float2(0.f, 0.f); }
+  // one packed two-lane FMA (the stencil taps' real weight on a complex sample)
   static __device__ __forceinline__ void fma(float2& a, float w, float2 v) {
-    a.x += w * v.x;
-    a.y += w * v.y;
+#if defined(__CUDA_ARCH__)
+    a = p2_fma(make_float2(w, w), v, a);
+#endif
   }
+
   static __device__ __forceinline__ float2 cplx(float2 v) { return v; }
   // projection of a complex gradient onto the element space
   static __device__ __forceinline__ float2 proj(float2 g) { return g; }

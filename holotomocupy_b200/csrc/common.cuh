@@ -34,8 +34,55 @@ const char* last_error();
 enum Status : int { kOk = 0, kBadArgument = 1, kCudaError = 2, kUnsupported = 3 };
 
 // ------------------------------------------------------------ complex math
-__host__ __device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
-__host__ __device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+// On the device the two parts of a complex value go through one packed
+// two-lane FP32 instruction (add/sub/mul/fma .f32x2, sm_100): the same IEEE
+// operation on each part as the scalar forms, in half the instructions
+// (cmul/cmulc stay scalar: their lane swaps cost more than they save).  A
+// translation unit that defines HT_SCALAR_COMPLEX before including this
+// keeps scalar adds and scales (the column passes of prop.cu run faster so).
+#if defined(__CUDA_ARCH__)
+__device__ __forceinline__ float2 p2_add(float2 a, float2 b) {
+  float2 d;
+  asm("{\n .reg .b64 pa, pb, pd;\n mov.b64 pa, {%2, %3};\n mov.b64 pb, {%4, %5};\n add.rn.f32x2 pd, pa, pb;\n"
+      " mov.b64 {%0, %1}, pd;\n}" : "=f"(d.x), "=f"(d.y) : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+  return d;
+}
+__device__ __forceinline__ float2 p2_sub(float2 a, float2 b) {
+  float2 d;
+  asm("{\n .reg .b64 pa, pb, pd;\n mov.b64 pa, {%2, %3};\n mov.b64 pb, {%4, %5};\n sub.rn.f32x2 pd, pa, pb;\n"
+      " mov.b64 {%0, %1}, pd;\n}" : "=f"(d.x), "=f"(d.y) : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+  return d;
+}
+__device__ __forceinline__ float2 p2_mul(float2 a, float2 b) {
+  float2 d;
+  asm("{\n .reg .b64 pa, pb, pd;\n mov.b64 pa, {%2, %3};\n mov.b64 pb, {%4, %5};\n mul.rn.f32x2 pd, pa, pb;\n"
+      " mov.b64 {%0, %1}, pd;\n}" : "=f"(d.x), "=f"(d.y) : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+  return d;
+}
+// a * b + c, lane by lane
+__device__ __forceinline__ float2 p2_fma(float2 a, float2 b, float2 c) {
+  float2 d;
+  asm("{\n .reg .b64 pa, pb, pc, pd;\n mov.b64 pa, {%2, %3};\n mov.b64 pb, {%4, %5};\n mov.b64 pc, {%6, %7};\n"
+      " fma.rn.f32x2 pd, pa, pb, pc;\n mov.b64 {%0, %1}, pd;\n}"
+      : "=f"(d.x), "=f"(d.y) : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y), "f"(c.x), "f"(c.y));
+  return d;
+}
+#endif
+
+__host__ __device__ __forceinline__ float2 cadd(float2 a, float2 b) {
+#if defined(__CUDA_ARCH__) && !defined(HT_SCALAR_COMPLEX)
+  return p2_add(a, b);
+#else
+  return make_float2(a.x + b.x, a.y + b.y);
+#endif
+}
+__host__ __device__ __forceinline__ float2 csub(float2 a, float2 b) {
+#if defined(__CUDA_ARCH__) && !defined(HT_SCALAR_COMPLEX)
+  return p2_sub(a, b);
+#else
+  return make_float2(a.x - b.x, a.y - b.y);
+#endif
+}
 __host__ __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
   return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
@@ -44,7 +91,13 @@ __host__ __device__ __forceinline__ float2 cmulc(float2 a, float2 b) {
   return make_float2(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y);
 }
 __host__ __device__ __forceinline__ float2 cconj(float2 a) { return make_float2(a.x, -a.y); }
-__host__ __device__ __forceinline__ float2 cscale(float2 a, float s) { return make_float2(a.x * s, a.y * s); }
+__host__ __device__ __forceinline__ float2 cscale(float2 a, float s) {
+#if defined(__CUDA_ARCH__) && !defined(HT_SCALAR_COMPLEX)
+  return p2_mul(a, make_float2(s, s));
+#else
+  return make_float2(a.x * s, a.y * s);
+#endif
+}
 // multiply by -i (forward sign) or +i (inverse sign)
 template <bool INV>
 __host__ __device__ __forceinline__ float2 rot(float2 a) {

@@ -20,6 +20,7 @@
 //
 // Kernels: row DCT-II  ->  column [DCT-II, x Hw, DCT-III]  ->  row DCT-III.
 // The column pass works in place, so D needs no scratch buffer.
+#define HT_SCALAR_COMPLEX 1  // the column passes run faster on scalar complex adds (common.cuh)
 #include "lines.cuh"
 #include "row512.cuh"
 #include "holotomo_b200_internal.h"
