@@ -50,6 +50,8 @@ SIGNATURES = {
     "ht_shift_d2S": [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _c_long, _vp],
     "ht_shift_dSadj": [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _c_long, _vp],
     "ht_filter_rows": [_c_int, _vp, _vp, _c_long, _vp, _vp],
+    "ht_prbfit_grad": [_vp, _vp, _vp, _vp, _vp, _c_float, _vp],
+    "ht_prbfit_forms": [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _c_double, _c_int, _vp],
     "ht_laplacian_grad": [_vp, _vp, _c_int, _c_int, _c_int, _c_int, _c_float, _vp, _vp],
     "ht_laplacian_dot": [_vp, _vp, _c_int, _c_int, _c_int, _c_int, _c_double, _vp, _vp, _vp, _vp, _vp],
     "ht_laplacian_energy": [_vp, _c_int, _c_int, _c_int, _c_int, _c_double, _vp, _vp, _vp],

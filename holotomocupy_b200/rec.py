@@ -199,6 +199,10 @@ class Rec:
         self._vol = z(self.nzobj, self.nobj, self.nobj) if self._fold else None
         # Laplacian regulariser workspace (the inner Laplacian on nzobj + 2 slices)
         self._lapw = z(self.nzobj + 2, self.nobj, self.nobj) if self.lam_laplacian != 0 else None
+        # probe-fit workspace: three propagated probe-sized arrays and 32 KiB of partial sums
+        self._pfw = (z(3 * self.ndist * self.nz * self.n + 4096, dt=torch.complex64)
+                     if self.lam_prbfit != 0 else None)
+        self._pf3 = z(3, dt=torch.float64)
 
     def _coeff_into(self, src, dst):
         """dst = coeff(src) (shift.py:74-82) for a [ntheta, nzobj, nobj] array."""
@@ -313,32 +317,29 @@ class Rec:
 
     # ------------------------------------------------- probe-fit term
     def gradient_prbfit(self, grad_prb, prb):
-        """rec_mpi.py:365-377"""
+        """rec_mpi.py:365-377: grad_prb += rho lam/N D^H(2 (D prb - ref D prb/|D prb|)) (ht_prbfit_grad)."""
         if self.lam_prbfit == 0:
             return
-        for j in range(self.ndist):
-            tmp = self.cl_prop.D(prb[j: j + 1].contiguous(), j)
-            td = self.ref[j: j + 1] * (tmp / torch.abs(tmp))
-            td = self.lam_prbfit / self.prb_size * self.cl_prop.DT(2 * (tmp - td), j)
-            grad_prb[j: j + 1] += td * self.rho_sq["prb"]
+        scale = float(np.float32(self.lam_prbfit / self.prb_size) * np.float32(self.rho_sq["prb"]))
+        _lib.call("ht_prbfit_grad", self.cl_prop._h, _lib.ptr(prb.contiguous()), _lib.ptr(self.ref),
+                  _lib.ptr(self._pfw), _lib.ptr(grad_prb), scale, _lib.stream_ptr())
+
+    def _prbfit_forms_dev(self, prb, d1, d2, out, hess_slots):
+        """hessian_prbfit (rec_mpi.py:379-398) on the device (ht_prbfit_forms): the
+        forms of (d1,d1), (d1,d2), (d2,d2) into out[0..2], or added to the BH
+        Hessian slots of out (hess_slots)."""
+        _lib.call("ht_prbfit_forms", self.cl_prop._h, _lib.ptr(prb.contiguous()), _lib.ptr(d1.contiguous()),
+                  _lib.ptr(d2.contiguous()) if d2 is not None else None, _lib.ptr(self.ref), _lib.ptr(self._pfw),
+                  out, self.lam_prbfit / self.prb_size, int(hess_slots), _lib.stream_ptr())
 
     def _prbfit_forms(self, prb, d1, d2):
-        """hessian_prbfit (rec_mpi.py:379-398) for the pairs (d1,d1), (d1,d2), (d2,d2)."""
+        """hessian_prbfit (rec_mpi.py:379-398) for the pairs (d1,d1), (d1,d2), (d2,d2)
+        (d2 None: d1 for both)."""
         if self.lam_prbfit == 0:
             return 0.0, 0.0, 0.0
-        out = [0.0, 0.0, 0.0]
-        for j in range(self.ndist):
-            Dp = self.cl_prop.D(prb[j: j + 1].contiguous(), j)
-            Da = self.cl_prop.D(d1[j: j + 1].contiguous(), j)
-            Db = self.cl_prop.D(d2[j: j + 1].contiguous(), j) if d2 is not None else Da
-            l0 = Dp / torch.abs(Dp)
-            d0 = self.ref[j: j + 1] / torch.abs(Dp)
-            for i, (u, w) in enumerate(((Da, Da), (Da, Db), (Db, Db))):
-                v1 = torch.sum(((1 - d0) * reprod(u, w)).double())
-                v2 = torch.sum((d0 * reprod(l0, u) * reprod(l0, w)).double())
-                out[i] += float(2 * (v1 + v2))
-        s = self.lam_prbfit / self.prb_size
-        return out[0] * s, out[1] * s, out[2] * s
+        self._prbfit_forms_dev(prb, d1, d2, _lib.ptr(self._pf3), 0)
+        f = [float(v) for v in self._pf3.cpu().numpy()]
+        return (f[0], f[1], f[2]) if d2 is not None else (f[0], f[0], f[0])
 
     # ------------------------------------------ 3-D Laplacian regulariser
     # rec_mpi.py:402-496 (ht_laplacian_*): gradient 2 lam/N B vars obj, Hessian
@@ -432,15 +433,14 @@ class Rec:
 
         mode="host" iterates as the reference does (step sizes on the host).
         mode="graph" keeps the step sizes on the device and replays the
-        steady-state iteration from a CUDA graph (same arithmetic; needs
-        lam_prbfit == 0, no error table and no checkpoints).  ``writer``
+        steady-state iteration from a CUDA graph (same arithmetic; needs no
+        error table and no checkpoints).  ``writer``
         (checkpoint.Writer) saves obj/prb/pos every vis_step iterations
         (rec_mpi.py:837-860, vis_debug)."""
         self.bh_setup()
         niter = self.niter if niter is None else niter
         checkpoints = writer is not None and getattr(self, "vis_step", -1) not in (-1, 0, None)
-        if (mode == "graph" and self.lam_prbfit == 0 and self.err_step == -1 and not checkpoints
-                and niter > self.start_iter):
+        if mode == "graph" and self.err_step == -1 and not checkpoints and niter > self.start_iter:
             cur = torch.cuda.current_stream(self.device)
             side = torch.cuda.Stream(device=self.device)
             side.wait_stream(cur)
@@ -534,8 +534,11 @@ class Rec:
                 self._lap_form(grads["obj"], etas["obj"], ctypes.c_void_p(hp + 8), etas["obj"],
                                ctypes.c_void_p(hp + 16))
                 self._lap_form(grads["obj"], etas["obj"], ctypes.c_void_p(hp + 24))
-        if sync or self.lam_prbfit != 0:
+        if sync:
             return self._bh_update_host(H.cpu().numpy(), first)
+        if self.lam_prbfit != 0:
+            # the probe-fit forms added to the Hessian slots on the device
+            self._prbfit_forms_dev(vars["prb"], grads["prb"], None if first else etas["prb"], _lib.ptr(H), 1)
         # ---- the same with the step sizes on the device
         st = _lib.stream_ptr()
         bh = self._bh
@@ -601,8 +604,6 @@ class Rec:
         the current stream into a CUDA graph; replay_iteration() then runs it
         with one launch.  Call after one iteration has run on this device (so
         every kernel's launch attributes are set).  Recording runs nothing."""
-        if self.lam_prbfit != 0:
-            raise ValueError("graph capture needs lam_prbfit == 0 (the probe-fit forms are host-side)")
         self.release_graph()
         st = _lib.stream_ptr()
         gc_on = gc.isenabled()

@@ -298,6 +298,27 @@ int ht_rec_objective_noalloc(ht_prop_s* prop, int nobj, int nzobj, int ntheta, i
                              void* stream);
 
 /* ------------------------------------------------------------------------
+ * Probe-fit regulariser lam |||D prb| - ref||^2 / (ndist nz n) on the device.
+ * Replaces Rec.gradient_prbfit and Rec.hessian_prbfit
+ * (src/holotomocupy/rec_mpi.py:365-398), whose host-side sums keep a BH
+ * iteration with the term out of a CUDA graph.  prb, d1, d2: complex64
+ * [ndist, nz, n]; ref: float32 [ndist, nz, n] (|D prb_true|, gen_sqrt_ref).
+ * --------------------------------------------------------------------- */
+/* grad += scale * D^H(2 (D prb - ref D prb / |D prb|)) per distance
+ * (scale = lam / (ndist nz n) times the variable scaling rho_prb);
+ * work: ndist*nz*n complex64. */
+int ht_prbfit_grad(ht_prop_s* prop, const void* prb, const float* ref, void* work, void* grad, float scale,
+                   void* stream);
+/* The forms f(u, w) = 2 scale sum (1 - ref/|p|) Re(u conj w) + ref/|p| Re(conj(l) u) Re(conj(l) w),
+ * p = D prb, l = p/|p|, u = D d1, w = D d2, for the pairs (d1,d1), (d1,d2),
+ * (d2,d2) (d2 = NULL: the first only), reduced in FP64 in a fixed order.
+ * hess_slots = 0: out[0..2] = the three forms; hess_slots = 1: out[0] +=
+ * f(d1,d1), out[1] += f(d1,d2), out[2] += f(d2,d2), out[3] += f(d1,d2) (the
+ * slots of ht_rec_hessian).  work: 3*ndist*nz*n complex64 plus 32 KiB. */
+int ht_prbfit_forms(ht_prop_s* prop, const void* prb, const void* d1, const void* d2, const float* ref, void* work,
+                    double* out, double scale, int hess_slots, void* stream);
+
+/* ------------------------------------------------------------------------
  * 3-D Laplacian regulariser (rec_mpi.py:402-496).  Arrays [nz, ny, nx],
  * complex64 (is_complex) or float32; work: (nz + 2) * ny * nx elements of the
  * same type.  L: the 7-point Laplacian, periodic in y and x, of the object

@@ -334,9 +334,11 @@ def test_prbfit_terms_match_reference(golden):
         assert rel_l2(rec.grads[k].cpu().numpy(), g[f"p_grad_{k}"]) < TOL, k
 
 
-def test_bh_with_prbfit_matches_reference(golden):
-    """4 BH iterations with lam_prbfit = 2e-3 (host step sizes) against the
-    reference's run: state and step sizes."""
+@pytest.mark.parametrize("mode", ["host", "graph"])
+def test_bh_with_prbfit_matches_reference(golden, mode):
+    """4 BH iterations with lam_prbfit = 2e-3 against the reference's run:
+    state and step sizes, with host step sizes and graph-replayed (the
+    probe-fit gradient and forms on the device, ht_prbfit_grad/forms)."""
     gr = golden("rec")
     g = golden("prbfit")
     from holotomocupy_b200.rec import Rec
@@ -354,7 +356,7 @@ def test_bh_with_prbfit_matches_reference(golden):
     rec.vars["prb"][:] = 1
     rec.vars["pos"][:] = cuda(gr["bh_pos_true"] + gr["bh_pos_err"])
     record = []
-    rec.BH(record=record)
+    rec.BH(record=record, mode=mode)
     tb = g["pbh_topbottom"]
     ref_alpha = [tb[0, 0] / tb[0, 1]] + [tb[2 * i, 0] / tb[2 * i, 1] for i in range(1, niter)]
     ref_beta = [0.0] + [tb[2 * i - 1, 0] / tb[2 * i - 1, 1] for i in range(1, niter)]
