@@ -54,3 +54,24 @@ def test_bad_arguments_are_rejected_without_gpu():
     assert L.ht_prop_create(0, 8, 1, None, ctypes.byref(h)) == 1
     assert L.ht_prop_D(None, None, None, 1, 0, None) == 1
     assert b"null" in L.ht_last_error()
+
+
+def test_new_entry_points_reject_bad_arguments_without_gpu():
+    """The padded-grid, slab, chunk, shared-coefficient and probe-fit entry
+    points check their arguments before touching a device."""
+    from holotomocupy_b200 import _lib
+    L = _lib.lib()
+    h = ctypes.c_void_p()
+    assert L.ht_conv2d_create(100, 64, ctypes.byref(h)) == 3          # 100 is not 2^a 3^b
+    assert L.ht_conv2d_run(None, None, None, None, 1, None) == 1
+    assert L.ht_pad_mirror(None, None, 1, 8, 8, None) == 1
+    x = ctypes.c_void_p(16)                                           # never dereferenced: the check fails first
+    assert L.ht_pad_mirror(x, x, 1, 8, 7, None) == 1                  # odd width
+    assert L.ht_pad_fold(x, x, 1, 7, 8, None) == 1                    # odd height
+    assert L.ht_tomo_R_slab(None, None, None, 1, 1, 0, None) == 1
+    assert L.ht_tomo_RT_slab(None, None, None, 1, 1, 0, 1.0, None) == 1
+    assert L.ht_rec_set_data_size(None, 1.0) == 1
+    assert L.ht_rec_set_shared_coefficients(None, 1) == 1
+    assert L.ht_prbfit_grad(None, None, None, None, None, 1.0, None) == 1
+    assert L.ht_prbfit_forms(None, None, None, None, None, None, None, 1.0, 0, None) == 1
+    assert b"null" in L.ht_last_error()
