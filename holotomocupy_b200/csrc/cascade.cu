@@ -488,6 +488,13 @@ k_casc_hess_q512(const float2* __restrict__ tmp, const float2* __restrict__ x0c,
   const bool valid = row < nrow;
   SmRow sm0{smem + line * SmRow::padded(N)};
   SmRow sm1{smem + (NDIR - 1) * kR512Lines * SmRow::padded(N) + line * SmRow::padded(N)};
+  // the rows read after the first transform (the second direction's
+  // spectrum, x0 and the data) are brought into L2 now
+  if (t == 0 && valid) {
+    if (NDIR == 2) l2_prefetch(tmp + (nrow + row) * N, N * sizeof(float2));
+    l2_prefetch(x0c + row * N, N * sizeof(float2));
+    l2_prefetch(data + row * N, N * sizeof(float));
+  }
   float2 v[16];
   r512_dct3_head(v, tmp + row * N, valid, sm0, t, tw4);
   r512_finish_to_regs(v, sm0, t, tw4);

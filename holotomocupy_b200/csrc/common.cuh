@@ -105,6 +105,18 @@ __host__ __device__ __forceinline__ float2 rot(float2 a) {
 }
 __host__ __device__ __forceinline__ float2 cmul_i(float2 a) { return make_float2(-a.y, a.x); }  // i*a
 
+// Bulk prefetch of [p, p + bytes) into L2 by the TMA unit: one instruction, no
+// registers, no shared memory and nothing to wait for; a kernel issues it for
+// rows it reads only later, so that those loads hit L2.  Skipped unless p is
+// 16-byte aligned and bytes a multiple of 16 (the instruction's rules); the
+// whole range must lie inside one allocation.
+__device__ __forceinline__ void l2_prefetch(const void* p, unsigned bytes) {
+#if defined(__CUDA_ARCH__)
+  if ((reinterpret_cast<unsigned long long>(p) & 15ull) == 0ull && (bytes & 15u) == 0u)
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+#endif
+}
+
 // --------------------------------------------------------- twiddle tables
 // For every supported transform length N the library keeps, per device, a
 // table tw4[m] = exp(-2*pi*i*m/(4N)), m in [0, 4N), computed in double and

@@ -261,136 +261,6 @@ k_dct_cols512(float2* data, int n, const float2* __restrict__ Hall, int ntab, co
                                               tw4, sync);
 }
 
-// ---------------- column pass at NZ = 512, staged through shared memory
-// The C = 8 columns of a CTA, and the same columns of the table, are copied
-// into shared memory with asynchronous 8-byte copies (cp.async): every warp
-// access covers whole 64-byte row segments, and all of a thread's copies are
-// in flight at once.  The data land in their DCT-II order (row r at position
-// dct_perm_inv(r) of its column line), each column line padded like a row
-// line (SmRow) and the lines an odd number of slots apart, so both the
-// row-segment copies and the line transforms are free of bank conflicts.  One
-// warp then owns one column: the DCT-II FFT, the in-register combine with the
-// table (as in k_dct_cols512) and the DCT-III FFT run with warp barriers only,
-// and the CTA stores the tile back, row segment by row segment.  Two CTA
-// barriers in all, against six in k_dct_cols512.
-struct Col512T {
-  static constexpr int N = 512, C = 8, THREADS = 32 * C;
-  static constexpr int LINE = SmRow::padded(N) + 1;  // odd: lines fall on different banks
-  static constexpr int SMEM = 2 * C * LINE * (int)sizeof(float2);
-};
-
-__device__ __forceinline__ void cp_async8(void* sdst, const void* gsrc) {
-  const unsigned s = (unsigned)__cvta_generic_to_shared(sdst);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gsrc) : "memory");
-}
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
-
-// col_combine with the table column in shared memory (position k = row k)
-template <bool CONJ>
-__device__ __forceinline__ void col_combine_s(float2& lo, float2& hi, int k, const SmRow& Hs,
-                                              const float2* __restrict__ tw4) {
-  const float2 w = __ldg(&tw4[k]);
-  const float2 P = cmul(w, lo), Q = cmulc(hi, w);
-  float2 hk = Hs.ld(k), hn = Hs.ld(512 - k);
-  if (CONJ) {
-    hk.y = -hk.y;
-    hn.y = -hn.y;
-  }
-  const float2 Gk = cmul(cscale(cadd(P, Q), 0.5f), hk);
-  const float2 Gn = cmul(cscale(cmul_i(csub(P, Q)), 0.5f), hn);
-  lo = cscale(cmul(w, cadd(Gk, cmul_i(Gn))), 0.5f);
-  hi = cscale(cmulc(csub(Gk, cmul_i(Gn)), w), 0.5f);
-}
-
-template <bool CONJ>
-__global__ void __launch_bounds__(Col512T::THREADS)
-k_dct_cols512t(float2* data, int n, const float2* __restrict__ Hall, int ntab, const float2* __restrict__ tw4) {
-  constexpr int N = 512, E = 16, C = Col512T::C, LINE = Col512T::LINE;
-  extern __shared__ float2 tile[];
-  float2* tabs = tile + C * LINE;
-  const int col0 = blockIdx.x * C;
-  float2* img = data + (long)blockIdx.y * N * n;
-  const float2* __restrict__ H = Hall + (long)(blockIdx.y % ntab) * N * n;
-  // ---- copy in: element (r, c) of the tile and of the table
-  for (int idx = threadIdx.x; idx < N * C; idx += Col512T::THREADS) {
-    const int r = idx / C, c = idx % C;
-    const int col = min(col0 + c, n - 1);  // columns past the edge: copies of the last (never stored)
-    const SmRow dl{tile + c * LINE}, hl{tabs + c * LINE};
-    const int pd = dct_perm_inv(r, N);
-    cp_async8(dl.p + pd + (pd >> 4), img + (long)r * n + col);
-    cp_async8(hl.p + r + (r >> 4), H + (long)r * n + col);
-  }
-  cp_async_wait_all();
-  __syncthreads();
-  // ---- warp w transforms column w
-  {
-    const int t = threadIdx.x % 32, c = threadIdx.x / 32;
-    const SmRow sm{tile + c * LINE}, Hs{tabs + c * LINE};
-    const WarpSync ws{};
-    float2 v[E];
-    fft_stage<N, E, 8, 1, false, true, true>(v, sm, t, tw4, ws);
-    fft_stage<N, E, 8, 8, false, true, true>(v, sm, t, tw4, ws);
-    // stage 3 (P = 64) for the butterflies b0, b1, kept in registers: v[8 s + j] = X[b_s + 64 j]
-    const int b0 = t, b1 = r512_b1(t);
-#pragma unroll
-    for (int s2 = 0; s2 < 2; ++s2) {
-      const int b = s2 ? b1 : b0;
-#pragma unroll
-      for (int j = 0; j < 8; ++j) v[8 * s2 + j] = sm.ld(b + 64 * j);
-      float2 w[8];
-      twiddles<8, false>(tw4, b, N, w);
-#pragma unroll
-      for (int j = 1; j < 8; ++j) v[8 * s2 + j] = cmul(v[8 * s2 + j], w[j]);
-      Dft<8, false>::run(&v[8 * s2]);
-    }
-    // combine, x Hw, pre-combine
-    if (t != 0) {
-#pragma unroll
-      for (int j = 0; j < 4; ++j) col_combine_s<CONJ>(v[j], v[15 - j], t + 64 * j, Hs, tw4);
-#pragma unroll
-      for (int j = 4; j < 8; ++j) col_combine_s<CONJ>(v[15 - j], v[j], 64 - t + 64 * (7 - j), Hs, tw4);
-    } else {
-      {
-        float2 h = Hs.ld(0);
-        if (CONJ) h.y = -h.y;
-        const float2 w = __ldg(&tw4[0]);
-        v[0] = cmul(cscale(cadd(cmul(w, v[0]), cmulc(v[0], w)), 0.5f), h);
-      }
-      {
-        float2 h = Hs.ld(256);
-        if (CONJ) h.y = -h.y;
-        const float2 w = __ldg(&tw4[256]);
-        const float2 G = cmul(cscale(cadd(cmul(w, v[4]), cmulc(v[4], w)), 0.5f), h);
-        v[4] = cscale(cmul(w, cadd(G, cmul_i(G))), 0.5f);
-      }
-#pragma unroll
-      for (int j = 1; j < 4; ++j) col_combine_s<CONJ>(v[j], v[8 - j], 64 * j, Hs, tw4);
-#pragma unroll
-      for (int j = 0; j < 4; ++j) col_combine_s<CONJ>(v[8 + j], v[15 - j], 32 + 64 * j, Hs, tw4);
-    }
-    __syncwarp();  // every stage-3 load is done before the stores below
-    // DCT-III FFT: stage 1 on the same butterflies, then stages 2 and 3 in place
-#pragma unroll
-    for (int s2 = 0; s2 < 2; ++s2) {
-      const int b = s2 ? b1 : b0;
-      Dft<8, false>::run(&v[8 * s2]);
-#pragma unroll
-      for (int j = 0; j < 8; ++j) sm.st(b * 8 + j, v[8 * s2 + j]);
-    }
-    __syncwarp();
-    fft_stage<N, E, 8, 8, false, true, true>(v, sm, t, tw4, ws);
-    fft_stage<N, E, 8, 64, false, true, false>(v, sm, t, tw4, ws);
-  }
-  __syncthreads();
-  // ---- copy out: output row g sits at position dct_perm(g)
-  for (int idx = threadIdx.x; idx < N * C; idx += Col512T::THREADS) {
-    const int r = idx / C, c = idx % C;
-    if (col0 + c >= n) continue;
-    const SmRow dl{tile + c * LINE};
-    img[(long)r * n + col0 + c] = dl.ld(dct_perm(r, N));
-  }
-}
-
 // ---------------------------------------------------------------- launch
 template <int N>
 static cudaError_t launch_dct_rows(bool inverse, const float2* in, float2* out, long nrows,
