@@ -23,11 +23,14 @@ def _requests(host=False):
 
 
 @pytest.mark.parametrize("host", [False, True])
-def test_served_results_equal_alone(host):
+@pytest.mark.parametrize("workers", [True, False])
+def test_served_results_equal_alone(host, workers):
+    """Admissions and retirements on the host worker threads (workers=True)
+    or inline in the launch loop give the same results."""
     from holotomocupy_b200.serving import Server, run_plain
     reqs = _requests(host)
     _, _, alone = run_plain(reqs)
-    srv = Server(max_active=8)
+    srv = Server(max_active=8, host_workers=workers)
     for r in reqs:
         srv.submit(r)
     done = {r.rid: r for r in srv.run(realtime=False)}
