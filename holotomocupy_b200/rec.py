@@ -158,6 +158,23 @@ class Rec:
     def __del__(self):
         self.close()
 
+    def reset(self):
+        """Return to the state of a new Rec of the same arguments -- every
+        array zero, no recorded graph, an empty convergence table -- keeping
+        the device memory, the library handles and the operator tables: a
+        server hands a finished reconstruction's Rec to the next request of
+        the same arguments without freeing and allocating (each free
+        synchronises the device).  Runs on the current stream."""
+        self.release_graph()
+        for d in (self.vars, self.grads, self.etas, self._c):
+            for t in d.values():
+                t.zero_()
+        for t in (self.data, self.ref, self.shrink_nd, self._gc, self._gpos, self._gprb, self._H, self._dots,
+                  self._bh, self._hist, self._count, self._vol, self._lapw, self._pfw, self._pf3, self._scal):
+            if t is not None:
+                t.zero_()
+        self.table = []
+
     # ------------------------------------------------------------ state
     def alloc_arrays(self):
         """rec_mpi.py:105-136 (device-resident, zero-initialised)."""

@@ -61,6 +61,22 @@ def estimate_bytes(args):
     return int(total * 1.1) + (64 << 20)
 
 
+def args_key(args):
+    """Hashable identity of a request's Rec arguments: requests with equal
+    keys can share one Rec, one after the other."""
+    import hashlib
+    items = []
+    for k, v in sorted(vars(args).items()):
+        if isinstance(v, torch.Tensor):
+            v = v.detach().cpu().numpy()
+        if isinstance(v, (np.ndarray, list, tuple)):
+            a = np.asarray(v)
+            items.append((k, a.dtype.str, a.shape, hashlib.sha1(np.ascontiguousarray(a).tobytes()).hexdigest()))
+        else:
+            items.append((k, repr(v)))
+    return tuple(items)
+
+
 @dataclass
 class Request:
     """One reconstruction: ``args`` as for Rec, measured amplitudes, initial
@@ -102,6 +118,8 @@ class _Slot:
         self.inflight = deque()  # (start, end) event pairs of the queued iterations, oldest first
         self.bytes = estimate_bytes(req.args)
         self.job = None          # the host worker's admission or retirement of this request
+        self.key = args_key(req.args)
+        self.reused = None       # a retired request's (rec, bytes, key) this one takes over
         self.state = "admitting"  # -> "running" -> "retiring"
 
 
@@ -112,9 +130,12 @@ class Server:
     admissions (building the Rec, uploading, the set-up pass) and retirements
     (the final pass, copying the results to the host) run on two host worker
     threads, so that the launch loop keeps feeding the GPU meanwhile; False
-    runs them inline in the loop."""
+    runs them inline in the loop.  reuse: a request takes over the Rec of a
+    retired request with the same arguments (Rec.reset) instead of freeing
+    it and allocating its own."""
 
-    def __init__(self, budget_bytes=None, max_active=16, graphs=True, device=None, depth=4, host_workers=True):
+    def __init__(self, budget_bytes=None, max_active=16, graphs=True, device=None, depth=4, host_workers=True,
+                 reuse=True):
         self.device = torch.device("cuda", torch.cuda.current_device() if device is None else device)
         if budget_bytes is None:
             free, _ = torch.cuda.mem_get_info(self.device)
@@ -124,6 +145,7 @@ class Server:
         self.graphs = graphs
         self.depth = max(1, int(depth))
         self.host_workers = host_workers
+        self.reuse = reuse
         self.queue = []
         self.done = []
         self.peak_bytes = 0
@@ -138,8 +160,13 @@ class Server:
         # would end the recording with an error.  The loop never waits for
         # it -- when a worker holds it, the iteration runs eagerly instead.
         self._dev_lock = threading.Lock()
-        self._retired = []        # (rec, bytes) retired and not yet released
-        self._ret_lock = threading.Lock()   # guards _retired (two worker threads use it)
+        # (rec, bytes, key) of retired requests whose device memory is still
+        # held: the next request with the same arguments takes the Rec over
+        # (Rec.reset), the others are released when an admission needs room.
+        # The retirement thread appends; only the loop takes entries out.
+        self._retired = []
+        self._ret_lock = threading.Lock()
+        self.reused = 0           # admissions that took over a retired request's Rec
 
     def submit(self, req):
         if estimate_bytes(req.args) > self.budget:
@@ -150,7 +177,11 @@ class Server:
     def _admit(self, slot):
         r = slot.req
         with torch.cuda.stream(slot.stream):
-            rec = Rec(r.args)
+            if slot.reused is not None:
+                rec = slot.reused[0]
+                rec.reset()
+            else:
+                rec = Rec(r.args)
             rec.data.copy_(r.data, non_blocking=True)
             if r.obj0 is not None:
                 rec.vars["obj"].copy_(r.obj0, non_blocking=True)
@@ -159,11 +190,11 @@ class Server:
             rec.bh_setup()
         slot.rec = rec
 
-    def _admit_job(self, slot, release_first):
-        """Worker side of an admission: release the retired requests first if
-        the loop asked for it; returns (bytes released, error or None)."""
+    def _admit_job(self, slot, to_release):
+        """Worker side of an admission: release the retired requests the loop
+        handed over first; returns (bytes released, error or None)."""
         with torch.cuda.device(self.device), self._dev_lock:
-            freed = self._release() if release_first else 0
+            freed = self._release(to_release) if to_release else 0
             try:
                 self._admit(slot)
             except (torch.OutOfMemoryError, _lib.HoloError) as err:
@@ -201,22 +232,26 @@ class Server:
         r.result = out
         r.t_done = time.perf_counter() - t0
         with self._ret_lock:
-            self._retired.append((rec, slot.bytes))   # freed lazily, graph included (see _release)
+            self._retired.append((rec, slot.bytes, slot.key))   # kept for reuse or freed lazily
         slot.rec = None
 
-    def _retired_bytes(self):
+    def _take_retired(self, entries=None):
+        """Remove entries (all when None) from the retired list; returns them."""
         with self._ret_lock:
-            return sum(b for _, b in self._retired)
+            if entries is None:
+                entries, self._retired = self._retired, []
+            else:
+                ids = {id(e) for e in entries}
+                self._retired = [e for e in self._retired if id(e) not in ids]
+        return entries
 
-    def _release(self):
-        """Free the retired reconstructions' device memory (synchronises the
+    def _release(self, retired):
+        """Free these retired reconstructions' device memory (synchronises the
         device); returns the bytes released."""
-        with self._ret_lock:
-            retired, self._retired = self._retired, []
-        freed = sum(b for _, b in retired)
+        freed = sum(e[1] for e in retired)
         torch.cuda.synchronize(self.device)
-        for rec, _ in retired:
-            rec.close()
+        for e in retired:
+            e[0].close()
         del retired
         # the library allocates outside torch's caching allocator: hand the
         # cached blocks back so that its next allocations find them
@@ -246,21 +281,30 @@ class Server:
                 now = time.perf_counter() - t0
                 while (pending and not wait_retire and len(active) < self.max_active
                        and (not realtime or pending[0].arrival <= now)):
-                    need = estimate_bytes(pending[0].args)
-                    releasable = self._retired_bytes()
+                    slot = _Slot(pending[0], self._streams[-1])
+                    with self._ret_lock:
+                        snap = list(self._retired)
+                    reuse = next((e for e in snap if e[2] == slot.key), None) if self.reuse else None
+                    need = 0 if reuse is not None else slot.bytes   # a reused Rec's bytes are counted already
+                    others = [e for e in snap if e is not reuse]
+                    releasable = sum(e[1] for e in others)
                     release_first = releasable > 0 and (force_release or self.used_bytes + need > self.budget)
                     projected = self.used_bytes - (releasable if release_first else 0)
                     if active and projected + need > self.budget:
                         break
+                    to_release = others if release_first else []
+                    self._take_retired(([reuse] if reuse is not None else []) + to_release)
+                    slot.reused = reuse
+                    self.reused += reuse is not None
                     r = pending.pop(0)
-                    slot = _Slot(r, self._streams.pop())
+                    self._streams.pop()
                     r.t_admit = time.perf_counter() - t0
                     # the ledger drops by what the release frees when the job reports it
-                    slot.job = admit_pool.submit(self._admit_job, slot, release_first)
+                    slot.job = admit_pool.submit(self._admit_job, slot, to_release)
                     force_release = False
                     active.append(slot)
-                    self.used_bytes += slot.bytes
-                    self.peak_bytes = max(self.peak_bytes, projected + slot.bytes)
+                    self.used_bytes += need
+                    self.peak_bytes = max(self.peak_bytes, projected + need)
                     self.max_concurrent = max(self.max_concurrent, len(active))
                 progressed = False
                 for slot in list(active):
@@ -276,14 +320,19 @@ class Server:
                             # other users of the GPU): retry once the others have made room
                             active.remove(slot)
                             self._streams.append(slot.stream)
-                            self.used_bytes -= slot.bytes
+                            if slot.reused is not None:   # its Rec stays held: back to the retired list
+                                with self._ret_lock:
+                                    self._retired.append(slot.reused)
+                            else:
+                                self.used_bytes -= slot.bytes
                             pending.insert(0, slot.req)
                             if not active or "out of memory" not in str(err):
                                 raise err
                             # retry after releasing the retired requests, or, with none
                             # retired, once an active request has retired
                             force_release = True
-                            wait_retire = self._retired_bytes() == 0
+                            with self._ret_lock:
+                                wait_retire = not self._retired
                             continue
                         slot.state = "running"
                     if slot.state == "retiring":
@@ -320,7 +369,7 @@ class Server:
                 admit_pool.shutdown(wait=True)
                 retire_pool.shutdown(wait=True)
         with self._dev_lock:
-            self.used_bytes -= self._release()
+            self.used_bytes -= self._release(self._take_retired())
         return self.done
 
     @staticmethod

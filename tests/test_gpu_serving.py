@@ -109,7 +109,7 @@ def test_out_of_memory_admission_returns_the_released_bytes():
     reqs = _requests()
     _, _, alone = run_plain(reqs)
     big = max(estimate_bytes(r.args) for r in reqs)
-    srv = Server(budget_bytes=4 * big, max_active=2)
+    srv = Server(budget_bytes=4 * big, max_active=2, reuse=False)
     admit = srv._admit
     state = {"injected": False}
 
@@ -127,3 +127,23 @@ def test_out_of_memory_admission_returns_the_released_bytes():
     assert srv.used_bytes == 0
     for r, ref in zip(reqs, alone):
         assert rel_l2(done[r.rid].result["obj"].numpy(), ref["obj"].numpy()) < 1e-5
+
+
+def test_reused_rec_gives_the_result_alone():
+    """One slot: the third request (the first one's arguments) takes over the
+    first request's retired Rec (Rec.reset) and still gives its result alone;
+    the ledger ends at zero."""
+    from holotomocupy_b200.serving import Server, run_plain
+    reqs = _requests()
+    _, _, alone = run_plain(reqs)
+    srv = Server(max_active=1)
+    for r in reqs:
+        srv.submit(r)
+    done = {r.rid: r for r in srv.run(realtime=False)}
+    assert srv.reused == 1
+    assert srv.used_bytes == 0
+    for r, ref in zip(reqs, alone):
+        got = done[r.rid].result
+        for k in ("obj", "prb", "pos"):
+            assert rel_l2(got[k].numpy(), ref[k].numpy()) < 1e-5, (r.rid, k)
+        assert len(got["history"]) == r.niter
