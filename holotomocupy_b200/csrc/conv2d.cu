@@ -59,10 +59,10 @@ k_conv_cols(float2* data, int ncols, const float2* __restrict__ H, const float2*
   const int col = min((int)blockIdx.x * C + c, ncols - 1);
   float2* img = data + (long)blockIdx.y * N * ncols + col;
   SmCol<C> sm{tile + c};
-  fft_line_from<N, false>(GColIn{img, ncols, valid}, sm, t, tw4);
+  fft_line_from<N, false, typename ColCfg<N>::PL>(GColIn{img, ncols, valid}, sm, t, tw4);
   for (int k = t; k < N; k += T) sm.st(k, cmul(sm.ld(k), __ldg(&H[(long)k * ncols + col])));
   __syncthreads();
-  fft_line_to<N, true>(sm, GColOut{img, ncols, valid}, t, tw4);
+  fft_line_to<N, true, typename ColCfg<N>::PL>(sm, GColOut{img, ncols, valid}, t, tw4);
 }
 
 // Mirror map of the padded grid onto the image along one axis: padded index

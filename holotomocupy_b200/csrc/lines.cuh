@@ -20,7 +20,8 @@ struct RowCfg {
 // at N >= 2048 the 4-column tile's rows are swizzled, see SmCol).
 template <int N>
 struct ColCfg {
-  static constexpr int T = Plan<N>::T;
+  using PL = ColPlan<N>;
+  static constexpr int T = PL::T;
   static constexpr int C = (N >= 2048) ? 4 : ((N >= 256) ? 8 : 16);
   static constexpr int THREADS = C * T;
   static constexpr int SMEM = N * C * (int)sizeof(float2);

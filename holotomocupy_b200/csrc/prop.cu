@@ -132,7 +132,7 @@ k_dct_cols(float2* data, int n, const float2* __restrict__ Hall, int ntab, const
   const int col = min((int)blockIdx.x * C + c, n - 1);
   float2* img = data + (long)blockIdx.y * NZ * n + col;
   SmCol<C> sm{tile + c};
-  fft_line_from<NZ, false>(ColIn<NZ>{img, n, valid}, sm, t, tw4);
+  fft_line_from<NZ, false, typename ColCfg<NZ>::PL>(ColIn<NZ>{img, n, valid}, sm, t, tw4);
   for (int k = t; k <= NZ / 2; k += T) {
     const float2 A = sm.ld(k), B = sm.ld(k == 0 ? 0 : NZ - k);
     const float2 w = __ldg(&tw4[k]);
@@ -153,7 +153,7 @@ k_dct_cols(float2* data, int n, const float2* __restrict__ Hall, int ntab, const
     }
   }
   __syncthreads();
-  fft_line_to<NZ, false>(sm, ColOut<NZ>{img, n, valid}, t, tw4);
+  fft_line_to<NZ, false, typename ColCfg<NZ>::PL>(sm, ColOut<NZ>{img, n, valid}, t, tw4);
 }
 
 // ------------------- column pass at NZ = 512: the combine in registers

@@ -396,10 +396,10 @@ k_symbol_cols(const float2* in, float2* out, int ncols, const float* __restrict_
   const int col = min((int)blockIdx.x * C + c, ncols - 1);
   const long off = (long)blockIdx.y * N * ncols + col;
   SmCol<C> sm{tile + c};
-  fft_line_from<N, false>(GColIn{in + off, ncols, valid}, sm, t, tw4);
+  fft_line_from<N, false, typename ColCfg<N>::PL>(GColIn{in + off, ncols, valid}, sm, t, tw4);
   for (int k = t; k < N; k += T) sm.st(k, cscale(sm.ld(k), __ldg(&sym[k])));
   __syncthreads();
-  fft_line_to<N, true>(sm, GColOut{out + off, ncols, valid}, t, tw4);
+  fft_line_to<N, true, typename ColCfg<N>::PL>(sm, GColOut{out + off, ncols, valid}, t, tw4);
 }
 
 template <int N>

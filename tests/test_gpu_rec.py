@@ -174,11 +174,12 @@ def test_taylor_orders():
     assert 3.0 < e2[0] / e2[1] < 5.0 and 6.0 < e3[0] / e3[1] < 10.0
 
 
-@pytest.mark.parametrize("n", [64, 512])
+@pytest.mark.parametrize("n", [64, 384, 512])
 def test_cascade_at_large_magnifications_matches_oracle(n):
-    """Magnifications from 0 to 3.5, detector and object n = 64 and 512 (the
-    512-row transforms have their own kernels).  Gradient and Hessian forms
-    against the FP64 oracle (rel <= 1e-4)."""
+    """Magnifications from 0 to 3.5, detector and object n = 64, 384 (lines
+    with a radix-3 stage) and 512 (the 512-row transforms have their own
+    kernels).  Gradient and Hessian forms against the FP64 oracle (rel <=
+    1e-4)."""
     from oracle import holo_oracle as O
     from holotomocupy_b200.rec import Rec
     ntheta, ndist = 3, 2
