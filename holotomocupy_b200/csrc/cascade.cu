@@ -204,11 +204,13 @@ __host__ __device__ constexpr int red_doubles(int K, int threads) {
 // the threads per SM grow with the row's shared memory.
 template <int N, int NSET, int NFFT>
 struct StCfg {
-  static constexpr int T = Plan<N>::T;
+  using PL = StPlan<N>;
+  static constexpr int T = PL::T;
   static constexpr int TR = NFFT * T;
   static constexpr int PER_LINE = NFFT * SmRow::padded(N) * 8 + NSET * N * 8;
   static constexpr int fit(int l) { return (l > 1 && l * PER_LINE > 100 * 1024) ? fit(l / 2) : l; }
-  static constexpr int LINES = fit(RowCfg<N>::LINES / NFFT > 0 ? RowCfg<N>::LINES / NFFT : 1);
+  static constexpr int ROW_LINES = (T >= 256) ? 1 : (256 / T);  // lines a CTA of plain row lines holds
+  static constexpr int LINES = fit(ROW_LINES / NFFT > 0 ? ROW_LINES / NFFT : 1);
   static constexpr int THREADS = LINES * TR;
   // each FFT group of T threads is a line with its own named barrier (1..15)
   static_assert(T % 32 != 0 || LINES * NFFT <= 15, "at most 15 line barriers per block");
@@ -350,7 +352,7 @@ k_casc_fwd(const T* __restrict__ c, const float* __restrict__ pos, const float* 
     dct2_put<N>(sm, tx, u);
   }
   __syncthreads();
-  dct2_finish<N, TT>(sm, t, tw4, tmp + row * N, valid);
+  dct2_finish<N, TT, typename CF::PL>(sm, t, tw4, tmp + row * N, valid);
 }
 
 // ======================================== residual row pass
@@ -621,7 +623,7 @@ k_casc_adj(const float2* __restrict__ tmp, float2* __restrict__ Pc, T* __restric
            double* __restrict__ rows, CascDims D, const float2* __restrict__ tw4) {
   using CF = StCfg<N, 3, 1>;
   constexpr int TT = CF::T;
-  constexpr int E = Plan<N>::E;
+  constexpr int E = CF::PL::E;
   extern __shared__ float2 smem[];
   double* red = reinterpret_cast<double*>(reinterpret_cast<char*>(smem) + CF::FFT_BYTES);
   const int line = threadIdx.x / TT, t = threadIdx.x % TT;
@@ -641,7 +643,7 @@ k_casc_adj(const float2* __restrict__ tmp, float2* __restrict__ Pc, T* __restric
     const float* const w[3] = {rg.py, rg.dpy, rg.d2py};
     vrows_adj<T>(V, V + adj_pair_off(D.nobj), D.nobj, c + coef_off(D, th), rg.yy, w, t, TT);
   }
-  dct3_start<N, TT>(sm, t, tw4, tmp + row * N, valid);  // ends with a barrier: V is complete
+  dct3_start<N, TT, typename CF::PL>(sm, t, tw4, tmp + row * N, valid);  // ends with a barrier: V is complete
   const T* V0 = V;
   const T* V12 = V + adj_pair_off(D.nobj);
   float s[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
@@ -961,7 +963,7 @@ k_casc_hess_fwd(const T* __restrict__ c, const float* __restrict__ pos, const fl
   // direction d's line is transformed by the row's d-th group of CF::T threads
   const long nrow = D.nimg * D.nz;
   const int d = t / CF::T;
-  dct2_finish<N, CF::T>(d == 0 ? sm0 : sm1, t % CF::T, tw4, tmp + (d * nrow + row) * N, valid);
+  dct2_finish<N, CF::T, typename CF::PL>(d == 0 ? sm0 : sm1, t % CF::T, tw4, tmp + (d * nrow + row) * N, valid);
 }
 
 // ======================================== Hessian quadratic terms

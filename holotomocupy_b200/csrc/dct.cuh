@@ -22,10 +22,11 @@ __device__ __forceinline__ void dct2_put(const SmRow& sm, int g, float2 v) {
 
 // FFT the staged line and write C[0..N) to dst (skipped when !valid).  The
 // caller has synchronised after the last dct2_put.
-template <int N, int T>
+template <int N, int T, class PL = Plan<N>>
 __device__ __forceinline__ void dct2_finish(const SmRow& sm, int t, const float2* __restrict__ tw4, float2* dst,
                                             bool valid) {
-  fft_line<N, false>(sm, t, tw4, line_sync<T>());
+  static_assert(T == PL::T, "T threads a line is the plan's");
+  fft_line<N, false, PL>(sm, t, tw4, line_sync<T>());
   if (!valid) return;
   for (int k = t; k <= N / 2; k += T) {
     const float2 A = sm.ld(k), B = sm.ld(k == 0 ? 0 : N - k);
@@ -39,9 +40,10 @@ __device__ __forceinline__ void dct2_finish(const SmRow& sm, int t, const float2
 // Load the DCT-III input G[0..N) from src, pre-combine and FFT.  Afterwards
 // output sample g is sm.ld(dct_perm(g, N)).  Ends with a barrier over the
 // line's threads.
-template <int N, int T>
+template <int N, int T, class PL = Plan<N>>
 __device__ __forceinline__ void dct3_start(const SmRow& sm, int t, const float2* __restrict__ tw4, const float2* src,
                                            bool valid) {
+  static_assert(T == PL::T, "T threads a line is the plan's");
   // every load of the line is issued before the first store, so the thread
   // waits for global memory once
   constexpr int NM = (N / 2) / T + 1;  // m = t + i T covers 0..N/2
@@ -66,7 +68,7 @@ __device__ __forceinline__ void dct3_start(const SmRow& sm, int t, const float2*
     }
   }
   line_sync<T>()();
-  fft_line<N, false>(sm, t, tw4, line_sync<T>());
+  fft_line<N, false, PL>(sm, t, tw4, line_sync<T>());
 }
 
 // Sums of K values over the T threads of each line, in double precision; the

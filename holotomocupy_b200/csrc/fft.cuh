@@ -141,7 +141,7 @@ HT_PLAN(192, 24, 8, 8, 3)
 HT_PLAN(256, 8, 8, 8, 4)
 HT_PLAN(384, 12, 4, 4, 4, 3, 2)   // 12 samples a thread: the stencil row kernels keep their occupancy
 HT_PLAN(512, 8, 8, 8, 8)
-HT_PLAN(768, 24, 8, 8, 4, 3)
+HT_PLAN(768, 12, 4, 4, 4, 4, 3)
 HT_PLAN(1024, 16, 8, 8, 8, 2)
 HT_PLAN(1536, 24, 8, 8, 8, 3)
 HT_PLAN(2048, 16, 8, 8, 8, 4)
@@ -157,6 +157,19 @@ template <int N>
 struct ColPlan : Plan<N> {};
 template <>
 struct ColPlan<384> : PlanOf<384, 24, 8, 8, 3, 2> {};
+template <>
+struct ColPlan<768> : PlanOf<768, 24, 8, 8, 4, 3> {};
+
+// StPlan<N>: the plan of the stencil row kernels of the fused cascade, whose
+// rows carry the stencil work beside the transform (so more threads a line
+// pay): the row plan, except at 1024 samples, where 8 samples a thread (128
+// threads a line) beat 16 (BH iteration at 1024^2 x 256 x 4: 273 against
+// 283 ms); the other 1024-sample lines (the Radon transform's at n = 512)
+// keep 16, which is faster for them.
+template <int N>
+struct StPlan : Plan<N> {};
+template <>
+struct StPlan<1024> : PlanOf<1024, 8, 8, 8, 8, 2> {};
 
 // ------------------------------------------------------ synchronisation
 // Barrier between the stages of one line's transform.  CtaSync: the whole
@@ -310,10 +323,9 @@ __device__ __forceinline__ void fft_stages_io(float2 (&v)[E], const IN& in, cons
 // barrier `sync` covers (it barriers between stages).  The caller
 // synchronises before (so the input is complete); the result is complete
 // for the threads `sync` covers on return.
-template <int N, bool INV, class SM, class SY = CtaSync>
+template <int N, bool INV, class PL = Plan<N>, class SM, class SY = CtaSync>
 __device__ __forceinline__ void fft_line(const SM& sm, int t, const float2* __restrict__ tw4,
                                          const SY& sync = SY{}) {
-  using PL = Plan<N>;
   float2 v[PL::E];
   fft_stages<N, PL::E, 1, INV>(v, sm, t, tw4, sync, typename PL::R{});
 }
@@ -331,10 +343,9 @@ __device__ __forceinline__ void fft_line_from(const IN& in, const SM& sm, int t,
 // FFT of a line read from `in` and written to `out` (the first stage loads
 // from `in`, the last stage stores to `out`, the stages between pass through
 // shared memory); no barrier is needed before it, none is made after it.
-template <int N, bool INV, class IN, class SM, class OUT, class SY = CtaSync>
+template <int N, bool INV, class PL = Plan<N>, class IN, class SM, class OUT, class SY = CtaSync>
 __device__ __forceinline__ void fft_line_io(const IN& in, const SM& sm, const OUT& out, int t,
                                             const float2* __restrict__ tw4, const SY& sync = SY{}) {
-  using PL = Plan<N>;
   float2 v[PL::E];
   fft_stages_io<N, PL::E, 1, INV, true, true>(v, in, sm, out, t, tw4, sync, typename PL::R{});
 }

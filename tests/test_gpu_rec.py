@@ -174,16 +174,18 @@ def test_taylor_orders():
     assert 3.0 < e2[0] / e2[1] < 5.0 and 6.0 < e3[0] / e3[1] < 10.0
 
 
-@pytest.mark.parametrize("n", [64, 384, 512])
-def test_cascade_at_large_magnifications_matches_oracle(n):
-    """Magnifications from 0 to 3.5, detector and object n = 64, 384 (lines
-    with a radix-3 stage) and 512 (the 512-row transforms have their own
-    kernels).  Gradient and Hessian forms against the FP64 oracle (rel <=
-    1e-4)."""
+@pytest.mark.parametrize("n,nz", [(64, 64), (384, 384), (512, 512), (768, 96), (1024, 64)])
+def test_cascade_at_large_magnifications_matches_oracle(n, nz):
+    """Magnifications from 0 to 3.5; rows of n = 64, 384 and 768 samples
+    (lines with a radix-3 stage), 512 (the 512-sample rows have their own
+    kernels) and 1024, nz detector rows and as many object rows (short images
+    at 768 and 1024 keep the FP64 oracle's volumes small).  Gradient and
+    Hessian forms against the FP64 oracle (rel <= 1e-4)."""
     from oracle import holo_oracle as O
     from holotomocupy_b200.rec import Rec
     ntheta, ndist = 3, 2
     args = rec_args(n, ntheta, ndist, n)
+    args.nz = args.nzobj = nz
     rec = Rec(args)
     orc = O.Rec(args, "complex128")
     eff = np.array([[1.0, 3.5], [0.5, 1.3], [2.9, 0.0]])
@@ -191,14 +193,14 @@ def test_cascade_at_large_magnifications_matches_oracle(n):
     orc.eff_demagnifications[:] = eff.astype("float32")
     rng = np.random.default_rng(7)
     cn = lambda *s: rng.standard_normal(s) + 1j * rng.standard_normal(s)
-    data = (np.abs(rng.standard_normal((ntheta, ndist, n, n))) + 0.5).astype("float32")
+    data = (np.abs(rng.standard_normal((ntheta, ndist, nz, n))) + 0.5).astype("float32")
     rec.data[:] = cuda(data)
     orc.data[:] = data
 
     def state(sc):
-        return {"prb": (1 + 0.1 * cn(ndist, n, n)).astype("complex64") if sc == 1 else
-                (sc * cn(ndist, n, n)).astype("complex64"),
-                "proj": (0.05 * cn(ntheta, n, n)).astype("complex64"),
+        return {"prb": (1 + 0.1 * cn(ndist, nz, n)).astype("complex64") if sc == 1 else
+                (sc * cn(ndist, nz, n)).astype("complex64"),
+                "proj": (0.05 * cn(ntheta, nz, n)).astype("complex64"),
                 "pos": rng.uniform(-2, 2, (ntheta, ndist, 2)).astype("float32")}
     v, gr, et = state(1), state(0.1), state(0.1)
     g = lambda d: {k: cuda(x) for k, x in d.items()}
@@ -220,7 +222,7 @@ def test_cascade_at_large_magnifications_matches_oracle(n):
     assert abs(f / fo - 1) < 1e-4, (f, fo)
     from holotomocupy_b200 import _lib
     c = rec._coeff_into(gv["proj"], torch.empty_like(gv["proj"]))
-    amp = torch.empty(ntheta, ndist, n, n, dtype=torch.float32, device="cuda")
+    amp = torch.empty(ntheta, ndist, nz, n, dtype=torch.float32, device="cuda")
     _lib.call("ht_rec_forward", rec._h, _lib.ptr(c), _lib.ptr(gv["pos"]), _lib.ptr(rec.eff_demagnifications),
               _lib.ptr(gv["prb"]), None, _lib.ptr(amp), None, _lib.stream_ptr())
     y = [ov["prb"], ov["proj"], ov["pos"]]

@@ -27,7 +27,7 @@ def test_R_RT_match_reference(golden, tag):
         assert rel_l2(out, ref) < TOL, (key, rel_l2(out, ref))
 
 
-@pytest.mark.parametrize("n,ntheta,nz", [(128, 180, 3), (256, 96, 2), (384, 48, 2)])
+@pytest.mark.parametrize("n,ntheta,nz", [(128, 180, 3), (256, 96, 2), (384, 48, 2), (512, 32, 2)])
 def test_R_RT_against_oracle(n, ntheta, nz):
     from holotomocupy_b200 import Tomo
     rng = np.random.default_rng(n)
