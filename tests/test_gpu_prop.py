@@ -38,7 +38,8 @@ def test_D_DT_match_reference(golden, tag):
     assert rel_l2(d2.cpu().numpy(), g[f"{tag}_D2d"]) < TOL_REF
 
 
-@pytest.mark.parametrize("n,nz", [(128, 128), (512, 512), (36, 512), (384, 256), (36, 18), (18, 36), (64, 2048), (32, 4096)])
+@pytest.mark.parametrize("n,nz", [(128, 128), (512, 512), (36, 512), (384, 256), (36, 18), (18, 36), (48, 1024), (64, 2048),
+                                  (32, 4096)])
 def test_D_against_fp64_oracle(n, nz):
     from holotomocupy_b200 import Propagation
     rng = np.random.default_rng(n + nz)
