@@ -444,7 +444,8 @@ def main():
                   "latency_ms_p99": float(np.percentile(lat_plain, 99)),
                   "form": "host step sizes (H and dots copied to the host each iteration), eager launches"},
         "served": served,
-        "gpu_launches": launches,
+        "gpu_launches": launches * a.steps,      # the library's kernels in the timed region (all steps)
+        "gpu_launches_per_step": launches,
         "roofline": roof,
         "e2e": e2e,
         "clocks": clk,
