@@ -265,6 +265,165 @@ def build_problem(n, ntheta, ndist, seed, device):
     return rec, obj, prb, pos, data
 
 
+def run_rows(a):
+    """The rows beside the BH hot path, each timed on the device with CUDA
+    events around `steps` calls after `warmup` (a checkpoint, host work, with
+    the host clock), and -- where the oracle restates the reference's
+    algorithm -- the oracle beside it on a bounded sample of the same workload
+    on all host cores, scaled linearly as the main CPU baseline is:
+      * a BH iteration at 512^3 x 900 x 4, graph-replayed, plain, with the
+        probe-fit regulariser (lam_prbfit = 2e-3; rec_mpi.py:365-398) and with
+        the Laplacian regulariser (lam_laplacian = 1e-3; rec_mpi.py:400-496);
+      * Tomo.fbp and Tomo.rec_tomo (4 CG iterations) of a 900 x 512 x 512
+        sinogram (tomo.py:163-210); oracle: one slice;
+      * Shift.Sback of 3600 images of 512^2 (shift.py:138-148); oracle: 16 images;
+      * RecNFP (rec_nfp_mpi.py:100-144), a 512^2 probe, a 768^2 projection and
+        256 scan positions: BH iterations (host step sizes, as the reference);
+      * a checkpoint of the 512^3 x 900 x 4 state written and read back
+        (writer.py:57-110, reader.py:260-340; the .npz layout, h5py being
+        absent on the box)."""
+    import tempfile
+    import types
+    import torch
+    from holotomocupy_b200 import RecNFP, Shift, Tomo
+    from holotomocupy_b200.checkpoint import Writer, read_checkpoint
+    from holotomocupy_b200.rec import Rec
+    dev = torch.device("cuda", 0)
+    threads = os.cpu_count() or 1
+    n, ntheta, ndist = 512, 900, 4
+    g = torch.Generator(device=dev).manual_seed(8)
+    rng = np.random.default_rng(8)
+
+    def timed(fn, steps=None, warmup=None):
+        for _ in range(a.warmup if warmup is None else warmup):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        k = a.steps if steps is None else steps
+        e0.record()
+        for _ in range(k):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / k
+
+    out = {}
+    # ---- BH iterations, plain and with each regulariser
+    base, obj, prb, pos, data = build_problem(n, ntheta, ndist, 4321, dev)
+    del obj
+    prb0 = torch.ones_like(prb)
+
+    def bh_ms(rec):
+        st = torch.cuda.Stream(device=dev)
+        with torch.cuda.stream(st):
+            reset_state(rec, prb0, pos, data)
+            rec.bh_setup()
+            rec.bh_iteration(0, sync=False)
+            rec.capture_iteration()
+            ms = timed(rec.replay_iteration)
+            rec.release_graph()
+        return ms
+
+    out["bh_plain_ms"] = bh_ms(base)
+    base.close()
+    del base
+    torch.cuda.empty_cache()
+    for key, lam in (("lam_prbfit", 2e-3), ("lam_laplacian", 1e-3)):
+        args = workload_args(n, ntheta, ndist)
+        setattr(args, key, lam)
+        rec = Rec(args)
+        rec.ref.copy_(prb.abs())   # the probe-fit's reference amplitude
+        out[f"bh_{key}_ms"] = bh_ms(rec)
+        rec.close()
+        del rec
+        torch.cuda.empty_cache()
+    for key in ("lam_prbfit", "lam_laplacian"):
+        out[f"bh_{key}_extra_pct"] = 100.0 * (out[f"bh_{key}_ms"] / out["bh_plain_ms"] - 1.0)
+    del data, prb, pos, prb0
+    torch.cuda.empty_cache()
+
+    O = _oracle(threads)
+    # ---- filtered back-projection and the CG initial guess
+    theta = workload_args(n, ntheta, ndist).theta
+    tomo = Tomo(n, n, theta, 0.9)
+    d = torch.randn(ntheta, n, n, dtype=torch.complex64, device=dev, generator=g)
+    out["fbp_ms"] = timed(lambda: tomo.fbp(d))
+    out["rec_tomo_4it_ms"] = timed(lambda: tomo.rec_tomo(d, 4), steps=2, warmup=1)
+    ot = O.Tomo(n, 1, theta, 0.9, "complex64")
+    ds = (rng.standard_normal((ntheta, 1, n)) + 1j * rng.standard_normal((ntheta, 1, n))).astype("complex64")
+    t0 = time.perf_counter()
+    ot.fbp(ds)
+    t1 = time.perf_counter()
+    ot.rec_tomo(ds, 4)
+    t2 = time.perf_counter()
+    out["fbp_cpu_ms"] = (t1 - t0) * 1e3 * n
+    out["rec_tomo_4it_cpu_ms"] = (t2 - t1) * 1e3 * n
+    del tomo, d
+    torch.cuda.empty_cache()
+    # ---- back-projection shift
+    nimg = ntheta * ndist
+    sh = Shift(n, n, n, n, "complex64")
+    sp = torch.randn(nimg, n, n, dtype=torch.complex64, device=dev, generator=g)
+    rs = 4 * torch.rand(nimg, 2, device=dev, generator=g) - 2
+    out["sback_ms"] = timed(lambda: sh.Sback(sp, rs, 1.0))
+    osh = O.Shift(n, n, n, n, "complex64", dtype="complex64")
+    t0 = time.perf_counter()
+    osh.Sback(sp[:16].cpu().numpy(), rs[:16].cpu().numpy(), np.float32(1.0))
+    out["sback_cpu_ms"] = (time.perf_counter() - t0) * 1e3 * nimg / 16
+    del sh, sp, rs
+    torch.cuda.empty_cache()
+    # ---- near-field ptychography
+    nargs = types.SimpleNamespace(distance=np.array([4e-3]), wavelength=WAVELENGTH, voxelsize=VOXEL, ntheta=256,
+                                  nz=512, n=512, nzobj=768, nobj=768, obj_dtype="complex64", rho=[1, 0.5, 0.1],
+                                  niter=10 ** 6, nchunk=256, vis_step=-1, err_step=-1, start_iter=0)
+    rn = RecNFP(nargs)
+    pos_t = 8 * torch.rand(256, 2, device=dev, generator=g) - 4
+    rn.vars["prb"].copy_(1 + 0.2 * torch.randn(512, 512, dtype=torch.complex64, device=dev, generator=g))
+    rn.vars["proj"].copy_(0.05 * torch.randn(768, 768, dtype=torch.complex64, device=dev, generator=g))
+    rn.vars["pos"].copy_(pos_t)
+    rn.gen_sqrt_data(rn.vars, rn.data)
+    for dd in (rn.vars, rn.grads, rn.etas):
+        for v in dd.values():
+            v.zero_()
+    rn.vars["prb"].fill_(1)
+    rn.vars["pos"].copy_(pos_t + 0.3 * (2 * torch.rand(256, 2, device=dev, generator=g) - 1))
+    rn.BH(niter=2)   # warm-up
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    rn.BH(niter=8)   # a solve of 8 iterations from the warm-up's state
+    e1.record()
+    torch.cuda.synchronize()
+    out["nfp_bh_iteration_ms"] = e0.elapsed_time(e1) / 8
+    rn.close()
+    del rn
+    torch.cuda.empty_cache()
+    # ---- checkpoint of the 512^3 state
+    st = {"obj": torch.randn(n, n, n, dtype=torch.complex64, device=dev, generator=g),
+          "prb": torch.randn(ndist, n, n, dtype=torch.complex64, device=dev, generator=g),
+          "pos": torch.rand(ntheta, ndist, 2, device=dev, generator=g)}
+    nbytes = sum(v.numel() * v.element_size() for v in st.values())
+    with tempfile.TemporaryDirectory() as tmp:
+        w = Writer(tmp, fmt="npz")
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        path = w.write_checkpoint(st, 1, 1.0)
+        t1 = time.perf_counter()
+        back = read_checkpoint(path, n, n, device=dev)
+        torch.cuda.synchronize()
+        t2 = time.perf_counter()
+        out["checkpoint_write_s"], out["checkpoint_read_s"] = t1 - t0, t2 - t1
+        out["checkpoint_write_gbs"], out["checkpoint_read_gbs"] = nbytes / (t1 - t0) / 1e9, nbytes / (t2 - t1) / 1e9
+        out["checkpoint_obj_max_abs_diff"] = float((back["obj"] - st["obj"]).abs().max())
+    line = {"metric": "rows beside the BH hot path: device time per call (ms), oracle on the host cores beside it",
+            "unit": "ms", "value": out["bh_plain_ms"], "higher_is_better": False, "steps": a.steps,
+            "warmup": a.warmup, "n_gpus": 1, "dtype": "c64", "data": "synthetic (seeded)", "cpu_cores": threads,
+            "config": {"workload": "512^3 object, 900 angles, 4 distances; RecNFP 512^2 probe, 768^2 projection, "
+                                   "256 positions"},
+            "rows": {k: (round(v, 4) if isinstance(v, float) else v) for k, v in out.items()}}
+    print(json.dumps(line), flush=True)
+
+
 def reset_state(rec, prb0, pos0, data=None):
     import torch
     for d in (rec.vars, rec.grads, rec.etas):
@@ -301,6 +460,9 @@ def main():
     ap.add_argument("--prop", action="store_true",
                     help="the propagator against the padded-grid path on torch's cuFFT (1024^2 x 4, 512^2, 2048^2) "
                          "instead of the BH line")
+    ap.add_argument("--rows", action="store_true",
+                    help="the rows beside the BH path (regularisers, fbp / rec_tomo, Sback, RecNFP, checkpoints) "
+                         "instead of the BH line")
     ap.add_argument("--no-small-chain", action="store_true",
                     help="reference arm: skip the unscaled small-chain BH iterations")
     ap.add_argument("--profile", action="store_true",
@@ -323,6 +485,9 @@ def main():
         return
     if a.large:
         run_large(a)
+        return
+    if a.rows:
+        run_rows(a)
         return
 
     import torch

@@ -315,15 +315,23 @@ __device__ __forceinline__ bool sback_tap(int p, int npix, int ncell, float shif
   return true;
 }
 
-// The pixels whose windows can reach `cell`, padded by two on each side
-// (membership is decided by sback_tap).
+// The pixels whose windows can reach `cell`: sback_tap admits pixel p only
+// when its position x(p) lies in (cell - 2m, cell + 2m], so p lies within
+// (cell -+ 2m - c) / m + npix / 2; the range is widened by 0.01 cell units
+// (far above the float rounding of x) and one pixel on each side, and
+// membership is still decided by sback_tap.
 __device__ __forceinline__ void sback_range(int cell, int npix, int ncell, float shift, float m0, int* p0, int* p1) {
   const float c = -shift + (m0 - 1.0f) / 2.0f + (float)(ncell / 2);
-  const float lo = ((float)cell - 2.0f * m0 - 2.0f - c) / m0 + (float)(npix / 2);
-  const float hi = ((float)cell + 2.0f * m0 + 2.0f - c) / m0 + (float)(npix / 2);
-  *p0 = max(0, (int)floorf(fmaxf(lo, -1.0f)) - 2);
-  *p1 = min(npix - 1, (int)ceilf(fminf(hi, (float)npix)) + 2);
+  const float lo = ((float)cell - 2.0f * m0 - 0.01f - c) / m0 + (float)(npix / 2);
+  const float hi = ((float)cell + 2.0f * m0 + 0.01f - c) / m0 + (float)(npix / 2);
+  *p0 = max(0, (int)floorf(fmaxf(lo, -1.0f)) - 1);
+  *p1 = min(npix - 1, (int)ceilf(fminf(hi, (float)npix)) + 1);
 }
+
+// Candidate pixels of a cell's row taps held in registers (the x taps are the
+// same for every row of the cell); wider candidate ranges (very small
+// magnifications) take the loop that tests them per row.
+constexpr int kSbackX = 16;
 
 __global__ void k_sback(const float2* __restrict__ g, float2* __restrict__ f, const float* __restrict__ r,
                         const float* __restrict__ mag, int nmag, ShiftDims S, long batch) {
@@ -339,20 +347,46 @@ __global__ void k_sback(const float2* __restrict__ g, float2* __restrict__ f, co
     sback_range(xx, S.n, S.npsi, rx, m0, &tx0, &tx1);
     sback_range(yy, S.nz, S.nzpsi, ry, m0, &ty0, &ty1);
     const float2* gb = g + b * (long)S.nz * S.n;
-    for (int ty = ty0; ty <= ty1; ++ty) {
-      float wy;
-      if (!sback_tap(ty, S.nz, S.nzpsi, ry, m0, yy, &wy)) continue;
-      const float2* grow = gb + (long)ty * S.n;
-      float2 row = make_float2(0.f, 0.f);
-      for (int tx = tx0; tx <= tx1; ++tx) {
-        float wx;
-        if (!sback_tap(tx, S.n, S.npsi, rx, m0, xx, &wx)) continue;
-        const float2 v = __ldg(&grow[tx]);
-        row.x += wx * v.x;
-        row.y += wx * v.y;
+    if (tx1 - tx0 < kSbackX) {
+      // the x taps once per cell: weights and a membership mask over tx0 + k
+      float wxs[kSbackX];
+      unsigned mx = 0u;
+#pragma unroll
+      for (int k = 0; k < kSbackX; ++k) {
+        wxs[k] = 0.f;
+        if (tx0 + k <= tx1 && sback_tap(tx0 + k, S.n, S.npsi, rx, m0, xx, &wxs[k])) mx |= 1u << k;
       }
-      acc.x += wy * row.x;
-      acc.y += wy * row.y;
+      for (int ty = ty0; ty <= ty1; ++ty) {
+        float wy;
+        if (!sback_tap(ty, S.nz, S.nzpsi, ry, m0, yy, &wy)) continue;
+        const float2* grow = gb + (long)ty * S.n + tx0;
+        float2 row = make_float2(0.f, 0.f);
+#pragma unroll
+        for (int k = 0; k < kSbackX; ++k) {
+          if (!((mx >> k) & 1u)) continue;
+          const float2 v = __ldg(&grow[k]);
+          row.x += wxs[k] * v.x;
+          row.y += wxs[k] * v.y;
+        }
+        acc.x += wy * row.x;
+        acc.y += wy * row.y;
+      }
+    } else {
+      for (int ty = ty0; ty <= ty1; ++ty) {
+        float wy;
+        if (!sback_tap(ty, S.nz, S.nzpsi, ry, m0, yy, &wy)) continue;
+        const float2* grow = gb + (long)ty * S.n;
+        float2 row = make_float2(0.f, 0.f);
+        for (int tx = tx0; tx <= tx1; ++tx) {
+          float wx;
+          if (!sback_tap(tx, S.n, S.npsi, rx, m0, xx, &wx)) continue;
+          const float2 v = __ldg(&grow[tx]);
+          row.x += wx * v.x;
+          row.y += wx * v.y;
+        }
+        acc.x += wy * row.x;
+        acc.y += wy * row.y;
+      }
     }
   }
   f[(b * S.nzpsi + yy) * (long)S.npsi + xx] = acc;

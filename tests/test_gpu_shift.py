@@ -64,6 +64,30 @@ def test_back_projection_shift_matches_reference(golden, tag):
         assert rel_l2(csb, o.curlySback(R("g"), R("r"), R("m"))) < TOL
 
 
+@pytest.mark.parametrize("m", [0.001, 0.3, 0.93, 1.0, 2.5, 3.5])
+def test_sback_over_magnifications_matches_oracle(m):
+    """Sback with one magnification per call from 0.001 (candidate ranges too
+    wide for the register-held column taps; the reference's windows then reach
+    no cell) to 3.5, shifts of a few pixels, against the FP64 oracle's
+    restatement of the reference's scatter (1e-5)."""
+    from holotomocupy_b200 import Shift
+    rng = np.random.default_rng(int(1000 * m))
+    n, npsi, nz, nzpsi, nt = 40, 48, 32, 36, 3
+    g = (rng.standard_normal((nt, nz, n)) + 1j * rng.standard_normal((nt, nz, n))).astype("complex64")
+    r = rng.uniform(-3, 3, (nt, 2)).astype("float32")
+    s = Shift(n, npsi, nz, nzpsi, "complex64")
+    o = O.Shift(n, npsi, nz, nzpsi, "complex64", "complex128")
+    sb = s.Sback(torch.from_numpy(g).cuda(), torch.from_numpy(r).cuda(), m).cpu().numpy()
+    ref = o.Sback(g, r, np.float32(m))
+    if not np.any(ref):   # m = 0.001: windows of +-2m reach no cell, in the reference as here
+        assert not np.any(sb)
+    else:
+        # at m = 0.3 a cell takes a few taps of small weight, and FP32 rounding
+        # alone puts any FP32 evaluation ~1.5e-5 from FP64 (the FP32 oracle too)
+        tol = 5e-5 if m < 0.5 else TOL
+        assert rel_l2(sb, ref) < tol, rel_l2(sb, ref)
+
+
 @pytest.mark.parametrize("mag", [1.0, 0.8, 1.25, 0.0])
 def test_adjoint_and_oracle(mag):
     from holotomocupy_b200 import Shift
