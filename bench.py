@@ -292,6 +292,12 @@ def run_rows(a):
     threads = os.cpu_count() or 1
     n, ntheta, ndist = 512, 900, 4
     g = torch.Generator(device=dev).manual_seed(8)
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    peak = float(peaks.get("hbm_gbs", 6650.0))
     rng = np.random.default_rng(8)
 
     def timed(fn, steps=None, warmup=None):
@@ -348,6 +354,9 @@ def run_rows(a):
     tomo = Tomo(n, n, theta, 0.9)
     d = torch.randn(ntheta, n, n, dtype=torch.complex64, device=dev, generator=g)
     out["fbp_ms"] = timed(lambda: tomo.fbp(d))
+    # algorithmic bytes: the sinogram read once, the volume written once
+    out["fbp_gbs"] = (ntheta + n) * n * n * 8 / (out["fbp_ms"] * 1e-3) / 1e9
+    out["fbp_frac"] = out["fbp_gbs"] / peak
     out["rec_tomo_4it_ms"] = timed(lambda: tomo.rec_tomo(d, 4), steps=2, warmup=1)
     ot = O.Tomo(n, 1, theta, 0.9, "complex64")
     ds = (rng.standard_normal((ntheta, 1, n)) + 1j * rng.standard_normal((ntheta, 1, n))).astype("complex64")
@@ -366,6 +375,9 @@ def run_rows(a):
     sp = torch.randn(nimg, n, n, dtype=torch.complex64, device=dev, generator=g)
     rs = 4 * torch.rand(nimg, 2, device=dev, generator=g) - 2
     out["sback_ms"] = timed(lambda: sh.Sback(sp, rs, 1.0))
+    # algorithmic bytes: the detector images read once, the coefficient grids written once
+    out["sback_gbs"] = nimg * 2 * n * n * 8 / (out["sback_ms"] * 1e-3) / 1e9
+    out["sback_frac"] = out["sback_gbs"] / peak
     osh = O.Shift(n, n, n, n, "complex64", dtype="complex64")
     t0 = time.perf_counter()
     osh.Sback(sp[:16].cpu().numpy(), rs[:16].cpu().numpy(), np.float32(1.0))
@@ -418,6 +430,7 @@ def run_rows(a):
     line = {"metric": "rows beside the BH hot path: device time per call (ms), oracle on the host cores beside it",
             "unit": "ms", "value": out["bh_plain_ms"], "higher_is_better": False, "steps": a.steps,
             "warmup": a.warmup, "n_gpus": 1, "dtype": "c64", "data": "synthetic (seeded)", "cpu_cores": threads,
+            "peak_gbs": peak, "peak_source": "measured" if peaks else "fallback",
             "config": {"workload": "512^3 object, 900 angles, 4 distances; RecNFP 512^2 probe, 768^2 projection, "
                                    "256 positions"},
             "rows": {k: (round(v, 4) if isinstance(v, float) else v) for k, v in out.items()}}

@@ -328,65 +328,107 @@ __device__ __forceinline__ void sback_range(int cell, int npix, int ncell, float
   *p1 = min(npix - 1, (int)ceilf(fminf(hi, (float)npix)) + 1);
 }
 
-// Candidate pixels of a cell's row taps held in registers (the x taps are the
-// same for every row of the cell); wider candidate ranges (very small
-// magnifications) take the loop that tests them per row.
+// Candidate pixels a cell line's tap table holds; wider candidate ranges
+// (very small magnifications) take the loop that tests them per pixel.
 constexpr int kSbackX = 16;
 
-__global__ void k_sback(const float2* __restrict__ g, float2* __restrict__ f, const float* __restrict__ r,
-                        const float* __restrict__ mag, int nmag, ShiftDims S, long batch) {
-  const int xx = blockIdx.x * blockDim.x + threadIdx.x;
-  const int yy = blockIdx.y * blockDim.y + threadIdx.y;
+// Tap table of one cell line: first candidate pixel, membership mask over
+// the kSbackX candidates (bit 31: the candidate range is wider, the cell
+// takes the per-pixel loop) and the weights.
+__device__ __forceinline__ unsigned sback_taps(int cell, int npix, int ncell, float shift, float m0, int* p0,
+                                               float (&w)[kSbackX]) {
+  int p1;
+  sback_range(cell, npix, ncell, shift, m0, p0, &p1);
+  unsigned mask = 0u;
+#pragma unroll
+  for (int k = 0; k < kSbackX; ++k) w[k] = 0.f;
+  if (p1 - *p0 >= kSbackX) return 1u << 31;
+#pragma unroll
+  for (int k = 0; k < kSbackX; ++k)
+    if (*p0 + k <= p1 && sback_tap(*p0 + k, npix, ncell, shift, m0, cell, &w[k])) mask |= 1u << k;
+  return mask;
+}
+
+// A CTA covers kSbackCX x kSbackCY cells of one image.  The x taps depend
+// on the cell column only and the y taps on the cell row only, so the CTA
+// forms them once -- the first warp the columns', the second the rows' --
+// in shared memory; each cell then sums its rows of taps in the fixed order.
+constexpr int kSbackCX = 32, kSbackCY = 8;
+
+__global__ void __launch_bounds__(kSbackCX * kSbackCY)
+k_sback(const float2* __restrict__ g, float2* __restrict__ f, const float* __restrict__ r,
+        const float* __restrict__ mag, int nmag, ShiftDims S, long batch) {
+  __shared__ float xw[kSbackX][kSbackCX], yw[kSbackX][kSbackCY];
+  __shared__ int xp0[kSbackCX], yp0[kSbackCY];
+  __shared__ unsigned xm[kSbackCX], ym[kSbackCY];
+  const int xx = blockIdx.x * kSbackCX + threadIdx.x;
+  const int yy = blockIdx.y * kSbackCY + threadIdx.y;
   const long b = blockIdx.z;
-  if (xx >= S.npsi || yy >= S.nzpsi || b >= batch) return;
   const float m0 = mag[nmag == 1 ? 0 : b];
+  const float ry = r[2 * b + 0], rx = r[2 * b + 1];
+  const bool tapped = m0 > 0.f;   // m <= 0: the reference's tap ranges are empty
+  if (threadIdx.y == 0) {
+    int p0 = 0;
+    float w[kSbackX];
+    const unsigned mask = (tapped && xx < S.npsi) ? sback_taps(xx, S.n, S.npsi, rx, m0, &p0, w) : 0u;
+    xp0[threadIdx.x] = p0;
+    xm[threadIdx.x] = mask;
+#pragma unroll
+    for (int k = 0; k < kSbackX; ++k) xw[k][threadIdx.x] = (mask >> 31) ? 0.f : w[k];
+  } else if (threadIdx.y == 1 && threadIdx.x < kSbackCY) {
+    const int row = blockIdx.y * kSbackCY + threadIdx.x;
+    int p0 = 0;
+    float w[kSbackX];
+    const unsigned mask = (tapped && row < S.nzpsi) ? sback_taps(row, S.nz, S.nzpsi, ry, m0, &p0, w) : 0u;
+    yp0[threadIdx.x] = p0;
+    ym[threadIdx.x] = mask;
+#pragma unroll
+    for (int k = 0; k < kSbackX; ++k) yw[k][threadIdx.x] = (mask >> 31) ? 0.f : w[k];
+  }
+  __syncthreads();
+  if (xx >= S.npsi || yy >= S.nzpsi || b >= batch) return;
   float2 acc = make_float2(0.f, 0.f);
-  if (m0 > 0.f) {   // m <= 0: the reference's tap ranges are empty
-    const float ry = r[2 * b + 0], rx = r[2 * b + 1];
+  const float2* gb = g + b * (long)S.nz * S.n;
+  const unsigned mx = xm[threadIdx.x], my = ym[threadIdx.y];
+  if (tapped && !((mx | my) >> 31)) {
+    float wx[kSbackX];
+#pragma unroll
+    for (int k = 0; k < kSbackX; ++k) wx[k] = xw[k][threadIdx.x];
+    const float2* g0 = gb + (long)yp0[threadIdx.y] * S.n + xp0[threadIdx.x];
+    for (int ky = 0; ky < kSbackX; ++ky) {
+      if (!((my >> ky) & 1u)) continue;
+      const float wy = yw[ky][threadIdx.y];
+      const float2* grow = g0 + (long)ky * S.n;
+      float2 rsum = make_float2(0.f, 0.f);
+#pragma unroll
+      for (int kx = 0; kx < kSbackX; ++kx) {
+        if (!((mx >> kx) & 1u)) continue;
+        const float2 v = __ldg(&grow[kx]);
+        rsum.x += wx[kx] * v.x;
+        rsum.y += wx[kx] * v.y;
+      }
+      acc.x += wy * rsum.x;
+      acc.y += wy * rsum.y;
+    }
+  } else if (tapped) {
+    // a candidate range wider than the tables (very small magnifications)
     int tx0, tx1, ty0, ty1;
     sback_range(xx, S.n, S.npsi, rx, m0, &tx0, &tx1);
     sback_range(yy, S.nz, S.nzpsi, ry, m0, &ty0, &ty1);
-    const float2* gb = g + b * (long)S.nz * S.n;
-    if (tx1 - tx0 < kSbackX) {
-      // the x taps once per cell: weights and a membership mask over tx0 + k
-      float wxs[kSbackX];
-      unsigned mx = 0u;
-#pragma unroll
-      for (int k = 0; k < kSbackX; ++k) {
-        wxs[k] = 0.f;
-        if (tx0 + k <= tx1 && sback_tap(tx0 + k, S.n, S.npsi, rx, m0, xx, &wxs[k])) mx |= 1u << k;
+    for (int ty = ty0; ty <= ty1; ++ty) {
+      float wy;
+      if (!sback_tap(ty, S.nz, S.nzpsi, ry, m0, yy, &wy)) continue;
+      const float2* grow = gb + (long)ty * S.n;
+      float2 rsum = make_float2(0.f, 0.f);
+      for (int tx = tx0; tx <= tx1; ++tx) {
+        float wx;
+        if (!sback_tap(tx, S.n, S.npsi, rx, m0, xx, &wx)) continue;
+        const float2 v = __ldg(&grow[tx]);
+        rsum.x += wx * v.x;
+        rsum.y += wx * v.y;
       }
-      for (int ty = ty0; ty <= ty1; ++ty) {
-        float wy;
-        if (!sback_tap(ty, S.nz, S.nzpsi, ry, m0, yy, &wy)) continue;
-        const float2* grow = gb + (long)ty * S.n + tx0;
-        float2 row = make_float2(0.f, 0.f);
-#pragma unroll
-        for (int k = 0; k < kSbackX; ++k) {
-          if (!((mx >> k) & 1u)) continue;
-          const float2 v = __ldg(&grow[k]);
-          row.x += wxs[k] * v.x;
-          row.y += wxs[k] * v.y;
-        }
-        acc.x += wy * row.x;
-        acc.y += wy * row.y;
-      }
-    } else {
-      for (int ty = ty0; ty <= ty1; ++ty) {
-        float wy;
-        if (!sback_tap(ty, S.nz, S.nzpsi, ry, m0, yy, &wy)) continue;
-        const float2* grow = gb + (long)ty * S.n;
-        float2 row = make_float2(0.f, 0.f);
-        for (int tx = tx0; tx <= tx1; ++tx) {
-          float wx;
-          if (!sback_tap(tx, S.n, S.npsi, rx, m0, xx, &wx)) continue;
-          const float2 v = __ldg(&grow[tx]);
-          row.x += wx * v.x;
-          row.y += wx * v.y;
-        }
-        acc.x += wy * row.x;
-        acc.y += wy * row.y;
-      }
+      acc.x += wy * rsum.x;
+      acc.y += wy * rsum.y;
     }
   }
   f[(b * S.nzpsi + yy) * (long)S.npsi + xx] = acc;
@@ -600,7 +642,8 @@ extern "C" int ht_shift_Sback(ht_shift_s* s, const void* g, const float* r, cons
   HT_REQUIRE(batch >= 0 && batch <= 65535, "ht_shift_Sback: batch must be in [0, 65535]");
   if (batch == 0) return kOk;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  k_sback<<<coef_grid(s, batch), kBlock, 0, st>>>(static_cast<const float2*>(g), static_cast<float2*>(out), r, mag,
+  const dim3 sgrid((s->npsi + kSbackCX - 1) / kSbackCX, (s->nzpsi + kSbackCY - 1) / kSbackCY, (unsigned)batch);
+  k_sback<<<sgrid, dim3(kSbackCX, kSbackCY), 0, st>>>(static_cast<const float2*>(g), static_cast<float2*>(out), r, mag,
                                                   nmag, dims(s), batch);
   count_launch();
   HT_CHECK_CUDA(cudaGetLastError());
