@@ -10,6 +10,8 @@
 //   k_lap_apply: (B u)(z) = lap[z] + lap[z + 2] + in-plane neighbours of lap[z + 1] - 6 lap[z + 1],
 //                then g += s * B u, or out += s * Re<y, B u> in double precision.
 // The sums keep the reference's order a + c + b[y+1] + b[y-1] + b[x+1] + b[x-1] - 6 b.
+#include <algorithm>
+
 #include "common.cuh"
 #include "holotomo_b200_internal.h"
 
@@ -45,20 +47,25 @@ __device__ __forceinline__ T lap7(T a, T c, T byp, T bym, T bxp, T bxm, T b) {
   return RE<T>::sub(v, RE<T>::scale(b, 6.f));
 }
 
+// The kernels walk rows (z, y) of the volume, the threads of a CTA across x,
+// so a row's indices are formed once per row rather than divided out of a
+// flat index per element.
 template <class T>
 __global__ void __launch_bounds__(256) k_lap_ext(const T* __restrict__ u, T* __restrict__ lap, int nz, int ny, int nx) {
-  const long plane = (long)ny * nx;
-  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= (long)(nz + 2) * plane) return;
-  const int ze = (int)(i / plane);
-  const int y = (int)((i % plane) / nx), x = (int)(i % nx);
-  const int z = ze - 1;
-  auto U = [&](int zz, int yy, int xx) -> T {
-    return (zz < 0 || zz >= nz) ? RE<T>::zero() : __ldg(&u[((long)zz * ny + yy) * nx + xx]);
-  };
-  const int yp = (y + 1 == ny) ? 0 : y + 1, ym = (y == 0) ? ny - 1 : y - 1;
-  const int xp = (x + 1 == nx) ? 0 : x + 1, xm = (x == 0) ? nx - 1 : x - 1;
-  lap[i] = lap7(U(z - 1, y, x), U(z + 1, y, x), U(z, yp, x), U(z, ym, x), U(z, y, xp), U(z, y, xm), U(z, y, x));
+  const int nrows = (nz + 2) * ny;
+  for (int r = blockIdx.x; r < nrows; r += gridDim.x) {
+    const int ze = r / ny, y = r - ze * ny;
+    const int z = ze - 1;
+    const int yp = (y + 1 == ny) ? 0 : y + 1, ym = (y == 0) ? ny - 1 : y - 1;
+    auto U = [&](int zz, int yy, int xx) -> T {
+      return (zz < 0 || zz >= nz) ? RE<T>::zero() : __ldg(&u[((long)zz * ny + yy) * nx + xx]);
+    };
+    T* out = lap + (long)r * nx;
+    for (int x = threadIdx.x; x < nx; x += blockDim.x) {
+      const int xp = (x + 1 == nx) ? 0 : x + 1, xm = (x == 0) ? nx - 1 : x - 1;
+      out[x] = lap7(U(z - 1, y, x), U(z + 1, y, x), U(z, yp, x), U(z, ym, x), U(z, y, xp), U(z, y, xm), U(z, y, x));
+    }
+  }
 }
 
 constexpr int kRegThreads = 256;
@@ -68,22 +75,26 @@ __global__ void __launch_bounds__(kRegThreads)
 k_lap_apply(const T* __restrict__ lap, int nz, int ny, int nx, float s, T* __restrict__ g, const T* __restrict__ yv,
             double* __restrict__ out, const T* __restrict__ yv2, double* __restrict__ out2, double sd) {
   const long plane = (long)ny * nx;
-  const long n = (long)nz * plane;
+  const int nrows = nz * ny;
   double acc = 0.0, acc2 = 0.0;
-  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
-    const int z = (int)(i / plane);
-    const int y = (int)((i % plane) / nx), x = (int)(i % nx);
+  for (int r = blockIdx.x; r < nrows; r += gridDim.x) {
+    const int z = r / ny, y = r - z * ny;
     const int yp = (y + 1 == ny) ? 0 : y + 1, ym = (y == 0) ? ny - 1 : y - 1;
-    const int xp = (x + 1 == nx) ? 0 : x + 1, xm = (x == 0) ? nx - 1 : x - 1;
     const T* b = lap + (long)(z + 1) * plane;
-    const T v = lap7(__ldg(&lap[(long)z * plane + (long)y * nx + x]), __ldg(&lap[(long)(z + 2) * plane + (long)y * nx + x]),
-                     __ldg(&b[(long)yp * nx + x]), __ldg(&b[(long)ym * nx + x]), __ldg(&b[(long)y * nx + xp]),
-                     __ldg(&b[(long)y * nx + xm]), __ldg(&b[(long)y * nx + x]));
-    if (MODE == 0) {
-      g[i] = RE<T>::add(g[i], RE<T>::scale(v, s));
-    } else {
-      acc += RE<T>::redot(__ldg(&yv[i]), v);
-      if (yv2) acc2 += RE<T>::redot(__ldg(&yv2[i]), v);
+    const long row = (long)r * nx;
+    for (int x = threadIdx.x; x < nx; x += blockDim.x) {
+      const int xp = (x + 1 == nx) ? 0 : x + 1, xm = (x == 0) ? nx - 1 : x - 1;
+      const long i = row + x;
+      const T v = lap7(__ldg(&lap[(long)z * plane + (long)y * nx + x]),
+                       __ldg(&lap[(long)(z + 2) * plane + (long)y * nx + x]), __ldg(&b[(long)yp * nx + x]),
+                       __ldg(&b[(long)ym * nx + x]), __ldg(&b[(long)y * nx + xp]), __ldg(&b[(long)y * nx + xm]),
+                       __ldg(&b[(long)y * nx + x]));
+      if (MODE == 0) {
+        g[i] = RE<T>::add(g[i], RE<T>::scale(v, s));
+      } else {
+        acc += RE<T>::redot(__ldg(&yv[i]), v);
+        if (yv2) acc2 += RE<T>::redot(__ldg(&yv2[i]), v);
+      }
     }
   }
   if (MODE == 1) {
@@ -131,6 +142,12 @@ k_lap_energy(const T* __restrict__ lap, long n, double* __restrict__ out, double
   }
 }
 
+// k_lap_apply's grid: CTAs over the rows (z, y) of the volume
+static unsigned reg_grid_rows(int nz, int ny) {
+  const long rows = (long)nz * ny;
+  return (unsigned)std::max<long>(1, std::min<long>(rows, 148L * 16));
+}
+
 static unsigned reg_grid(long n) {
   long g = (n + kRegThreads - 1) / kRegThreads;
   if (g > 148L * 16) g = 148L * 16;
@@ -139,9 +156,9 @@ static unsigned reg_grid(long n) {
 
 template <class T>
 static cudaError_t lap_ext(const void* u, void* work, int nz, int ny, int nx, cudaStream_t st) {
-  const long n = (long)(nz + 2) * ny * nx;
-  k_lap_ext<T><<<(unsigned)((n + 255) / 256), 256, 0, st>>>(static_cast<const T*>(u), static_cast<T*>(work), nz, ny,
-                                                            nx);
+  const long rows = (long)(nz + 2) * ny;
+  k_lap_ext<T><<<(unsigned)std::min<long>(rows, 148L * 32), 256, 0, st>>>(static_cast<const T*>(u),
+                                                                          static_cast<T*>(work), nz, ny, nx);
   count_launch();
   return cudaGetLastError();
 }
@@ -158,15 +175,15 @@ extern "C" int ht_laplacian_grad(const void* u, void* g, int nz, int ny, int nx,
   HT_REQUIRE(u && g, "ht_laplacian_grad: null pointer");
   HT_REG_CHECK("ht_laplacian_grad");
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  const long n = (long)nz * ny * nx;
+  const unsigned rows = reg_grid_rows(nz, ny);
   if (is_complex) {
     HT_CHECK_CUDA(lap_ext<float2>(u, work, nz, ny, nx, st));
-    k_lap_apply<float2, 0><<<reg_grid(n), kRegThreads, 0, st>>>(static_cast<const float2*>(work), nz, ny, nx, scale,
+    k_lap_apply<float2, 0><<<rows, kRegThreads, 0, st>>>(static_cast<const float2*>(work), nz, ny, nx, scale,
                                                                 static_cast<float2*>(g), nullptr, nullptr, nullptr,
                                                                 nullptr, 0.0);
   } else {
     HT_CHECK_CUDA(lap_ext<float>(u, work, nz, ny, nx, st));
-    k_lap_apply<float, 0><<<reg_grid(n), kRegThreads, 0, st>>>(static_cast<const float*>(work), nz, ny, nx, scale,
+    k_lap_apply<float, 0><<<rows, kRegThreads, 0, st>>>(static_cast<const float*>(work), nz, ny, nx, scale,
                                                                static_cast<float*>(g), nullptr, nullptr, nullptr,
                                                                nullptr, 0.0);
   }
@@ -182,15 +199,15 @@ extern "C" int ht_laplacian_dot(const void* y, const void* z, int nz, int ny, in
   HT_REQUIRE(!y2 || out2, "ht_laplacian_dot: y2 needs out2");
   HT_REG_CHECK("ht_laplacian_dot");
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  const long n = (long)nz * ny * nx;
+  const unsigned rows = reg_grid_rows(nz, ny);
   if (is_complex) {
     HT_CHECK_CUDA(lap_ext<float2>(z, work, nz, ny, nx, st));
-    k_lap_apply<float2, 1><<<reg_grid(n), kRegThreads, 0, st>>>(static_cast<const float2*>(work), nz, ny, nx, 0.f,
+    k_lap_apply<float2, 1><<<rows, kRegThreads, 0, st>>>(static_cast<const float2*>(work), nz, ny, nx, 0.f,
                                                                 nullptr, static_cast<const float2*>(y), out,
                                                                 static_cast<const float2*>(y2), out2, scale);
   } else {
     HT_CHECK_CUDA(lap_ext<float>(z, work, nz, ny, nx, st));
-    k_lap_apply<float, 1><<<reg_grid(n), kRegThreads, 0, st>>>(static_cast<const float*>(work), nz, ny, nx, 0.f,
+    k_lap_apply<float, 1><<<rows, kRegThreads, 0, st>>>(static_cast<const float*>(work), nz, ny, nx, 0.f,
                                                                nullptr, static_cast<const float*>(y), out,
                                                                static_cast<const float*>(y2), out2, scale);
   }
