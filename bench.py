@@ -596,9 +596,10 @@ def main():
     # ---- end to end through the public API with pinned host buffers
     e2e = None if a.profile else end_to_end(a, rec, obj_true, prb0, pos0, data, device, barrier, world)
 
-    # ---- mixed served stream vs the same requests one at a time
+    # ---- mixed served stream vs the same requests one at a time (one GPU: the
+    # stream's pinned requests and results take ~60 GB of host memory a process)
     served = None
-    if a.serve_requests > 0 and not a.profile:
+    if a.serve_requests > 0 and not a.profile and world == 1:
         del rec, data, obj_true, prb_true, pos_true
         gc.collect()   # the reconstruction's device handles go with it (cudaMalloc'd outside torch's cache)
         torch.cuda.synchronize()
