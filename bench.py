@@ -278,7 +278,8 @@ def run_rows(a):
         sinogram (tomo.py:163-210); oracle: one slice;
       * Shift.Sback of 3600 images of 512^2 (shift.py:138-148); oracle: 16 images;
       * RecNFP (rec_nfp_mpi.py:100-144), a 512^2 probe, a 768^2 projection and
-        256 scan positions: BH iterations (host step sizes, as the reference);
+        256 scan positions: BH iterations, host step sizes (as the reference) and
+        graph-replayed with device step sizes;
       * a checkpoint of the 512^3 x 900 x 4 state written and read back
         (writer.py:57-110, reader.py:260-340; the .npz layout, h5py being
         absent on the box)."""
@@ -399,14 +400,15 @@ def run_rows(a):
             v.zero_()
     rn.vars["prb"].fill_(1)
     rn.vars["pos"].copy_(pos_t + 0.3 * (2 * torch.rand(256, 2, device=dev, generator=g) - 1))
-    rn.BH(niter=2)   # warm-up
-    torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record()
-    rn.BH(niter=8)   # a solve of 8 iterations from the warm-up's state
-    e1.record()
-    torch.cuda.synchronize()
-    out["nfp_bh_iteration_ms"] = e0.elapsed_time(e1) / 8
+    for mode in ("host", "graph"):
+        rn.BH(niter=2, mode=mode)   # warm-up
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        rn.BH(niter=8, mode=mode)   # a solve of 8 iterations from the warm-up's state
+        e1.record()
+        torch.cuda.synchronize()
+        out["nfp_bh_iteration_ms" if mode == "host" else "nfp_bh_iteration_graph_ms"] = e0.elapsed_time(e1) / 8
     rn.close()
     del rn
     torch.cuda.empty_cache()

@@ -23,6 +23,7 @@ The operator-by-operator ``F*`` / ``dF*`` / ``d2F_dF*`` / ``gF*`` functions are
 not kept (the fused passes replace them; ``Rec`` has them for the 3-D case).
 """
 import ctypes
+import gc
 import time
 
 import numpy as np
@@ -85,8 +86,17 @@ class RecNFP:
         self._dots = torch.zeros(4, dtype=torch.float64, device=dev)
         self._bh = torch.zeros(2, dtype=torch.float64, device=dev)
         self._scratch = (z(self.ntheta, 2, dt=torch.float32), z(self.nz, self.n, dt=torch.complex64))
+        # the device-side step-size history of the graph-replayed iterations
+        self._hist_cap = 4096
+        self._hist = z(self._hist_cap, 2, dt=torch.float64)
+        self._count = z(1, dt=torch.int32)
+        self._graph = None
 
     def close(self):
+        try:
+            self.release_graph()
+        except Exception:
+            pass
         h = getattr(self, "_h", None)
         if h is not None and h.value:
             try:
@@ -179,32 +189,37 @@ class RecNFP:
         _lib.call("ht_axpby", _lib.ptr(x), _lib.ptr(y), float(a), float(b), n,
                   _lib.ptr(dot) if dot is not None else None, _lib.stream_ptr())
 
-    def BH(self, writer=None, niter=None, record=None):
-        """rec_nfp_mpi.py:100-144, with the Hessian forms of one fused pass: H(g,e)
-        and H(e,e) give beta, and the bottom of alpha follows from them and
-        H(g,g) by bilinearity (beta^2 H(e,e) - 2 beta H_sym(g,e) + H(g,g)), which
-        is H(eta, eta) of the updated direction.  ``record`` receives
-        (iteration, alpha, beta)."""
+    def _axpby_dev(self, x, y, A, sa, B, sb, dot=None):
+        n = x.numel() * (2 if x.is_complex() else 1)
+        _lib.call("ht_axpby_dev", _lib.ptr(x), _lib.ptr(y), A, float(sa), B, float(sb), n,
+                  _lib.ptr(dot) if dot is not None else None, _lib.stream_ptr())
+
+    def bh_iteration(self, i, sync=True):
+        """One BH iteration (rec_nfp_mpi.py:100-144), with the Hessian forms of
+        one fused pass: H(g,e) and H(e,e) give beta, and the bottom of alpha
+        follows from them and H(g,g) by bilinearity (beta^2 H(e,e) - 2 beta
+        H_sym(g,e) + H(g,g)), which is H(eta, eta) of the updated direction.
+        Returns (alpha, beta).  sync=False keeps alpha and beta on the device
+        (ht_bh_scalars, ht_axpby_dev: the same formulas), so the iteration
+        makes no host round trip and can be recorded into a CUDA graph; the
+        step sizes then go to the device history (bh_history())."""
         vars, grads, etas, C = self.vars, self.grads, self.etas, self._c
         rho = self.rho_sq
-        niter = self.niter if niter is None else niter
-        self.time_start = time.time()
-        self.error_debug(vars, -1)
-        for i in range(self.start_iter, niter):
-            first = i == self.start_iter
-            self._coeff(vars["proj"], C["vars"])
-            # gradients, scaled (rec_nfp_mpi.py:106-109)
-            self._gradient_pass(C["vars"], vars["pos"], vars["prb"], grads["pos"], grads["prb"], rho["pos"],
-                                rho["prb"])
-            self._coeff(self._gc, grads["proj"])
-            if rho["proj"] != 1:
-                grads["proj"] *= rho["proj"]
-            self._coeff(grads["proj"], C["grads"])
-            y = (C["grads"], grads["pos"], grads["prb"])
-            z = None if first else (C["etas"], etas["pos"], etas["prb"])
-            H = self._hessian_pass(C["vars"], vars["pos"], vars["prb"], y, z).cpu().numpy()
+        first = i == self.start_iter
+        self._coeff(vars["proj"], C["vars"])
+        # gradients, scaled (rec_nfp_mpi.py:106-109)
+        self._gradient_pass(C["vars"], vars["pos"], vars["prb"], grads["pos"], grads["prb"], rho["pos"], rho["prb"])
+        self._coeff(self._gc, grads["proj"])
+        if rho["proj"] != 1:
+            grads["proj"] *= rho["proj"]
+        self._coeff(grads["proj"], C["grads"])
+        y = (C["grads"], grads["pos"], grads["prb"])
+        z = None if first else (C["etas"], etas["pos"], etas["prb"])
+        H = self._hessian_pass(C["vars"], vars["pos"], vars["prb"], y, z)
+        dots = self._dots
+        if sync:
+            H = H.cpu().numpy()
             beta = 0.0 if first else H[1] / H[2]
-            dots = self._dots
             dots.zero_()
             for k, v in enumerate(("proj", "pos", "prb")):
                 self._axpby(etas[v], grads[v], beta, -1.0, dots[k:k + 1])
@@ -215,7 +230,87 @@ class RecNFP:
             alpha = top / bottom
             for v in ("prb", "proj", "pos"):
                 self._axpby(vars[v], etas[v], 1.0, alpha)
+            return float(alpha), float(beta)
+        st = _lib.stream_ptr()
+        bh = self._bh
+        rr = (float(rho["proj"]), float(rho["pos"]), float(rho["prb"]))
+        # phase 0: beta, and the dots cleared for the direction updates below
+        _lib.call("ht_bh_scalars", _lib.ptr(H), _lib.ptr(dots), int(first), 0, *rr, _lib.ptr(bh), None, 0, None, st)
+        beta = _lib.ptr(bh)
+        for k, v in enumerate(("proj", "pos", "prb")):
+            self._axpby_dev(etas[v], grads[v], beta, 1.0, None, -1.0, dots[k:k + 1])
+        self._axpby_dev(C["etas"], C["grads"], beta, 1.0, None, -1.0)
+        _lib.call("ht_bh_scalars", _lib.ptr(H), _lib.ptr(dots), int(first), 1, *rr, _lib.ptr(bh),
+                  _lib.ptr(self._hist), self._hist_cap, _lib.ptr(self._count), st)
+        alpha = ctypes.c_void_p(bh.data_ptr() + 8)
+        for v in ("prb", "proj", "pos"):
+            self._axpby_dev(vars[v], etas[v], None, 1.0, alpha, 1.0)
+        return None
+
+    def capture_iteration(self):
+        """Record one steady-state device-scalar iteration (not the first) on
+        the current stream into a CUDA graph; replay_iteration() then runs it
+        with one launch.  Call after one iteration has run on this device.
+        Recording runs nothing."""
+        self.release_graph()
+        st = _lib.stream_ptr()
+        gc_on = gc.isenabled()
+        gc.disable()   # no collector-driven destructors (device frees) while recording
+        _lib.call("ht_graph_begin", st)
+        try:
+            self.bh_iteration(self.start_iter + 1, sync=False)
+        finally:
+            ex = ctypes.c_void_p()
+            _lib.call("ht_graph_end", st, ctypes.byref(ex))
+            if gc_on:
+                gc.enable()
+        self._graph = ex
+        return ex
+
+    def replay_iteration(self):
+        """Run the recorded iteration on the current stream."""
+        _lib.call("ht_graph_launch", self._graph, _lib.stream_ptr())
+
+    def release_graph(self):
+        if getattr(self, "_graph", None) is not None:
+            _lib.lib().ht_graph_destroy(self._graph)
+            self._graph = None
+
+    def bh_history(self):
+        """(alpha, beta) of the device-scalar iterations since BH started."""
+        n = min(int(self._count.item()), self._hist_cap)
+        return [tuple(r) for r in self._hist[:n].cpu().numpy()]
+
+    def BH(self, writer=None, niter=None, record=None, mode="host"):
+        """rec_nfp_mpi.py:100-144.  ``record`` (a list) receives (iteration,
+        alpha, beta).  mode="host" iterates as the reference does (step sizes
+        on the host); mode="graph" keeps them on the device and replays the
+        steady-state iteration from a CUDA graph (same arithmetic; complex
+        projections, no error table -- otherwise it iterates as "host")."""
+        vars = self.vars
+        niter = self.niter if niter is None else niter
+        self.time_start = time.time()
+        self.error_debug(vars, -1)
+        self._count.zero_()
+        if mode == "graph" and self.complex_obj and self.err_step == -1 and niter > self.start_iter:
+            cur = torch.cuda.current_stream(self.device)
+            side = torch.cuda.Stream(device=self.device)
+            side.wait_stream(cur)
+            with torch.cuda.stream(side):
+                self.bh_iteration(self.start_iter, sync=False)
+                if niter - self.start_iter > 1:
+                    self.capture_iteration()
+                    for _ in range(self.start_iter + 1, niter):
+                        self.replay_iteration()
+                    self.release_graph()
+            cur.wait_stream(side)
             if record is not None:
-                record.append((i, float(alpha), float(beta)))
+                for k, (a, b) in enumerate(self.bh_history()):
+                    record.append((self.start_iter + k, float(a), float(b)))
+            return vars
+        for i in range(self.start_iter, niter):
+            alpha, beta = self.bh_iteration(i)
+            if record is not None:
+                record.append((i, alpha, beta))
             self.error_debug(vars, i)
         return vars

@@ -68,3 +68,32 @@ def test_nfp_bh_matches_reference(golden, tag, dt):
             assert abs(b / rb - 1) < 1e-4, (i, b, rb)
     for k in ("prb", "proj", "pos"):
         assert rel_l2(rec.vars[k].cpu().numpy(), g[f"{tag}_bh_{k}"]) < TOL, k
+
+
+def test_nfp_graph_iteration_matches_host(golden):
+    """BH(mode="graph"): step sizes on the device (ht_bh_scalars, ht_axpby_dev)
+    and the steady-state iteration replayed from a CUDA graph give the step
+    sizes (rtol 1e-9) and the state (rel L2 1e-6) of the host-scalar BH."""
+    from holotomocupy_b200 import RecNFP
+    g = golden("nfp")
+    tag, dt = "c", "complex64"
+    n, nobj, ntheta, niter = [int(v) for v in g[f"{tag}_dims"]]
+    out = []
+    st = torch.cuda.Stream()
+    for mode in ("host", "graph"):
+        with torch.cuda.stream(st):
+            rec = RecNFP(nfp_args(n, nobj, ntheta, dt, niter))
+            rec.data[:] = cuda(g[f"{tag}_data"])
+            rec.vars["prb"][:] = 1
+            rec.vars["proj"][:] = 0
+            rec.vars["pos"][:] = cuda(g[f"{tag}_pos_true"] + g[f"{tag}_pos_err"])
+            record = []
+            rec.BH(record=record, mode=mode)
+            out.append((np.array([(a, b) for _, a, b in record]),
+                        {k: rec.vars[k].cpu().numpy() for k in ("prb", "proj", "pos")}))
+            rec.close()
+    (h0, v0), (h1, v1) = out
+    assert h1.shape == (niter, 2)
+    np.testing.assert_allclose(h1, h0, rtol=1e-9)
+    for k in v0:
+        assert rel_l2(v1[k], v0[k]) < 1e-6, k
