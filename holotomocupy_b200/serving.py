@@ -110,15 +110,15 @@ class _Inline:
 
 
 class _Slot:
-    def __init__(self, req, stream):
+    def __init__(self, req, stream, key, nbytes):
         self.req = req
         self.stream = stream
         self.rec = None
         self.it = 0              # iterations launched
         self.inflight = deque()  # (start, end) event pairs of the queued iterations, oldest first
-        self.bytes = estimate_bytes(req.args)
+        self.bytes = nbytes      # estimate_bytes(req.args)
         self.job = None          # the host worker's admission or retirement of this request
-        self.key = args_key(req.args)
+        self.key = key           # args_key(req.args)
         self.reused = None       # a retired request's (rec, bytes, key) this one takes over
         self.state = "admitting"  # -> "running" -> "retiring"
 
@@ -265,6 +265,9 @@ class Server:
         their arrival times."""
         pending = sorted(self.queue, key=lambda q: q.arrival)
         self.queue = []
+        # each request's argument key and memory estimate, formed once (the
+        # admission test below runs on every pass of the loop)
+        meta = {id(q): (args_key(q.args), estimate_bytes(q.args)) for q in pending}
         active = []
         self.used_bytes = 0
         self._retired = []
@@ -281,7 +284,7 @@ class Server:
                 now = time.perf_counter() - t0
                 while (pending and not wait_retire and len(active) < self.max_active
                        and (not realtime or pending[0].arrival <= now)):
-                    slot = _Slot(pending[0], self._streams[-1])
+                    slot = _Slot(pending[0], self._streams[-1], *meta[id(pending[0])])
                     with self._ret_lock:
                         snap = list(self._retired)
                     reuse = next((e for e in snap if e[2] == slot.key), None) if self.reuse else None
