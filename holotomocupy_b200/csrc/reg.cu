@@ -8,7 +8,8 @@
 // energy uses the inner L on the object slices only (rec_mpi.py:486-493).
 //   k_lap_ext:   lap[ze] = (L u~)(ze - 1), ze in [0, nz + 2)   (u~: zero outside [0, nz))
 //   k_lap_apply: (B u)(z) = lap[z] + lap[z + 2] + in-plane neighbours of lap[z + 1] - 6 lap[z + 1],
-//                then g += s * B u, or out += s * Re<y, B u> in double precision.
+//                then g += s * B u, or the per-block double-precision partials of Re<y, B u>,
+//                which k_lap_finish adds in block order (the sums repeat bit for bit).
 // The sums keep the reference's order a + c + b[y+1] + b[y-1] + b[x+1] + b[x-1] - 6 b.
 #include <algorithm>
 
@@ -73,7 +74,7 @@ constexpr int kRegThreads = 256;
 template <class T, int MODE>
 __global__ void __launch_bounds__(kRegThreads)
 k_lap_apply(const T* __restrict__ lap, int nz, int ny, int nx, float s, T* __restrict__ g, const T* __restrict__ yv,
-            double* __restrict__ out, const T* __restrict__ yv2, double* __restrict__ out2, double sd) {
+            double* __restrict__ out, const T* __restrict__ yv2) {
   const long plane = (long)ny * nx;
   const int nrows = nz * ny;
   double acc = 0.0, acc2 = 0.0;
@@ -115,16 +116,16 @@ k_lap_apply(const T* __restrict__ lap, int nz, int ny, int nx, float s, T* __res
         t += red[0][w];
         t2 += red[1][w];
       }
-      atomicAdd(out, sd * t);
-      if (yv2) atomicAdd(out2, sd * t2);
+      out[2 * blockIdx.x] = t;   // out: the per-block partials (k_lap_finish adds them)
+      out[2 * blockIdx.x + 1] = t2;
     }
   }
 }
 
-// out += sd * sum over the object slices of |lap|^2
+// the per-block partials (out[2 b]) of the sum over the object slices of |lap|^2
 template <class T>
 __global__ void __launch_bounds__(kRegThreads)
-k_lap_energy(const T* __restrict__ lap, long n, double* __restrict__ out, double sd) {
+k_lap_energy(const T* __restrict__ lap, long n, double* __restrict__ out) {
   double acc = 0.0;
   for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
     const T v = __ldg(&lap[i]);
@@ -138,8 +139,38 @@ k_lap_energy(const T* __restrict__ lap, long n, double* __restrict__ out, double
   if (threadIdx.x == 0) {
     double t = 0.0;
     for (int w = 0; w < kRegThreads / 32; ++w) t += red[w];
-    atomicAdd(out, sd * t);
+    out[2 * blockIdx.x] = t;   // out: the per-block partials (k_lap_finish adds them)
   }
+}
+
+// *out += sd * (the partials part[2 b] summed), and the same for out2 with
+// part[2 b + 1], by one warp: lane l sums blocks l, l + 32, ... and the lanes
+// combine in a fixed shuffle tree, so the sums repeat bit for bit
+__global__ void k_lap_finish(const double* __restrict__ part, int nblk, double sd, double* __restrict__ out,
+                             double* __restrict__ out2) {
+  double t = 0.0, t2 = 0.0;
+  for (int b = threadIdx.x; b < nblk; b += 32) {
+    t += part[2 * b];
+    if (out2) t2 += part[2 * b + 1];
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    t += __shfl_down_sync(0xffffffffu, t, o);
+    t2 += __shfl_down_sync(0xffffffffu, t2, o);
+  }
+  if (threadIdx.x == 0) {
+    *out += sd * t;
+    if (out2) *out2 += sd * t2;
+  }
+}
+
+// Per-block partial sums of the forms and the energy sit after the extended
+// Laplacian in the workspace, at the next 16-byte boundary (at most
+// 148 * 16 blocks, two doubles each).
+constexpr long kLapPartBytes = 64 * 1024;
+static double* lap_partials(void* work, int nz, int ny, int nx, int is_complex) {
+  const long off = ((long)(nz + 2) * ny * nx * (is_complex ? 8 : 4) + 15) / 16 * 16;
+  return reinterpret_cast<double*>(static_cast<char*>(work) + off);
 }
 
 // k_lap_apply's grid: CTAs over the rows (z, y) of the volume
@@ -179,13 +210,11 @@ extern "C" int ht_laplacian_grad(const void* u, void* g, int nz, int ny, int nx,
   if (is_complex) {
     HT_CHECK_CUDA(lap_ext<float2>(u, work, nz, ny, nx, st));
     k_lap_apply<float2, 0><<<rows, kRegThreads, 0, st>>>(static_cast<const float2*>(work), nz, ny, nx, scale,
-                                                                static_cast<float2*>(g), nullptr, nullptr, nullptr,
-                                                                nullptr, 0.0);
+                                                         static_cast<float2*>(g), nullptr, nullptr, nullptr);
   } else {
     HT_CHECK_CUDA(lap_ext<float>(u, work, nz, ny, nx, st));
     k_lap_apply<float, 0><<<rows, kRegThreads, 0, st>>>(static_cast<const float*>(work), nz, ny, nx, scale,
-                                                               static_cast<float*>(g), nullptr, nullptr, nullptr,
-                                                               nullptr, 0.0);
+                                                        static_cast<float*>(g), nullptr, nullptr, nullptr);
   }
   count_launch();
   HT_CHECK_CUDA(cudaGetLastError());
@@ -200,17 +229,20 @@ extern "C" int ht_laplacian_dot(const void* y, const void* z, int nz, int ny, in
   HT_REG_CHECK("ht_laplacian_dot");
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   const unsigned rows = reg_grid_rows(nz, ny);
+  double* part = lap_partials(work, nz, ny, nx, is_complex);
   if (is_complex) {
     HT_CHECK_CUDA(lap_ext<float2>(z, work, nz, ny, nx, st));
     k_lap_apply<float2, 1><<<rows, kRegThreads, 0, st>>>(static_cast<const float2*>(work), nz, ny, nx, 0.f,
-                                                                nullptr, static_cast<const float2*>(y), out,
-                                                                static_cast<const float2*>(y2), out2, scale);
+                                                         nullptr, static_cast<const float2*>(y), part,
+                                                         static_cast<const float2*>(y2));
   } else {
     HT_CHECK_CUDA(lap_ext<float>(z, work, nz, ny, nx, st));
     k_lap_apply<float, 1><<<rows, kRegThreads, 0, st>>>(static_cast<const float*>(work), nz, ny, nx, 0.f,
-                                                               nullptr, static_cast<const float*>(y), out,
-                                                               static_cast<const float*>(y2), out2, scale);
+                                                        nullptr, static_cast<const float*>(y), part,
+                                                        static_cast<const float*>(y2));
   }
+  count_launch();
+  k_lap_finish<<<1, 32, 0, st>>>(part, (int)rows, scale, out, y2 ? out2 : nullptr);
   count_launch();
   HT_CHECK_CUDA(cudaGetLastError());
   return kOk;
@@ -223,13 +255,17 @@ extern "C" int ht_laplacian_energy(const void* u, int nz, int ny, int nx, int is
   HT_REG_CHECK("ht_laplacian_energy");
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   const long plane = (long)ny * nx, n = (long)nz * plane;
+  const unsigned nb = reg_grid(n);
+  double* part = lap_partials(work, nz, ny, nx, is_complex);
   if (is_complex) {
     HT_CHECK_CUDA(lap_ext<float2>(u, work, nz, ny, nx, st));
-    k_lap_energy<float2><<<reg_grid(n), kRegThreads, 0, st>>>(static_cast<const float2*>(work) + plane, n, out, scale);
+    k_lap_energy<float2><<<nb, kRegThreads, 0, st>>>(static_cast<const float2*>(work) + plane, n, part);
   } else {
     HT_CHECK_CUDA(lap_ext<float>(u, work, nz, ny, nx, st));
-    k_lap_energy<float><<<reg_grid(n), kRegThreads, 0, st>>>(static_cast<const float*>(work) + plane, n, out, scale);
+    k_lap_energy<float><<<nb, kRegThreads, 0, st>>>(static_cast<const float*>(work) + plane, n, part);
   }
+  count_launch();
+  k_lap_finish<<<1, 32, 0, st>>>(part, (int)nb, scale, out, nullptr);
   count_launch();
   HT_CHECK_CUDA(cudaGetLastError());
   return kOk;

@@ -214,8 +214,10 @@ class Rec:
         # objects); vars/grads/etas "proj" are recomputed by bh_finish()
         self._fold = self.complex_obj
         self._vol = z(self.nzobj, self.nobj, self.nobj) if self._fold else None
-        # Laplacian regulariser workspace (the inner Laplacian on nzobj + 2 slices)
-        self._lapw = z(self.nzobj + 2, self.nobj, self.nobj) if self.lam_laplacian != 0 else None
+        # Laplacian regulariser workspace: the inner Laplacian on nzobj + 2 slices, then
+        # 64 KiB of per-block partial sums from the next 16-byte boundary
+        lap_bytes = -(-(self.nzobj + 2) * self.nobj * self.nobj * (8 if self.complex_obj else 4) // 16) * 16
+        self._lapw = z(lap_bytes + 64 * 1024, dt=torch.uint8) if self.lam_laplacian != 0 else None
         # probe-fit workspace: three propagated probe-sized arrays and 32 KiB of partial sums
         self._pfw = (z(3 * self.ndist * self.nz * self.n + 4096, dt=torch.complex64)
                      if self.lam_prbfit != 0 else None)

@@ -321,7 +321,8 @@ int ht_prbfit_forms(ht_prop_s* prop, const void* prb, const void* d1, const void
 /* ------------------------------------------------------------------------
  * 3-D Laplacian regulariser (rec_mpi.py:402-496).  Arrays [nz, ny, nx],
  * complex64 (is_complex) or float32; work: (nz + 2) * ny * nx elements of the
- * same type.  L: the 7-point Laplacian, periodic in y and x, of the object
+ * same type, then, from the next 16-byte boundary, 64 KiB for the per-block
+ * partial sums of the forms and the energy (added in a fixed order).  L: the 7-point Laplacian, periodic in y and x, of the object
  * zero-padded in z; B = L o L with the inner L also on the ghost slice at each
  * end, as the reference evaluates it.
  * --------------------------------------------------------------------- */
