@@ -734,6 +734,8 @@ __global__ void k_sum_theta(const float2* __restrict__ Pc, float2* __restrict__ 
   const int k = (int)(i / npix);
   const long p = i % npix;
   double sx = 0.0, sy = 0.0;
+  // unrolled: the loads of eight angles are in flight, the sums keep angle order
+#pragma unroll 8
   for (long th = 0; th < ntheta; ++th) {
     const float2 v = Pc[(th * ndist + k) * npix + p];
     sx += v.x;
