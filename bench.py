@@ -914,7 +914,7 @@ def served_vs_plain(nreq, niter, seed):
         torch.cuda.empty_cache()
         for r in reqs:
             r.latencies_ms, r.result, r.t_admit, r.t_done = [], None, None, None
-        srv = Server(max_active=8)
+        srv = Server(max_active=4)
         for r in reqs:
             srv.submit(r)
         srv.run(realtime=realtime)

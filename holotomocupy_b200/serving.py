@@ -132,9 +132,11 @@ class Server:
     threads, so that the launch loop keeps feeding the GPU meanwhile; False
     runs them inline in the loop.  reuse: a request takes over the Rec of a
     retired request with the same arguments (Rec.reset) instead of freeing
-    it and allocating its own."""
+    it and allocating its own.  max_active: requests resident at once; more
+    than a few make their working sets compete for L2 (a saturated stream of
+    64 reconstructions of 128^3-512^3: 28.6 s with 4, 29-32 s with 8)."""
 
-    def __init__(self, budget_bytes=None, max_active=16, graphs=True, device=None, depth=4, host_workers=True,
+    def __init__(self, budget_bytes=None, max_active=4, graphs=True, device=None, depth=4, host_workers=True,
                  reuse=True):
         self.device = torch.device("cuda", torch.cuda.current_device() if device is None else device)
         if budget_bytes is None:
