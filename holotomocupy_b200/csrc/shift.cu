@@ -478,6 +478,61 @@ k_symbol_cols(const float2* in, float2* out, int ncols, const float* __restrict_
   fft_line_to<N, true, typename ColCfg<N>::PL>(sm, GColOut{out + off, ncols, valid}, t, tw4);
 }
 
+// The z pass at 512 rows: one 32-thread group per column, 16 samples a
+// thread, radices 8-8-8.  Thread t holds butterflies t and t + 32 of the
+// forward FFT's last stage (P = 64), i.e. samples b + 64 j, which are also
+// the samples of the inverse FFT's first stage (P = 1) on the same
+// butterflies: the symbol multiplies them in registers and the spectrum makes
+// no round trip through shared memory between the two transforms.  The same
+// butterflies as k_symbol_cols; the results agree to an ulp (the compiler
+// may fuse a complex product's multiply-adds differently in the two).
+constexpr int kSym512C = 8, kSym512Threads = 32 * kSym512C;
+
+__global__ void __launch_bounds__(kSym512Threads)
+k_symbol_cols512(const float2* in, float2* out, int ncols, const float* __restrict__ sym,
+                 const float2* __restrict__ tw4) {
+  constexpr int N = 512, E = 16, C = kSym512C;
+  extern __shared__ float2 tile[];
+  const int c = threadIdx.x % C, t = threadIdx.x / C;
+  const bool valid = blockIdx.x * C + c < ncols;
+  const int col = min((int)blockIdx.x * C + c, ncols - 1);
+  const long off = (long)blockIdx.y * N * ncols + col;
+  SmCol<C> sm{tile + c};
+  const CtaSync sync{};
+  float2 v[E];
+  // forward FFT: stage 1 (from global memory) and stage 2
+  fft_stage<N, E, 8, 1, false, false, true>(v, SplitView<GColIn, SmCol<C>>{GColIn{in + off, ncols, valid}, sm}, t,
+                                            tw4, sync);
+  fft_stage<N, E, 8, 8, false, true, true>(v, sm, t, tw4, sync);
+  // stage 3 (P = 64) kept in registers: v[8 s + j] = X[b_s + 64 j], b_s = t + 32 s; times the symbol
+#pragma unroll
+  for (int s2 = 0; s2 < 2; ++s2) {
+    const int b = t + 32 * s2;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) v[8 * s2 + j] = sm.ld(b + 64 * j);
+    float2 w[8];
+    twiddles<8, false>(tw4, b, N, w);
+#pragma unroll
+    for (int j = 1; j < 8; ++j) v[8 * s2 + j] = cmul(v[8 * s2 + j], w[j]);
+    Dft<8, false>::run(&v[8 * s2]);
+#pragma unroll
+    for (int j = 0; j < 8; ++j) v[8 * s2 + j] = cscale(v[8 * s2 + j], __ldg(&sym[b + 64 * j]));
+  }
+  sync();  // every stage-3 load is done before the stores below
+  // inverse FFT: stage 1 (P = 1) on the same butterflies, then stages 2 and 3 (to global memory)
+#pragma unroll
+  for (int s2 = 0; s2 < 2; ++s2) {
+    const int b = t + 32 * s2;
+    Dft<8, true>::run(&v[8 * s2]);
+#pragma unroll
+    for (int j = 0; j < 8; ++j) sm.st(b * 8 + j, v[8 * s2 + j]);
+  }
+  sync();
+  fft_stage<N, E, 8, 8, true, true, true>(v, sm, t, tw4, sync);
+  fft_stage<N, E, 8, 64, true, false, false>(v, SplitView<SmCol<C>, GColOut>{sm, GColOut{out + off, ncols, valid}},
+                                             t, tw4, sync);
+}
+
 template <int N>
 static cudaError_t l_symbol_rows(const float2* in, float2* out, long nrows, const float* sym, const float2* tw,
                                  cudaStream_t st) {
@@ -492,6 +547,13 @@ static cudaError_t l_symbol_rows(const float2* in, float2* out, long nrows, cons
 template <int N>
 static cudaError_t l_symbol_cols(const float2* in, float2* out, long nimg, int ncols, const float* sym,
                                  const float2* tw, cudaStream_t st) {
+  if constexpr (N == 512) {
+    constexpr int smem = N * kSym512C * (int)sizeof(float2);
+    k_symbol_cols512<<<dim3((ncols + kSym512C - 1) / kSym512C, (unsigned)nimg), kSym512Threads, smem, st>>>(
+        in, out, ncols, sym, tw);
+    ::ht::count_launch();
+    return cudaGetLastError();
+  }
   using CF = ColCfg<N>;
   cudaError_t e = allow_smem(k_symbol_cols<N>, CF::SMEM);
   if (e != cudaSuccess) return e;
