@@ -1065,7 +1065,7 @@ def end_to_end(a, rec, obj_true, prb0, pos0, data, device, barrier, world):
         torch.cuda.synchronize()
         if s > 0:
             times.append(e0.elapsed_time(e1))
-    ms = float(np.mean(times))
+    ms = max_over_ranks([float(np.mean(times))], device)[0]   # the slowest replica (every rank calls this)
     return {"value": world * a.e2e_iters * 1e3 / ms, "unit": UNIT, "h2d_bytes_per_step": h2d,
             "d2h_bytes_per_step": d2h, "iterations_per_step": a.e2e_iters, "ms_per_step": ms,
             "step": "upload data + initial obj/prb/pos from pinned host memory, Rec.BH(mode='graph') with the "
