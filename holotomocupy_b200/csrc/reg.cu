@@ -165,9 +165,11 @@ __global__ void k_lap_finish(const double* __restrict__ part, int nblk, double s
 }
 
 // Per-block partial sums of the forms and the energy sit after the extended
-// Laplacian in the workspace, at the next 16-byte boundary (at most
-// 148 * 16 blocks, two doubles each).
+// Laplacian in the workspace, at the next 16-byte boundary: at most
+// kRegMaxBlocks blocks, two doubles each, within the 64 KiB reserved there.
+constexpr long kRegMaxBlocks = 148L * 16;
 constexpr long kLapPartBytes = 64 * 1024;
+static_assert(kRegMaxBlocks * 2 * (long)sizeof(double) <= kLapPartBytes, "partial sums exceed their area");
 static double* lap_partials(void* work, int nz, int ny, int nx, int is_complex) {
   const long off = ((long)(nz + 2) * ny * nx * (is_complex ? 8 : 4) + 15) / 16 * 16;
   return reinterpret_cast<double*>(static_cast<char*>(work) + off);
@@ -176,12 +178,12 @@ static double* lap_partials(void* work, int nz, int ny, int nx, int is_complex) 
 // k_lap_apply's grid: CTAs over the rows (z, y) of the volume
 static unsigned reg_grid_rows(int nz, int ny) {
   const long rows = (long)nz * ny;
-  return (unsigned)std::max<long>(1, std::min<long>(rows, 148L * 16));
+  return (unsigned)std::max<long>(1, std::min<long>(rows, kRegMaxBlocks));
 }
 
 static unsigned reg_grid(long n) {
   long g = (n + kRegThreads - 1) / kRegThreads;
-  if (g > 148L * 16) g = 148L * 16;
+  if (g > kRegMaxBlocks) g = kRegMaxBlocks;
   return (unsigned)(g < 1 ? 1 : g);
 }
 
