@@ -213,6 +213,9 @@ class Rec:
         # the prefilter as Cx inside R / R^T and Cz on the volume (complex
         # objects); vars/grads/etas "proj" are recomputed by bh_finish()
         self._fold = self.complex_obj
+        # the folded (complex-object) iteration allocates nothing, so it may be
+        # recorded into a CUDA graph
+        self.graphable = self._fold
         self._vol = z(self.nzobj, self.nobj, self.nobj) if self._fold else None
         # Laplacian regulariser workspace: the inner Laplacian on nzobj + 2 slices, then
         # 64 KiB of per-block partial sums from the next 16-byte boundary
@@ -452,14 +455,17 @@ class Rec:
 
         mode="host" iterates as the reference does (step sizes on the host).
         mode="graph" keeps the step sizes on the device and replays the
-        steady-state iteration from a CUDA graph (same arithmetic; needs no
-        error table and no checkpoints).  ``writer``
+        steady-state iteration from a CUDA graph (same arithmetic; complex
+        objects, no error table and no checkpoints -- otherwise it iterates as
+        "host": the real-object iteration allocates temporaries, which a
+        recorded graph must not refer to).  ``writer``
         (checkpoint.Writer) saves obj/prb/pos every vis_step iterations
         (rec_mpi.py:837-860, vis_debug)."""
         self.bh_setup()
         niter = self.niter if niter is None else niter
         checkpoints = writer is not None and getattr(self, "vis_step", -1) not in (-1, 0, None)
-        if mode == "graph" and self.err_step == -1 and not checkpoints and niter > self.start_iter:
+        if (mode == "graph" and self.graphable and self.err_step == -1 and not checkpoints
+                and niter > self.start_iter):
             cur = torch.cuda.current_stream(self.device)
             side = torch.cuda.Stream(device=self.device)
             side.wait_stream(cur)
@@ -622,7 +628,13 @@ class Rec:
         """Record one steady-state device-scalar iteration (not the first) on
         the current stream into a CUDA graph; replay_iteration() then runs it
         with one launch.  Call after one iteration has run on this device (so
-        every kernel's launch attributes are set).  Recording runs nothing."""
+        every kernel's launch attributes are set).  Recording runs nothing.
+        Complex objects only (graphable): the real-object iteration allocates
+        temporaries from the caching allocator, which may hand that memory to
+        another tensor, or release it, while the graph still writes there."""
+        if not self.graphable:
+            raise ValueError("capture_iteration: the real-object (float32) iteration allocates temporaries "
+                             "and cannot be recorded; use bh_iteration(i, sync=False)")
         self.release_graph()
         st = _lib.stream_ptr()
         gc_on = gc.isenabled()

@@ -126,6 +126,9 @@ class _Slot:
 class Server:
     """Persistent request loop (continuous batching of BH reconstructions).
 
+    graphs: replay a request's steady-state iteration from a CUDA graph
+    (complex objects; a real-object request launches each iteration, with
+    the same device-side step sizes, since its iteration allocates).
     depth: iterations a request may have queued on its stream.  host_workers:
     admissions (building the Rec, uploading, the set-up pass) and retirements
     (the final pass, copying the results to the host) run on two host worker
@@ -208,7 +211,7 @@ class Server:
         ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         with torch.cuda.stream(slot.stream):
             ev0.record(slot.stream)
-            if slot.it == 0 or not self.graphs:
+            if slot.it == 0 or not self.graphs or not rec.graphable:   # real objects run eagerly
                 rec.bh_iteration(rec.start_iter + slot.it, sync=False)
             elif rec._graph is None and not self._dev_lock.acquire(blocking=False):
                 rec.bh_iteration(rec.start_iter + slot.it, sync=False)   # record on a later launch

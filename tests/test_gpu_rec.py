@@ -258,6 +258,36 @@ def test_bh_32_iterations_against_fp64_oracle(golden, mode):
         assert rel_l2(rec.vars[k].cpu().numpy(), orc.vars[k]) < 1e-4, k
 
 
+@pytest.mark.parametrize("mode", ["host", "graph"])
+def test_bh_real_object_against_fp64_oracle(golden, mode):
+    """A real-valued (obj_dtype float32) object: 8 BH iterations on the golden
+    problem (the real part of its object) stay within rel L2 1e-4 of the
+    FP64 oracle's BH.  This iteration allocates temporaries, so
+    mode="graph" iterates as "host" and records no graph."""
+    from oracle import holo_oracle as O
+    from holotomocupy_b200.rec import Rec
+    g = golden("rec")
+    n, ntheta, ndist, nobj, _ = [int(v) for v in g["bh_dims"]]
+    args = rec_args(n, ntheta, ndist, nobj, 8)
+    args.obj_dtype = "float32"
+    rec = Rec(args)
+    orc = O.Rec(args, "complex128")
+    assert rec.vars["obj"].dtype == torch.float32 and not rec.graphable
+    for r, put in ((rec, cuda), (orc, lambda a: a)):
+        r.vars["obj"][:] = put(np.ascontiguousarray(g["bh_obj_true"].real))
+        r.vars["prb"][:] = put(g["bh_prb_true"])
+        r.vars["pos"][:] = put(g["bh_pos_true"])
+        r.gen_sqrt_data(r.vars, r.data)
+        r.vars["obj"][:] = 0
+        r.vars["prb"][:] = 1
+        r.vars["pos"][:] = put(g["bh_pos_true"] + g["bh_pos_err"])
+    rec.BH(mode=mode)
+    orc.BH()
+    assert rec._graph is None
+    for k in ("obj", "prb", "pos"):
+        assert rel_l2(rec.vars[k].cpu().numpy(), orc.vars[k]) < 1e-4, k
+
+
 def test_laplacian_terms_match_reference(golden):
     """gradient_laplacian, hessian_laplacian and the energy against the
     reference's own values (rec_mpi.py:402-496)."""

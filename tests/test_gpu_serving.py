@@ -147,3 +147,66 @@ def test_reused_rec_gives_the_result_alone():
         for k in ("obj", "prb", "pos"):
             assert rel_l2(got[k].numpy(), ref[k].numpy()) < 1e-5, (r.rid, k)
         assert len(got["history"]) == r.niter
+
+
+def test_real_object_iterations_are_launched_not_recorded():
+    """A real-valued (float32) object's iteration allocates temporaries, so it
+    is never recorded into a graph: capture_iteration() raises before any
+    recording starts; the device-scalar iteration matches the host one step
+    for step; BH(mode="graph") iterates as "host"; the server serves such a
+    request beside a complex one with the results each has alone."""
+    import copy
+    from holotomocupy_b200.rec import Rec
+    from holotomocupy_b200.serving import Request, Server, run_plain
+    from holotomocupy_b200.synthetic import make_problem
+    args, data, prb0, pos0, _ = make_problem(64, 112, 4, 31)
+    args.obj_dtype = "float32"
+    out = []
+    st = torch.cuda.Stream()
+    with torch.cuda.stream(st):
+        for mode in ("host", "device"):
+            rec = Rec(args)
+            assert not rec.graphable
+            rec.data.copy_(data)
+            rec.vars["prb"].copy_(prb0)
+            rec.vars["pos"].copy_(pos0)
+            rec.bh_setup()
+            hist = [rec.bh_iteration(i, sync=mode == "host") for i in range(4)]
+            if mode == "device":
+                hist = list(rec.bh_history())
+                with pytest.raises(ValueError):
+                    rec.capture_iteration()
+                assert rec._graph is None
+            rec.bh_finish()
+            out.append((hist, {k: rec.vars[k].cpu().numpy() for k in ("obj", "prb", "pos")}))
+            rec.close()
+    (h0, v0), (h1, v1) = out
+    np.testing.assert_allclose(np.array(h1), np.array(h0), rtol=1e-9)
+    for k in v0:
+        assert rel_l2(v1[k], v0[k]) < 1e-6, k
+    res = []
+    for mode in ("host", "graph"):
+        rec = Rec(args)
+        rec.data.copy_(data)
+        rec.vars["prb"].copy_(prb0)
+        rec.vars["pos"].copy_(pos0)
+        record = []
+        rec.BH(niter=4, record=record, mode=mode)
+        assert rec._graph is None and len(record) == 4
+        res.append({k: rec.vars[k].cpu().numpy() for k in ("obj", "prb", "pos")})
+        rec.close()
+    for k in res[0]:
+        assert rel_l2(res[1][k], res[0][k]) < 1e-6, k
+    cargs, cdata, cprb0, cpos0, _ = make_problem(64, 112, 4, 32)
+    reqs = [Request(rid=0, args=copy.copy(args), data=data, prb0=prb0, pos0=pos0, niter=5, arrival=0.0),
+            Request(rid=1, args=cargs, data=cdata, prb0=cprb0, pos0=cpos0, niter=5, arrival=0.0)]
+    _, _, alone = run_plain(reqs)
+    srv = Server(max_active=4)
+    for r in reqs:
+        srv.submit(r)
+    done = {r.rid: r for r in srv.run(realtime=False)}
+    for r, ref in zip(reqs, alone):
+        got = done[r.rid].result
+        assert got["obj"].dtype == (torch.float32 if r.rid == 0 else torch.complex64)
+        for k in ("obj", "prb", "pos"):
+            assert rel_l2(got[k].numpy(), ref[k].numpy()) < 1e-5, (r.rid, k)
