@@ -466,6 +466,7 @@ class Rec:
         checkpoints = writer is not None and getattr(self, "vis_step", -1) not in (-1, 0, None)
         if (mode == "graph" and self.graphable and self.err_step == -1 and not checkpoints
                 and niter > self.start_iter):
+            self.reserve_history(niter - self.start_iter)
             cur = torch.cuda.current_stream(self.device)
             side = torch.cuda.Stream(device=self.device)
             side.wait_stream(cur)
@@ -623,6 +624,18 @@ class Rec:
         """(alpha, beta) of the device-scalar iterations since bh_setup()."""
         n = min(int(self._count.item()), self._hist_cap)
         return [tuple(r) for r in self._hist[:n].cpu().numpy()]
+
+    def reserve_history(self, n):
+        """Room for n device-side (alpha, beta) pairs (4096 by default; the
+        pairs beyond the room are counted but not kept).  A larger history
+        replaces the buffer, so the recorded graph, which refers to the old
+        one, is released: call before recording."""
+        if n > self._hist_cap:
+            self.release_graph()
+            old, k = self._hist, self._hist_cap
+            self._hist_cap = int(n)
+            self._hist = torch.zeros(self._hist_cap, 2, dtype=torch.float64, device=self.device)
+            self._hist[:k].copy_(old)
 
     def capture_iteration(self):
         """Record one steady-state device-scalar iteration (not the first) on

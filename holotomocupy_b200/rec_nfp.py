@@ -281,6 +281,15 @@ class RecNFP:
         n = min(int(self._count.item()), self._hist_cap)
         return [tuple(r) for r in self._hist[:n].cpu().numpy()]
 
+    def reserve_history(self, n):
+        """Room for n device-side (alpha, beta) pairs, as Rec.reserve_history."""
+        if n > self._hist_cap:
+            self.release_graph()
+            old, k = self._hist, self._hist_cap
+            self._hist_cap = int(n)
+            self._hist = torch.zeros(self._hist_cap, 2, dtype=torch.float64, device=self.device)
+            self._hist[:k].copy_(old)
+
     def BH(self, writer=None, niter=None, record=None, mode="host"):
         """rec_nfp_mpi.py:100-144.  ``record`` (a list) receives (iteration,
         alpha, beta).  mode="host" iterates as the reference does (step sizes
@@ -293,6 +302,7 @@ class RecNFP:
         self.error_debug(vars, -1)
         self._count.zero_()
         if mode == "graph" and self.complex_obj and self.err_step == -1 and niter > self.start_iter:
+            self.reserve_history(niter - self.start_iter)
             cur = torch.cuda.current_stream(self.device)
             side = torch.cuda.Stream(device=self.device)
             side.wait_stream(cur)

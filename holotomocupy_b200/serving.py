@@ -192,6 +192,7 @@ class Server:
                 rec.vars["obj"].copy_(r.obj0, non_blocking=True)
             rec.vars["prb"].copy_(r.prb0, non_blocking=True)
             rec.vars["pos"].copy_(r.pos0, non_blocking=True)
+            rec.reserve_history(r.niter)
             rec.bh_setup()
         slot.rec = rec
 

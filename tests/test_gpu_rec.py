@@ -258,6 +258,28 @@ def test_bh_32_iterations_against_fp64_oracle(golden, mode):
         assert rel_l2(rec.vars[k].cpu().numpy(), orc.vars[k]) < 1e-4, k
 
 
+def test_graph_history_beyond_the_default_room(golden):
+    """BH(mode="graph") over more iterations than the device-side step-size
+    history holds by default (4096) keeps every (alpha, beta) pair: the room
+    is reserved before the iteration is recorded."""
+    from holotomocupy_b200.rec import Rec
+    g = golden("rec")
+    n, ntheta, ndist, nobj, _ = [int(v) for v in g["bh_dims"]]
+    niter = 4100
+    rec = Rec(rec_args(n, ntheta, ndist, nobj, niter))
+    rec.vars["obj"][:] = cuda(g["bh_obj_true"])
+    rec.vars["prb"][:] = cuda(g["bh_prb_true"])
+    rec.vars["pos"][:] = cuda(g["bh_pos_true"])
+    rec.gen_sqrt_data(rec.vars, rec.data)
+    rec.vars["obj"][:] = 0
+    rec.vars["prb"][:] = 1
+    rec.vars["pos"][:] = cuda(g["bh_pos_true"] + g["bh_pos_err"])
+    record = []
+    rec.BH(mode="graph", record=record)
+    assert rec._hist_cap >= niter and int(rec._count.item()) == niter
+    assert [r[0] for r in record] == list(range(niter))
+
+
 @pytest.mark.parametrize("mode", ["host", "graph"])
 def test_bh_real_object_against_fp64_oracle(golden, mode):
     """A real-valued (obj_dtype float32) object: 8 BH iterations on the golden
