@@ -232,6 +232,41 @@ def rec_cases(ns):
     np.savez_compressed(os.path.join(HERE, "rec.npz"), **out)
 
 
+def realbh_cases(ns):
+    """A short BH run with a real-valued object (obj_dtype float32): the
+    reference's real-object path (rec_mpi.py:721, the real part of the
+    back-propagated projections)."""
+    n, ntheta, ndist, nobj, niter = 32, 12, 2, 32, 4
+    rng = np.random.default_rng(17)
+    args = rec_args(n, ntheta, ndist, nobj, niter)
+    args.obj_dtype = "float32"
+    rec = ns.rec_mpi.Rec(args)
+    obj = np.ascontiguousarray(phantom(nobj, rng).real).astype("float32")
+    prb = (1 + 0.1 * crand(rng, (ndist, n, n))).astype("complex64")
+    pos = frand(rng, (ntheta, ndist, 2), 1.0)
+    pos_err = frand(rng, (ntheta, ndist, 2), 0.2)
+    rec.vars["obj"][:] = obj
+    rec.vars["prb"][:] = ns.cp.array(prb)
+    rec.vars["pos"][:] = ns.cp.array(pos)
+    rec.gen_sqrt_data(rec.vars, rec.data)
+    data = np.array(rec.data)
+    rec.vars["obj"][:] = 0
+    rec.vars["prb"][:] = ns.cp.array(1)
+    rec.vars["pos"][:] = ns.cp.array(pos + pos_err)
+    pairs = []
+    orig = rec.allreduce2
+    rec.allreduce2 = lambda a, b: (pairs.append((float(a), float(b))), orig(a, b))[1]
+    rec.BH()
+    out = {
+        "rbh_dims": np.array([n, ntheta, ndist, nobj, niter]), "rbh_obj_true": obj, "rbh_prb_true": prb,
+        "rbh_pos_true": pos, "rbh_pos_err": pos_err, "rbh_data": data,
+        "rbh_obj": np.array(rec.vars["obj"]), "rbh_prb": np.asarray(rec.vars["prb"]),
+        "rbh_pos": np.asarray(rec.vars["pos"]), "rbh_proj": np.array(rec.vars["proj"]),
+        "rbh_topbottom": np.array(pairs, dtype="float64"),
+    }
+    np.savez_compressed(os.path.join(HERE, "realbh.npz"), **out)
+
+
 def lap_cases(ns):
     """The 3-D Laplacian regulariser (rec_mpi.py:402-496): its gradient, Hessian
     form and energy at one point, and a 4-iteration BH run with lam_laplacian > 0."""
@@ -533,9 +568,11 @@ def main():
     if src is None:
         raise SystemExit("usage: make_golden.py <reference src dir>")
     ns = load_reference(src)
-    which = sys.argv[2:] or ["tomo", "prop", "shift", "rec", "lap", "sback", "c1", "prbfit", "rectomo", "nfp"]
+    which = sys.argv[2:] or ["tomo", "prop", "shift", "rec", "realbh", "lap", "sback", "c1", "prbfit", "rectomo",
+                             "nfp"]
     for w in which:
-        {"tomo": tomo_cases, "prop": prop_cases, "shift": shift_cases, "rec": rec_cases, "lap": lap_cases,
+        {"tomo": tomo_cases, "prop": prop_cases, "shift": shift_cases, "rec": rec_cases, "realbh": realbh_cases,
+         "lap": lap_cases,
          "sback": sback_cases, "c1": c1_cases, "prbfit": prbfit_cases, "rectomo": rectomo_cases,
          "nfp": nfp_cases}[w](ns)
         print("wrote", w)
