@@ -29,6 +29,7 @@ import numpy as np
 import torch
 
 from . import _lib
+from .convtable import log_error, new_table
 from .propagation import Propagation
 from .shift import Shift
 from .tomo import Tomo
@@ -94,7 +95,7 @@ class Rec:
         self.data_size = self.ntheta * self.ndist * self.nz * self.n
         self.prb_size = self.ndist * self.nz * self.n
         self.obj_size = self.nzobj * self.nobj ** 2
-        self.table = []
+        self.table = new_table()
         self.alloc_arrays()
         h = ctypes.c_void_p()
         _lib.call("ht_rec_create", self.n, self.nz, self.nobj, self.nzobj, self.angle_chunk, self.ndist,
@@ -173,7 +174,7 @@ class Rec:
                   self._bh, self._hist, self._count, self._vol, self._lapw, self._pfw, self._pf3, self._scal):
             if t is not None:
                 t.zero_()
-        self.table = []
+        self.table = new_table()
 
     # ------------------------------------------------------------ state
     def alloc_arrays(self):
@@ -673,7 +674,7 @@ class Rec:
             self._graph = None
 
     def error_debug(self, vars, i):
-        """rec_mpi.py:862-880 (the convergence table is kept in self.table)."""
+        """rec_mpi.py:862-880: a row of the convergence table self.table."""
         if self.err_step == -1 or i % self.err_step != 0:
             return
         if self._fold and i >= 0:   # proj is not kept up to date inside BH: use its coefficients
@@ -683,8 +684,7 @@ class Rec:
                 err += self.min(vars["prb"], None, vars["pos"], None, prbfit_only=True)
         else:
             err = self.min(vars["prb"], vars["obj"], vars["pos"], vars["proj"])
-        self.table.append((i, err, time.time() - self.time_start if i >= 0 else 0.0))
-        self.time_start = time.time()
+        log_error(self, i, err, "conv.csv")
 
     def gradients(self, vars, grads):
         """rec_mpi.py:305-325"""

@@ -30,6 +30,7 @@ import numpy as np
 import torch
 
 from . import _lib
+from .convtable import log_error, new_table
 from .propagation import Propagation
 from .shift import Shift
 
@@ -58,7 +59,7 @@ class RecNFP:
         self.cl_shift = Shift(self.n, self.nobj, self.nz, self.nzobj, self.obj_dtype)
         self.data_size = self.ntheta * self.nz * self.n
         self.prb_size = self.nz * self.n
-        self.table = []
+        self.table = new_table()
         self.alloc_arrays()
         h = ctypes.c_void_p()
         _lib.call("ht_rec_create", self.n, self.nz, self.nobj, self.nzobj, self.ntheta, 1,
@@ -176,12 +177,11 @@ class RecNFP:
                   _lib.ptr(vars["prb"].contiguous()), None, _lib.ptr(out), None, _lib.stream_ptr())
 
     def error_debug(self, vars, i):
-        """rec_nfp_mpi.py:442-458 (the table is kept in self.table)."""
+        """rec_nfp_mpi.py:442-458: a row of the convergence table self.table."""
         if self.err_step == -1 or i % self.err_step != 0:
             return
         err = self.min(vars["prb"], vars["proj"], vars["pos"])
-        self.table.append((i, err, time.time() - self.time_start if i >= 0 else 0.0))
-        self.time_start = time.time()
+        log_error(self, i, err, "conv_nfp.csv")
 
     # ------------------------------------------------------------------ BH
     def _axpby(self, x, y, a, b, dot=None):
