@@ -22,6 +22,7 @@ directly instead of deriving it from ``z1``/``energy`` (rec_mpi.py:55-60).
 """
 import ctypes
 import gc
+import logging
 import math
 import time
 
@@ -34,11 +35,19 @@ from .propagation import Propagation
 from .shift import Shift
 from .tomo import Tomo
 
+_log = logging.getLogger("holotomocupy_b200")
+
 
 def _t(x, device, dtype=None):
     if isinstance(x, torch.Tensor):
         return x.to(device=device, dtype=dtype or x.dtype)
     return torch.as_tensor(np.asarray(x), device=device, dtype=dtype)
+
+
+def position_drift(pos, pos_init):
+    """Mean over the angles of |pos - pos_init|: [ndist, 2] float64 (y, x in
+    pixels) from [ntheta, ndist, 2] position arrays."""
+    return (pos - pos_init).abs().double().sum(dim=0).cpu().numpy() / pos.shape[0]
 
 
 def reprod(a, b):
@@ -355,6 +364,11 @@ class Rec:
                   _lib.ptr(d2.contiguous()) if d2 is not None else None, _lib.ptr(self.ref), _lib.ptr(self._pfw),
                   out, self.lam_prbfit / self.prb_size, int(hess_slots), _lib.stream_ptr())
 
+    def hessian_prbfit(self, prb, dprb1, dprb2):
+        """rec_mpi.py:380-398: the probe-fit term's Hessian form at prb for
+        (dprb1, dprb2), summed in float64; 0 when lam_prbfit is 0."""
+        return self._prbfit_forms(prb, dprb1, dprb2)[1]
+
     def _prbfit_forms(self, prb, d1, d2):
         """hessian_prbfit (rec_mpi.py:379-398) for the pairs (d1,d1), (d1,d2), (d2,d2)
         (d2 None: d1 for both)."""
@@ -392,6 +406,11 @@ class Rec:
         acc = torch.zeros(1, dtype=torch.float64, device=self.device)
         self._lap_form(dobj1.contiguous(), self.etas["obj"], _lib.ptr(acc))
         return float(acc)
+
+    def _lap_energy_local(self):
+        """rec_mpi.py:472-496 under the reference's name (one GPU holds the
+        whole object, so the local energy is the energy)."""
+        return self._lap_energy()
 
     def _lap_energy(self):
         """rec_mpi.py:472-496"""
@@ -488,8 +507,8 @@ class Rec:
             if record is not None:
                 record.append((i, a, b))
             self.error_debug(self.vars, i)
-            if checkpoints and i % self.vis_step == 0 and i > self.start_iter:
-                writer.write_checkpoint(self.vars, i, self.norm_const)
+            if checkpoints:
+                self.vis_debug(self.vars, i, writer)
         return self.bh_finish()
 
     def bh_setup(self):
@@ -501,6 +520,7 @@ class Rec:
         vars["obj"] /= self.norm_const
         if self.start_iter == 0:
             vars["obj"] *= self.cl_tomo.mask
+        self.pos_init = vars["pos"].clone()   # rec_mpi.py:153, for vis_debug's drift
         self.fwd_tomo(vars["obj"], out=vars["proj"])
         self._coeff_into(vars["proj"], C["vars"])
         self.error_debug(vars, -1)
@@ -672,6 +692,20 @@ class Rec:
         if getattr(self, "_graph", None) is not None:
             _lib.lib().ht_graph_destroy(self._graph)
             self._graph = None
+
+    def vis_debug(self, vars, i, writer=None):
+        """rec_mpi.py:837-860: every vis_step iterations after the first, the
+        state goes to the checkpoint writer and the mean absolute drift of the
+        positions from their values at the start of BH is logged for each
+        distance.  Without a writer nothing happens (the reference draws the
+        state with matplotlib there)."""
+        if writer is None or self.vis_step in (-1, 0, None) or i % self.vis_step != 0 or i <= self.start_iter:
+            return
+        writer.write_checkpoint(vars, i, self.norm_const)
+        if getattr(self, "pos_init", None) is not None:
+            d = position_drift(vars["pos"], self.pos_init)
+            _log.warning("iteration %d: mean absolute position drift [px] %s", i,
+                         "; ".join(f"distance {j}: y {d[j, 0]:.4f} x {d[j, 1]:.4f}" for j in range(len(d))))
 
     def error_debug(self, vars, i):
         """rec_mpi.py:862-880: a row of the convergence table self.table."""
@@ -851,6 +885,12 @@ class Rec:
             for k in range(self.ndist):
                 y22[:, k] += self.cl_shift.dcurlySc(c, x33[:, k], self._eff(k), cw, w33[:, k])
         return [w31, y22]
+
+    def gF4(self, gradu, gradproj):
+        """rec_mpi.py:356-362: gradu = R^T gradproj, the object gradient from
+        the projections' gradient."""
+        self.cl_tomo.RT(gradproj.contiguous(), out=gradu)
+        return gradu
 
     def gF3(self, x, y):
         y21, y22 = y

@@ -1,7 +1,8 @@
-"""The BH solvers' convergence table (rec_mpi.py:85,862-880;
-rec_nfp_mpi.py:75,442-458): a DataFrame with the columns iter / err / time,
-the initial row at iter -1 with time 0, and the whole table rewritten to
-<path_out>/<name> after each row.  Host logic, on the CPU."""
+"""The BH solvers' host-side reporting: the convergence table
+(rec_mpi.py:85,862-880; rec_nfp_mpi.py:75,442-458) -- a DataFrame with the
+columns iter / err / time, the initial row at iter -1 with time 0, and the
+whole table rewritten to <path_out>/<name> after each row -- and vis_debug's
+checkpoints and position-drift log (rec_mpi.py:837-860).  On the CPU."""
 import time
 import types
 
@@ -50,3 +51,33 @@ def test_no_csv_without_path_out(tmp_path, monkeypatch):
     s = _solver()
     log_error(s, -1, 1.0, "conv.csv")
     assert not list(tmp_path.iterdir())
+
+
+def test_vis_debug_writes_checkpoints_and_logs_the_position_drift(caplog):
+    """Rec.vis_debug (rec_mpi.py:837-860): every vis_step iterations after
+    the first, the state goes to the writer with the normalisation constant,
+    and the mean absolute drift of the positions from BH's start is logged
+    per distance; without a writer, off-step or at the first iteration
+    nothing happens.  Host logic, run on CPU tensors."""
+    import numpy as np
+    import torch
+    from holotomocupy_b200.rec import Rec, position_drift
+
+    calls = []
+    writer = types.SimpleNamespace(write_checkpoint=lambda v, i, c: calls.append((i, c)))
+    pos0 = torch.zeros(4, 2, 2)
+    pos = pos0.clone()
+    pos[:, 0, 0] = torch.tensor([1.0, -1.0, 2.0, 0.0])     # distance 0, y: mean |drift| 1
+    pos[:, 1, 1] = 0.5                                       # distance 1, x: 0.5
+    fake = types.SimpleNamespace(vis_step=2, start_iter=0, norm_const=1.5, pos_init=pos0)
+    np.testing.assert_allclose(position_drift(pos, pos0), [[1.0, 0.0], [0.0, 0.5]])
+    with caplog.at_level("WARNING", logger="holotomocupy_b200"):
+        for i in range(5):
+            Rec.vis_debug(fake, {"pos": pos}, i, writer)
+        Rec.vis_debug(fake, {"pos": pos}, 6, None)
+    assert calls == [(2, 1.5), (4, 1.5)]
+    msgs = [r.getMessage() for r in caplog.records]
+    assert len(msgs) == 2 and "distance 0: y 1.0000 x 0.0000" in msgs[0] and "distance 1: y 0.0000 x 0.5000" in msgs[0]
+    fake.vis_step = -1
+    Rec.vis_debug(fake, {"pos": pos}, 4, writer)
+    assert len(calls) == 2
