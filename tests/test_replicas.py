@@ -33,7 +33,7 @@ def _rank(rank, world, port, out):
 def test_max_over_two_gloo_ranks():
     world = 2
     port = _free_port()
-    with mp.Manager() as m:
+    with mp.get_context("spawn").Manager() as m:   # no fork of this multi-threaded process
         out = m.dict()
         mp.start_processes(_rank, args=(world, port, out), nprocs=world, start_method="spawn")
         res = dict(out)
