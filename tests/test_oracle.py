@@ -43,6 +43,39 @@ def test_propagation(golden, tag, dt, tol):
     assert p.D(g[f"{tag}_a"][0], 1).shape == g[f"{tag}_D2d"].shape
 
 
+def _crand(rng, shape):
+    return rng.standard_normal(shape) + 1j * rng.standard_normal(shape)
+
+
+def test_tomo_adjoint():
+    """<R x, y> = <x, R^T y> in FP64 (the reference's tests/tomo/test_tomo.ipynb
+    adjoint check, asserted)."""
+    rng = np.random.default_rng(5)
+    n, nz, ntheta = 32, 4, 24
+    t = O.Tomo(n, nz, np.linspace(0, np.pi, ntheta, endpoint=False).astype("float32"), 1, "complex128")
+    x, y = _crand(rng, (nz, n, n)), _crand(rng, (ntheta, nz, n))
+    lhs, rhs = np.vdot(t.R(x), y), np.vdot(x, t.RT(y))
+    assert abs(lhs - rhs) / abs(lhs) < 1e-12
+
+
+def test_propagation_adjoint_and_energy():
+    """<D x, y> = <x, D^T y> in FP64, and D keeps the energy of a smooth field
+    away from the edges (the reference's
+    tests/propagation/test_propagation.py:42-88, adjoint and energy sections)."""
+    rng = np.random.default_rng(6)
+    n, nz = 48, 40
+    p = O.Propagation(n, nz, 2, 2, 7.3e-11, 20e-9, np.array([3e-3, 5e-3]), "complex128")
+    x, y = _crand(rng, (2, nz, n)), _crand(rng, (2, nz, n))
+    for j in range(2):
+        lhs, rhs = np.vdot(p.D(x, j), y), np.vdot(x, p.DT(y, j))
+        assert abs(lhs - rhs) / abs(lhs) < 1e-12
+    yy, xx = np.meshgrid(np.arange(nz) - nz / 2, np.arange(n) - n / 2, indexing="ij")
+    blob = np.exp(-(yy ** 2 + xx ** 2) / (2 * 4.0 ** 2))[None].astype("complex128")
+    d = p.D(blob, 0)
+    assert np.linalg.norm(d - blob) / np.linalg.norm(blob) > 0.5    # the field does change (measured 1.3)
+    assert abs(np.linalg.norm(d) / np.linalg.norm(blob) - 1) < 1e-9  # measured 6e-16
+
+
 def test_propagation_reference_table(golden):
     """table='ref32' rebuilds the reference's FP32 Fresnel table bit for bit."""
     g = golden("prop")
@@ -70,6 +103,25 @@ def test_shift(golden, key, dt, tol):
     o1, o2 = s.dcurlySadjc(c, G("r"), G("m"), G("g"))
     assert rel_l2(o1, G("dSadj1")) < tol
     assert rel_l2(o2, G("dSadj2")) < tol
+
+
+@pytest.mark.parametrize("ry,rx", [(0.0, 0.7), (1.3, -2.4), (-3.6, 0.25)])
+def test_curlyS_is_scipys_cubic_spline_shift(ry, rx):
+    """curlyS at unit magnification is a cubic B-spline interpolation: on an
+    object that is zero within n/4 of its edges it equals
+    scipy.ndimage.shift(order=3) (the comparison the reference's
+    tests/shift/test_shift.ipynb plots, here asserted; measured 1.4-1.9e-10)."""
+    import scipy.ndimage as nd
+    n = 64
+    s = O.Shift(n, n, n, n, "complex64", "complex128")
+    rng = np.random.default_rng(3)
+    pad = n // 4
+    a = np.zeros((1, n, n), "complex128")
+    a[0, pad:-pad, pad:-pad] = rng.standard_normal((n - 2 * pad,) * 2) + 1j * rng.standard_normal((n - 2 * pad,) * 2)
+    got = s.curlyS(a, np.array([[ry, rx]]), np.ones(1))[0]
+    ref = (nd.shift(a[0].real, [ry, rx], order=3, mode="constant", cval=0)
+           + 1j * nd.shift(a[0].imag, [ry, rx], order=3, mode="constant", cval=0))
+    assert rel_l2(got, ref) < 1e-8
 
 
 @pytest.mark.parametrize("dt,tol", [("complex64", TOL32), ("complex128", TOL64)])
