@@ -1,7 +1,9 @@
 """The CPU oracle against the golden vectors made by running the reference's
 own operators (tests/golden/make_golden.py).  FP32 mode must reproduce the
 reference to FP32 rounding; FP64 mode differs by the reference's own FP32
-error (and, for the propagator, by the FP32 rounding of its Fresnel table)."""
+error (and, for the propagator, by the FP32 rounding of its Fresnel table).
+Beside the fixtures, the properties the reference's own tests look at: the
+adjoints of R and D, D's energy, and curlyS against scipy's cubic spline."""
 import types
 
 import numpy as np
