@@ -81,3 +81,27 @@ def test_vis_debug_writes_checkpoints_and_logs_the_position_drift(caplog):
     fake.vis_step = -1
     Rec.vis_debug(fake, {"pos": pos}, 4, writer)
     assert len(calls) == 2
+
+
+def test_bh_loop_order_with_a_writer():
+    """Rec.BH's host loop (rec_mpi.py:163-227) with a checkpoint writer: each
+    iteration, then its error row, then vis_debug, which checkpoints every
+    vis_step iterations after the first; a writer turns mode="graph" into the
+    host loop.  The solver's steps are stand-ins; this is the loop's order."""
+    import torch
+    from holotomocupy_b200.rec import Rec
+
+    calls = []
+    fake = types.SimpleNamespace(niter=5, start_iter=0, err_step=-1, vis_step=2, graphable=True, norm_const=2.0,
+                                 vars={"pos": torch.zeros(3, 2, 2)}, pos_init=torch.zeros(3, 2, 2))
+    fake.bh_setup = lambda: calls.append("setup")
+    fake.bh_iteration = lambda i, sync=True: (calls.append(("it", i)), (0.1 * i, 0.2 * i))[1]
+    fake.error_debug = lambda v, i: calls.append(("err", i))
+    fake.bh_finish = lambda: (calls.append("finish"), fake.vars)[1]
+    fake.vis_debug = types.MethodType(Rec.vis_debug, fake)
+    writer = types.SimpleNamespace(write_checkpoint=lambda v, i, c: calls.append(("ck", i, c)))
+    record = []
+    Rec.BH(fake, writer=writer, record=record, mode="graph")
+    assert calls == ["setup", ("it", 0), ("err", 0), ("it", 1), ("err", 1), ("it", 2), ("err", 2), ("ck", 2, 2.0),
+                     ("it", 3), ("err", 3), ("it", 4), ("err", 4), ("ck", 4, 2.0), "finish"]
+    assert [r[0] for r in record] == [0, 1, 2, 3, 4]
