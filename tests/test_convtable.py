@@ -105,3 +105,18 @@ def test_bh_loop_order_with_a_writer():
     assert calls == ["setup", ("it", 0), ("err", 0), ("it", 1), ("err", 1), ("it", 2), ("err", 2), ("ck", 2, 2.0),
                      ("it", 3), ("err", 3), ("it", 4), ("err", 4), ("ck", 4, 2.0), "finish"]
     assert [r[0] for r in record] == [0, 1, 2, 3, 4]
+
+
+def test_bh_graph_mode_of_a_real_object_runs_the_host_loop():
+    """mode="graph" on an iteration that cannot be recorded (a real-valued
+    object: graphable False) runs the host loop, with the host step sizes."""
+    from holotomocupy_b200.rec import Rec
+
+    calls = []
+    fake = types.SimpleNamespace(niter=3, start_iter=0, err_step=-1, vis_step=-1, graphable=False, vars={})
+    fake.bh_setup = lambda: calls.append("setup")
+    fake.bh_iteration = lambda i, sync=True: (calls.append(("it", i, sync)), (1.0, 0.0))[1]
+    fake.error_debug = lambda v, i: None
+    fake.bh_finish = lambda: (calls.append("finish"), fake.vars)[1]
+    Rec.BH(fake, mode="graph")
+    assert calls == ["setup", ("it", 0, True), ("it", 1, True), ("it", 2, True), "finish"]
