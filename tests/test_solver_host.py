@@ -1,8 +1,9 @@
-"""The BH solvers' host-side reporting: the convergence table
+"""The BH solvers' host logic, on the CPU: the convergence table
 (rec_mpi.py:85,862-880; rec_nfp_mpi.py:75,442-458) -- a DataFrame with the
 columns iter / err / time, the initial row at iter -1 with time 0, and the
-whole table rewritten to <path_out>/<name> after each row -- and vis_debug's
-checkpoints and position-drift log (rec_mpi.py:837-860).  On the CPU."""
+whole table rewritten to <path_out>/<name> after each row; vis_debug's
+checkpoints and position-drift log (rec_mpi.py:837-860); and the order of
+Rec.BH's loop, with the solver's steps replaced by stand-ins."""
 import time
 import types
 
